@@ -1,0 +1,625 @@
+// capi.cu -- the C-ABI: receptor context, search orchestration, kernel.h-compatible calls.
+//
+// The search replaces the inline core of the reference drivers
+// (src/TranRotaConfSearchNoMini.cu:156-464): the receptor spectra are computed once at context
+// creation and stay resident; a search is cut into waves of rotations, each wave running the
+// five kernels of search_kernels.cu back to back on one stream. Only the per-rotation minimum
+// energy and best translation leave the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cdock_b200.h"
+#include "cdk_internal.h"
+
+namespace cdk {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+namespace {
+
+__global__ void k_build_tables(int nAtom, int nConf, int nQ, const float* quats,
+                               const float* charge, const float* eps, const int* slot,
+                               ConfDesc* confs, RotDesc* rots, AtomParam* params) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long nRot = (long)nConf * nQ;
+  if (t < nRot) {
+    RotDesc d;
+    for (int i = 0; i < 4; ++i) d.q[i] = quats[t * 4 + i];
+    d.conf = (int)(t / nQ);
+    d.out = (int)t;
+    d.pad0 = d.pad1 = 0;
+    rots[t] = d;
+  }
+  if (t < nConf) {
+    ConfDesc c;
+    c.coord_off = (int)t * nAtom;
+    c.param_off = 0;
+    c.n_atoms = nAtom;
+    c.pad = 0;
+    confs[t] = c;
+  }
+  if (t < nAtom) {
+    AtomParam p;
+    p.w_vdw = sqrtf(eps[t]);  // IEEE sqrt, as std::sqrt(float) in FillLigandGrid (:43)
+    p.charge = charge[t];
+    p.slot = slot[t];
+    p.pad = 0;
+    params[t] = p;
+  }
+}
+
+// largest atom-atom distance over all conformers, as float bits (non-negative floats order
+// like their bit patterns), plus a flag for slots outside [0, K-2]
+__global__ void k_diameter(int nAtom, int nConf, const float* coor, const int* slot, int K,
+                           unsigned int* out) {
+  const long total = (long)nConf * nAtom * nAtom;
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long)gridDim.x * blockDim.x) {
+    const long c = t / ((long)nAtom * nAtom);
+    const int i = (int)((t / nAtom) % nAtom), j = (int)(t % nAtom);
+    if (j <= i) continue;
+    const float* a = coor + (c * nAtom + i) * 3;
+    const float* b = coor + (c * nAtom + j) * 3;
+    const double dx = (double)a[0] - b[0], dy = (double)a[1] - b[1], dz = (double)a[2] - b[2];
+    const float d = (float)sqrt(dx * dx + dy * dy + dz * dz);
+    atomicMax(out, __float_as_uint(d));
+  }
+  const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t0 < nAtom && (slot[t0] < 0 || slot[t0] > K - 2)) atomicOr(out + 1, 1u);
+  if (t0 < (long)nConf * nAtom * 3 && !isfinite(coor[t0])) atomicOr(out + 1, 2u);
+}
+
+struct Arena {
+  void* base = nullptr;
+  size_t cap = 0;
+};
+
+bool grow(Arena& a, size_t bytes) {
+  if (bytes <= a.cap) return true;
+  if (a.base) cudaFree(a.base);
+  a.base = nullptr;
+  a.cap = 0;
+  if (cudaMalloc(&a.base, bytes) != cudaSuccess) return false;
+  a.cap = bytes;
+  return true;
+}
+
+size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+}  // namespace cdk
+
+using namespace cdk;
+
+struct cdk_ctx {
+  int dev = 0;
+  int n = 0, K = 0;
+  float spacing = 0.f;
+  cdk_opts opts{};
+  cudaStream_t stream = nullptr;
+  float* d_grids = nullptr;   // [K][n^3], kept for the FP64 re-score
+  float2* d_phat = nullptr;   // [n][K][ncol]
+  float2* d_tw = nullptr;     // [n]
+  Arena wave;                 // per-wave scratch
+  Arena tables;               // per-search tables
+  Arena io;                   // staging of host-buffer searches
+  unsigned int* d_misc = nullptr;  // [0] diameter bits, [1] flags, [2] error count
+  unsigned int* h_misc = nullptr;  // pinned mirror
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double stats[4] = {0, 0, 0, 0};
+};
+
+namespace {
+
+#define CDK_CUDA(call)                                                                 \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess) {                                                           \
+      set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                   \
+      return CDK_ERR_CUDA;                                                             \
+    }                                                                                  \
+  } while (0)
+
+bool supported_n(int n) { return n == 32 || n == 64 || n == 96 || n == 128; }
+
+// the search proper on device tables; nRot rotations, outputs indexed by RotDesc.out
+int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const ConfDesc* d_confs,
+              const RotDesc* d_rots, long nRot, int maxAtoms, int Lb, float* d_minE, int* d_idx,
+              cudaStream_t s) {
+  const int n = c->n, K = c->K;
+  const size_t ncol = (size_t)n * (n / 2 + 1);
+  int wave = c->opts.wave_rotations;
+  if (wave <= 0) {
+    // keep A + B of one wave near 6 GiB: big enough to fill the GPU, small next to HBM
+    const double per = (double)K * Lb * ncol * 8 + (double)n * ncol * 8;
+    wave = (int)std::min<double>(4096.0, std::max(64.0, 6.0 * (1ull << 30) / per));
+  }
+  wave = (int)std::min<long>(wave, std::min<long>(nRot, 65535));
+  if (wave < 1) wave = 1;
+  const size_t b_rotxyz = align_up((size_t)wave * maxAtoms * sizeof(float4));
+  const size_t b_rec = align_up((size_t)wave * sizeof(RotRec));
+  const size_t b_keys = align_up((size_t)wave * sizeof(unsigned long long));
+  const size_t b_A = align_up((size_t)wave * K * Lb * ncol * sizeof(float2));
+  const size_t b_B = align_up((size_t)wave * n * ncol * sizeof(float2));
+  if (!grow(c->wave, b_rotxyz + b_rec + b_keys + b_A + b_B)) {
+    set_error("cudaMalloc of the wave scratch failed (" +
+              std::to_string((b_rotxyz + b_rec + b_keys + b_A + b_B) >> 20) + " MiB)");
+    return CDK_ERR_NOMEM;
+  }
+  char* base = static_cast<char*>(c->wave.base);
+  WaveArgs a{};
+  a.n = n;
+  a.K = K;
+  a.Lb = Lb;
+  a.spacing = c->spacing;
+  a.max_atoms = maxAtoms;
+  a.coords = d_coor;
+  a.params = d_params;
+  a.confs = d_confs;
+  a.rot_xyz = reinterpret_cast<float4*>(base);
+  a.rec = reinterpret_cast<RotRec*>(base + b_rotxyz);
+  a.keys = reinterpret_cast<unsigned long long*>(base + b_rotxyz + b_rec);
+  a.A = reinterpret_cast<float2*>(base + b_rotxyz + b_rec + b_keys);
+  a.B = reinterpret_cast<float2*>(base + b_rotxyz + b_rec + b_keys + b_A);
+  a.phat = c->d_phat;
+  a.tw = c->d_tw;
+  a.minE = d_minE;
+  a.idx = d_idx;
+  a.err_count = reinterpret_cast<int*>(c->d_misc + 2);
+  a.col_tile = c->opts.col_tile > 0 ? c->opts.col_tile : pick_col_tile(n, K);
+  if (xpass_smem_bytes(n, K, a.col_tile) > 227 * 1024) {
+    set_error("column tile too large for shared memory");
+    return CDK_ERR_INVALID;
+  }
+  CDK_CUDA(cudaMemsetAsync(c->d_misc + 2, 0, sizeof(unsigned int), s));
+  long launches = 1, waves = 0;
+  for (long r0 = 0; r0 < nRot; r0 += wave) {
+    a.nrot = (int)std::min<long>(wave, nRot - r0);
+    a.rots = d_rots + r0;
+    CDK_CUDA(launch_prep(a, s));
+    CDK_CUDA(launch_spread_yz(a, s));
+    CDK_CUDA(launch_xpass(a, s));
+    CDK_CUDA(launch_yz_inv_argmin(a, s));
+    CDK_CUDA(launch_finalize(a, s));
+    launches += kLaunchesPerWave;
+    ++waves;
+  }
+  c->stats[0] = (double)launches;
+  c->stats[1] = (double)waves;
+  c->stats[2] = (double)nRot;
+  return CDK_OK;
+}
+
+// Checks inputs on the device (slots, finite coordinates) and plans the ligand box from the
+// largest atom-atom distance. Synchronises the stream once (4-byte read back).
+int plan_box(cdk_ctx* c, int nAtom, int nConf, const float* d_coor, const int* d_slot,
+             cudaStream_t s, int* Lb) {
+  CDK_CUDA(cudaMemsetAsync(c->d_misc, 0, 2 * sizeof(unsigned int), s));
+  const long pairs = (long)nConf * nAtom * nAtom;
+  long blocks = std::max<long>((pairs + 255) / 256, ((long)nConf * nAtom * 3 + 255) / 256);
+  blocks = std::min<long>(blocks, 4096);
+  k_diameter<<<(unsigned)std::max<long>(1, blocks), 256, 0, s>>>(nAtom, nConf, d_coor, d_slot,
+                                                                c->K, c->d_misc);
+  CDK_CUDA(cudaGetLastError());
+  CDK_CUDA(cudaMemcpyAsync(c->h_misc, c->d_misc, 2 * sizeof(unsigned int),
+                           cudaMemcpyDeviceToHost, s));
+  CDK_CUDA(cudaStreamSynchronize(s));
+  if (c->h_misc[1] & 1u) {
+    set_error("atom slot outside [0, K-2]");
+    return CDK_ERR_INVALID;
+  }
+  if (c->h_misc[1] & 2u) {
+    set_error("non-finite ligand coordinate");
+    return CDK_ERR_INVALID;
+  }
+  float diam;
+  std::memcpy(&diam, &c->h_misc[0], sizeof(float));
+  // the spread touches x planes up to int(len/h)+1 with len <= diameter; two planes of slack
+  // absorb rounding of rotated coordinates and non-unit quaternions
+  const int lb = (int)std::floor(diam / c->spacing + 1e-3) + 3;
+  *Lb = std::min(c->n, std::max(lb, 2));
+  return CDK_OK;
+}
+
+int search_device_impl(cdk_ctx* c, int nAtom, int nConf, const float* d_coor,
+                       const float* d_charge, const float* d_eps, const int* d_slot, int nQ,
+                       const float* d_quats, float* d_minE, int* d_idx, cudaStream_t s) {
+  if (nAtom <= 0 || nConf <= 0 || nQ < 0) {
+    set_error("nAtom and nConf must be positive, nQ non-negative");
+    return CDK_ERR_INVALID;
+  }
+  if (nAtom > c->opts.max_atoms) {
+    set_error("ligand has more atoms than the context's max_atoms");
+    return CDK_ERR_INVALID;
+  }
+  const long nRot = (long)nConf * nQ;
+  if (nRot == 0) return CDK_OK;
+  if (nRot > (1l << 31) / 4) {
+    set_error("too many rotations in one call");
+    return CDK_ERR_INVALID;
+  }
+  CDK_CUDA(cudaSetDevice(c->dev));
+  int Lb = 0;
+  int rc = plan_box(c, nAtom, nConf, d_coor, d_slot, s, &Lb);
+  if (rc) return rc;
+  const size_t b_conf = align_up(sizeof(ConfDesc) * nConf);
+  const size_t b_rot = align_up(sizeof(RotDesc) * nRot);
+  const size_t b_par = align_up(sizeof(AtomParam) * nAtom);
+  if (!grow(c->tables, b_conf + b_rot + b_par)) {
+    set_error("cudaMalloc of the search tables failed");
+    return CDK_ERR_NOMEM;
+  }
+  char* tb = static_cast<char*>(c->tables.base);
+  ConfDesc* confs = reinterpret_cast<ConfDesc*>(tb);
+  RotDesc* rots = reinterpret_cast<RotDesc*>(tb + b_conf);
+  AtomParam* params = reinterpret_cast<AtomParam*>(tb + b_conf + b_rot);
+  CDK_CUDA(cudaEventRecord(c->ev0, s));
+  const long tmax = std::max<long>(nRot, std::max(nConf, nAtom));
+  k_build_tables<<<(unsigned)((tmax + 255) / 256), 256, 0, s>>>(
+      nAtom, nConf, nQ, d_quats, d_charge, d_eps, d_slot, confs, rots, params);
+  CDK_CUDA(cudaGetLastError());
+  rc = run_waves(c, d_coor, params, confs, rots, nRot, nAtom, Lb, d_minE, d_idx, s);
+  if (rc) return rc;
+  CDK_CUDA(cudaEventRecord(c->ev1, s));
+  return CDK_OK;
+}
+
+int check_errors_after(cdk_ctx* c, cudaStream_t s) {
+  CDK_CUDA(cudaMemcpyAsync(c->h_misc + 2, c->d_misc + 2, sizeof(unsigned int),
+                           cudaMemcpyDeviceToHost, s));
+  CDK_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, c->ev0, c->ev1) == cudaSuccess) c->stats[3] = ms;
+  if (c->h_misc[2] != 0) {
+    set_error(std::to_string(c->h_misc[2]) +
+              " rotation(s) overflowed the planned ligand box; results for them are invalid");
+    return CDK_ERR_OVERFLOW;
+  }
+  return CDK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cdk_version(void) { return "cdock_b200 0.1 (sm_100a)"; }
+
+int cdk_last_error(char* buf, size_t cap) {
+  const std::string& m = g_last_error;
+  if (buf && cap) {
+    size_t k = std::min(cap - 1, m.size());
+    std::memcpy(buf, m.data(), k);
+    buf[k] = 0;
+  }
+  return (int)m.size();
+}
+
+void cdk_opts_default(cdk_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->device = 0;
+  o->form = CDK_FORM_FP32;
+  o->wave_rotations = 0;
+  o->max_atoms = 256;
+  o->col_tile = 0;
+  o->use_graphs = 0;
+}
+
+int cdk_ctx_create(int nx, int ny, int nz, float spacing, int K, const float* grids,
+                   const cdk_opts* opts, cdk_ctx** out) {
+  if (!out || !grids) {
+    set_error("null argument");
+    return CDK_ERR_INVALID;
+  }
+  *out = nullptr;
+  if (nx != ny || ny != nz || !supported_n(nx)) {
+    set_error("grid must be cubic with edge 32, 64, 96 or 128");
+    return CDK_ERR_UNSUPPORTED;
+  }
+  if (K < 2 || K > KMAX) {
+    set_error("K must be in [2, 16]");
+    return CDK_ERR_UNSUPPORTED;
+  }
+  if (!(spacing > 0.f) || !std::isfinite(spacing)) {
+    set_error("spacing must be positive");
+    return CDK_ERR_INVALID;
+  }
+  cdk_ctx* c = new cdk_ctx();
+  if (opts) c->opts = *opts;
+  else cdk_opts_default(&c->opts);
+  if (c->opts.max_atoms <= 0) c->opts.max_atoms = 256;
+  if (c->opts.form != CDK_FORM_FP32) {
+    delete c;
+    set_error("only the FP32 form is built in this library");
+    return CDK_ERR_UNSUPPORTED;
+  }
+  c->dev = c->opts.device;
+  c->n = nx;
+  c->K = K;
+  c->spacing = spacing;
+  auto fail = [&](int code) {
+    cdk_ctx_destroy(c);
+    return code;
+  };
+#define CTX_CUDA(call)                                                   \
+  do {                                                                   \
+    cudaError_t e_ = (call);                                             \
+    if (e_ != cudaSuccess) {                                             \
+      set_error(std::string(#call) + ": " + cudaGetErrorString(e_));     \
+      return fail(e_ == cudaErrorMemoryAllocation ? CDK_ERR_NOMEM : CDK_ERR_CUDA); \
+    }                                                                    \
+  } while (0)
+  CTX_CUDA(cudaSetDevice(c->dev));
+  CTX_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CTX_CUDA(cudaEventCreate(&c->ev0));
+  CTX_CUDA(cudaEventCreate(&c->ev1));
+  const int n = nx;
+  const size_t N = (size_t)n * n * n, ncol = (size_t)n * (n / 2 + 1);
+  CTX_CUDA(cudaMalloc(&c->d_grids, sizeof(float) * K * N));
+  CTX_CUDA(cudaMalloc(&c->d_phat, sizeof(float2) * K * n * ncol));
+  CTX_CUDA(cudaMalloc(&c->d_tw, sizeof(float2) * n));
+  CTX_CUDA(cudaMalloc(&c->d_misc, 4 * sizeof(unsigned int)));
+  CTX_CUDA(cudaMallocHost(&c->h_misc, 4 * sizeof(unsigned int)));
+  std::vector<float2> tw(n);
+  for (int j = 0; j < n; ++j) {
+    const double ang = -2.0 * M_PI * j / n;
+    tw[j] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+  }
+  CTX_CUDA(cudaMemcpyAsync(c->d_tw, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice,
+                           c->stream));
+  CTX_CUDA(cudaMemcpyAsync(c->d_grids, grids, sizeof(float) * K * N, cudaMemcpyHostToDevice,
+                           c->stream));
+  float2* scratch = nullptr;
+  CTX_CUDA(cudaMalloc(&scratch, sizeof(float2) * K * n * ncol));
+  cudaError_t e = launch_receptor_fft(n, K, c->d_grids, scratch, c->d_phat, c->d_tw,
+                                      pick_col_tile(n, 1), c->stream);
+  cudaError_t e2 = cudaStreamSynchronize(c->stream);
+  cudaFree(scratch);
+  CTX_CUDA(e);
+  CTX_CUDA(e2);
+#undef CTX_CUDA
+  *out = c;
+  return CDK_OK;
+}
+
+int cdk_ctx_destroy(cdk_ctx* c) {
+  if (!c) return CDK_OK;
+  cudaSetDevice(c->dev);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaFree(c->d_grids);
+  cudaFree(c->d_phat);
+  cudaFree(c->d_tw);
+  cudaFree(c->d_misc);
+  if (c->h_misc) cudaFreeHost(c->h_misc);
+  cudaFree(c->wave.base);
+  cudaFree(c->tables.base);
+  cudaFree(c->io.base);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return CDK_OK;
+}
+
+int cdk_search_device(cdk_ctx* c, int nAtom, int nConf, const float* d_coor,
+                      const float* d_charge, const float* d_eps, const int* d_slot, int nQ,
+                      const float* d_quats, float* d_minE, int* d_idx, void* stream) {
+  if (!c || !d_coor || !d_charge || !d_eps || !d_slot || !d_minE || !d_idx ||
+      (nQ > 0 && !d_quats)) {
+    set_error("null argument");
+    return CDK_ERR_INVALID;
+  }
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  int rc = search_device_impl(c, nAtom, nConf, d_coor, d_charge, d_eps, d_slot, nQ, d_quats,
+                              d_minE, d_idx, s);
+  if (rc) return rc;
+  return check_errors_after(c, s);
+}
+
+int cdk_search(cdk_ctx* c, int nAtom, int nConf, const float* coor, const float* charge,
+               const float* eps, const int* slot, int nQ, const float* quats, float* minE,
+               int* idx, void* stream) {
+  if (!c || !coor || !charge || !eps || !slot || !minE || !idx || (nQ > 0 && !quats)) {
+    set_error("null argument");
+    return CDK_ERR_INVALID;
+  }
+  if (nAtom <= 0 || nConf <= 0 || nQ < 0) {
+    set_error("nAtom and nConf must be positive, nQ non-negative");
+    return CDK_ERR_INVALID;
+  }
+  const long nRot = (long)nConf * nQ;
+  if (nRot == 0) return CDK_OK;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  CDK_CUDA(cudaSetDevice(c->dev));
+  const size_t b_coor = align_up(sizeof(float) * 3 * nAtom * (size_t)nConf);
+  const size_t b_atom = align_up(sizeof(float) * nAtom);
+  const size_t b_q = align_up(sizeof(float) * 4 * nRot);
+  const size_t b_e = align_up(sizeof(float) * nRot);
+  const size_t b_i = align_up(sizeof(int) * 3 * nRot);
+  if (!grow(c->io, b_coor + 3 * b_atom + b_q + b_e + b_i)) {
+    set_error("cudaMalloc of the input staging failed");
+    return CDK_ERR_NOMEM;
+  }
+  char* p = static_cast<char*>(c->io.base);
+  float* d_coor = reinterpret_cast<float*>(p);
+  float* d_charge = reinterpret_cast<float*>(p + b_coor);
+  float* d_eps = reinterpret_cast<float*>(p + b_coor + b_atom);
+  int* d_slot = reinterpret_cast<int*>(p + b_coor + 2 * b_atom);
+  float* d_q = reinterpret_cast<float*>(p + b_coor + 3 * b_atom);
+  float* d_e = reinterpret_cast<float*>(p + b_coor + 3 * b_atom + b_q);
+  int* d_i = reinterpret_cast<int*>(p + b_coor + 3 * b_atom + b_q + b_e);
+  CDK_CUDA(cudaMemcpyAsync(d_coor, coor, sizeof(float) * 3 * nAtom * (size_t)nConf,
+                           cudaMemcpyHostToDevice, s));
+  CDK_CUDA(cudaMemcpyAsync(d_charge, charge, sizeof(float) * nAtom, cudaMemcpyHostToDevice, s));
+  CDK_CUDA(cudaMemcpyAsync(d_eps, eps, sizeof(float) * nAtom, cudaMemcpyHostToDevice, s));
+  CDK_CUDA(cudaMemcpyAsync(d_slot, slot, sizeof(int) * nAtom, cudaMemcpyHostToDevice, s));
+  CDK_CUDA(cudaMemcpyAsync(d_q, quats, sizeof(float) * 4 * nRot, cudaMemcpyHostToDevice, s));
+  int rc = search_device_impl(c, nAtom, nConf, d_coor, d_charge, d_eps, d_slot, nQ, d_q, d_e,
+                              d_i, s);
+  if (rc) return rc;
+  CDK_CUDA(cudaMemcpyAsync(minE, d_e, sizeof(float) * nRot, cudaMemcpyDeviceToHost, s));
+  CDK_CUDA(cudaMemcpyAsync(idx, d_i, sizeof(int) * 3 * nRot, cudaMemcpyDeviceToHost, s));
+  return check_errors_after(c, s);
+}
+
+int cdk_rescore_fp64(cdk_ctx* c, int nAtom, int nConf, const float* coor, const float* charge,
+                     const float* eps, const int* slot, int nPose, const int* rot_conf,
+                     const float* quats, const int* tidx, double* energy, void* stream) {
+  if (!c || !coor || !charge || !eps || !slot || !rot_conf || !quats || !tidx || !energy ||
+      nAtom <= 0 || nConf <= 0 || nPose < 0) {
+    set_error("invalid argument");
+    return CDK_ERR_INVALID;
+  }
+  if (nPose == 0) return CDK_OK;
+  for (int i = 0; i < nAtom; ++i)
+    if (slot[i] < 0 || slot[i] > c->K - 2) {
+      set_error("atom slot outside [0, K-2]");
+      return CDK_ERR_INVALID;
+    }
+  for (int i = 0; i < nPose; ++i)
+    if (rot_conf[i] < 0 || rot_conf[i] >= nConf) {
+      set_error("pose conformer index out of range");
+      return CDK_ERR_INVALID;
+    }
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  CDK_CUDA(cudaSetDevice(c->dev));
+  std::vector<ConfDesc> confs(nConf);
+  for (int i = 0; i < nConf; ++i) confs[i] = ConfDesc{i * nAtom, 0, nAtom, 0};
+  std::vector<RotDesc> rots(nPose);
+  for (int i = 0; i < nPose; ++i) {
+    for (int d = 0; d < 4; ++d) rots[i].q[d] = quats[i * 4 + d];
+    rots[i].conf = rot_conf[i];
+    rots[i].out = i;
+    rots[i].pad0 = rots[i].pad1 = 0;
+  }
+  std::vector<AtomParam> prm(nAtom);
+  for (int i = 0; i < nAtom; ++i) prm[i] = AtomParam{std::sqrt(eps[i]), charge[i], slot[i], 0};
+  const size_t b_coor = align_up(sizeof(float) * 3 * nAtom * (size_t)nConf);
+  const size_t b_conf = align_up(sizeof(ConfDesc) * nConf);
+  const size_t b_rot = align_up(sizeof(RotDesc) * nPose);
+  const size_t b_prm = align_up(sizeof(AtomParam) * nAtom);
+  const size_t b_t = align_up(sizeof(int) * 3 * nPose);
+  const size_t b_e = align_up(sizeof(double) * nPose);
+  void* buf = nullptr;
+  CDK_CUDA(cudaMallocAsync(&buf, b_coor + b_conf + b_rot + b_prm + b_t + b_e, s));
+  char* p = static_cast<char*>(buf);
+  float* d_coor = reinterpret_cast<float*>(p);
+  ConfDesc* d_conf = reinterpret_cast<ConfDesc*>(p + b_coor);
+  RotDesc* d_rot = reinterpret_cast<RotDesc*>(p + b_coor + b_conf);
+  AtomParam* d_prm = reinterpret_cast<AtomParam*>(p + b_coor + b_conf + b_rot);
+  int* d_t = reinterpret_cast<int*>(p + b_coor + b_conf + b_rot + b_prm);
+  double* d_e = reinterpret_cast<double*>(p + b_coor + b_conf + b_rot + b_prm + b_t);
+  cudaMemcpyAsync(d_coor, coor, sizeof(float) * 3 * nAtom * (size_t)nConf, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(d_conf, confs.data(), sizeof(ConfDesc) * nConf, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(d_rot, rots.data(), sizeof(RotDesc) * nPose, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(d_prm, prm.data(), sizeof(AtomParam) * nAtom, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(d_t, tidx, sizeof(int) * 3 * nPose, cudaMemcpyHostToDevice, s);
+  cudaError_t e = launch_rescore_fp64(c->n, c->K, c->spacing, c->d_grids, d_coor, d_prm, d_conf,
+                                      d_rot, d_t, nPose, d_e, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(energy, d_e, sizeof(double) * nPose, cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(buf, s);
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  CDK_CUDA(e);
+  CDK_CUDA(e2);
+  return CDK_OK;
+}
+
+int cdk_fill_ligand_grid(int nQ, int nAtom, const float* coors, const float* mincoors,
+                         const float* charge, const float* eps, const int* slot, int nVdwUsed,
+                         int x, int y, int z, float spacing, float* out) {
+  if (nQ <= 0 || nAtom <= 0 || nVdwUsed < 0 || x < 2 || y < 2 || z < 2 || !coors ||
+      !mincoors || !charge || !eps || !slot || !out) {
+    set_error("invalid argument");
+    return CDK_ERR_INVALID;
+  }
+  // every corner the spread touches must lie inside the grid (the reference does not check)
+  for (int q = 0; q < nQ; ++q)
+    for (int a = 0; a < nAtom; ++a) {
+      const int dims[3] = {x, y, z};
+      for (int d = 0; d < 3; ++d) {
+        const double v = ((double)coors[((size_t)q * nAtom + a) * 3 + d] - mincoors[q * 3 + d]) / spacing;
+        if (!(v >= 0.0) || (int)v + 1 >= dims[d]) {
+          set_error("an atom's cell lies outside the grid");
+          return CDK_ERR_INVALID;
+        }
+      }
+      if (nVdwUsed > 0 && (slot[a] < 0 || slot[a] >= nVdwUsed)) {
+        set_error("atom slot outside [0, nVdwUsed-1]");
+        return CDK_ERR_INVALID;
+      }
+    }
+  std::vector<AtomParam> prm(nAtom);
+  for (int i = 0; i < nAtom; ++i) prm[i] = AtomParam{std::sqrt(eps[i]), charge[i], slot[i], 0};
+  const size_t N = (size_t)x * y * z;
+  const size_t outElems = (size_t)nQ * (nVdwUsed + 1) * N;
+  float *d_c = nullptr, *d_m = nullptr, *d_o = nullptr;
+  AtomParam* d_p = nullptr;
+  int rc = CDK_OK;
+  cudaStream_t s = nullptr;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&d_c, sizeof(float) * 3 * nAtom * (size_t)nQ) != cudaSuccess ||
+      cudaMalloc(&d_m, sizeof(float) * 3 * nQ) != cudaSuccess ||
+      cudaMalloc(&d_p, sizeof(AtomParam) * nAtom) != cudaSuccess ||
+      cudaMalloc(&d_o, sizeof(float) * outElems) != cudaSuccess) {
+    set_error("device allocation failed");
+    rc = CDK_ERR_NOMEM;
+  } else {
+    cudaMemcpyAsync(d_c, coors, sizeof(float) * 3 * nAtom * (size_t)nQ, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_m, mincoors, sizeof(float) * 3 * nQ, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_p, prm.data(), sizeof(AtomParam) * nAtom, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(d_o, 0, sizeof(float) * outElems, s);
+    cudaError_t e = launch_fill_dense(nQ, nAtom, d_c, d_m, d_p, nVdwUsed, x, y, z, spacing, d_o, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(out, d_o, sizeof(float) * outElems, cudaMemcpyDeviceToHost, s);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+      set_error(std::string("fill: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+      rc = CDK_ERR_CUDA;
+    }
+  }
+  cudaFree(d_c);
+  cudaFree(d_m);
+  cudaFree(d_p);
+  cudaFree(d_o);
+  if (s) cudaStreamDestroy(s);
+  return rc;
+}
+
+int cdk_conj_mult(const void* d_potential_F, void* d_ligand_F, int odist, int K, int Q,
+                  void* stream) {
+  if (!d_potential_F || !d_ligand_F || odist <= 0 || K <= 0 || Q <= 0) {
+    set_error("invalid argument");
+    return CDK_ERR_INVALID;
+  }
+  CDK_CUDA(launch_conj_mult(static_cast<const float2*>(d_potential_F),
+                            static_cast<float2*>(d_ligand_F), odist, K, Q,
+                            static_cast<cudaStream_t>(stream)));
+  return CDK_OK;
+}
+
+int cdk_sum_grids(const void* d_ligand_F, void* d_sum_F, int K, int odist, int idist, int Q,
+                  void* stream) {
+  if (!d_ligand_F || !d_sum_F || odist <= 0 || K <= 0 || Q <= 0 || idist <= 0) {
+    set_error("invalid argument");
+    return CDK_ERR_INVALID;
+  }
+  CDK_CUDA(launch_sum_grids(static_cast<const float2*>(d_ligand_F), static_cast<float2*>(d_sum_F),
+                            K, odist, idist, Q, static_cast<cudaStream_t>(stream)));
+  return CDK_OK;
+}
+
+int cdk_ctx_stats(cdk_ctx* c, double* out, int n) {
+  if (!c || !out) return CDK_ERR_INVALID;
+  for (int i = 0; i < n && i < 4; ++i) out[i] = c->stats[i];
+  return CDK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,106 @@
+// cdk_internal.h -- device data layout and launch interface shared by the .cu files.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+namespace cdk {
+
+constexpr int KMAX = 16;  // most receptor grids one context can hold
+
+// One conformer's atoms: coords at coord_off (atoms), per-atom parameters at param_off.
+struct ConfDesc {
+  int coord_off;
+  int param_off;
+  int n_atoms;
+  int pad;
+};
+
+// One rotation of the search: unit quaternion (w,x,y,z), its conformer, the output slot.
+struct RotDesc {
+  float q[4];
+  int conf;
+  int out;
+  int pad0, pad1;
+};
+
+// Per-atom ligand parameters: sqrt(epsilon) as FillLigandGrid weighs vdW grids
+// (src/FillLigandGrid.cpp:43), the charge (elec grid, :97), and the atom's vdW slot.
+struct AtomParam {
+  float w_vdw;
+  float charge;
+  int slot;
+  int pad;
+};
+
+// Per-rotation record written by the prep kernel.
+struct RotRec {
+  float mn[3];      // min corner of the rotated ligand (GetMinCoors)
+  int W[3];         // translation window per axis: n - int(len/h) - 2
+  int ext[3];       // cells touched by the spread per axis (max cell index + 2)
+  int valid;        // 1 when every window is non-empty
+  int err;          // nonzero when the ligand box exceeded the planned box
+  int nA;           // atoms
+  short xlo[KMAX];  // per channel: first and last x plane touched (xlo > xhi: empty)
+  short xhi[KMAX];
+};
+
+// Everything one wave of rotations needs on the device.
+struct WaveArgs {
+  int n;             // grid edge (cubic)
+  int K;             // channels (vdW grids + elec)
+  int Lb;            // planned ligand box edge (x planes stored per channel)
+  float spacing;
+  int nrot;          // rotations in this wave
+  int max_atoms;     // stride of rotated-atom storage
+  const float* coords;       // [atoms][3]
+  const AtomParam* params;   // [atom params]
+  const ConfDesc* confs;
+  const RotDesc* rots;       // [nrot]
+  float4* rot_xyz;           // [nrot][max_atoms]
+  RotRec* rec;               // [nrot]
+  float2* A;                 // [nrot][K][Lb][ncol]
+  float2* B;                 // [nrot][n][ncol]
+  unsigned long long* keys;  // [nrot]
+  const float2* phat;        // [n][K][ncol] (kx position-major)
+  const float2* tw;          // [n]
+  float* minE;               // output base (indexed by RotDesc.out)
+  int* idx;
+  int* err_count;
+  int col_tile;
+};
+
+// Launchers (stream-ordered, no synchronisation). Return cudaError_t of the launch.
+cudaError_t launch_prep(const WaveArgs& a, cudaStream_t s);
+cudaError_t launch_spread_yz(const WaveArgs& a, cudaStream_t s);
+cudaError_t launch_xpass(const WaveArgs& a, cudaStream_t s);
+cudaError_t launch_yz_inv_argmin(const WaveArgs& a, cudaStream_t s);
+cudaError_t launch_finalize(const WaveArgs& a, cudaStream_t s);
+// Dense forward transform of K receptor grids [K][n][n][n] -> phat [n][K][ncol].
+cudaError_t launch_receptor_fft(int n, int K, const float* grids, float2* scratch,
+                                float2* phat, const float2* tw, int col_tile, cudaStream_t s);
+// Shared memory per CTA of the x pass for given n, K, column tile.
+size_t xpass_smem_bytes(int n, int K, int col_tile);
+int pick_col_tile(int n, int K);
+// Dense FillLigandGrid on the GPU.
+cudaError_t launch_fill_dense(int nQ, int nAtom, const float* coors, const float* mincoors,
+                              const AtomParam* params, int nVdwUsed, int X, int Y, int Z,
+                              float spacing, float* out, cudaStream_t s);
+cudaError_t launch_conj_mult(const float2* pot, float2* lig, int odist, int K, int Q,
+                             cudaStream_t s);
+cudaError_t launch_sum_grids(const float2* lig, float2* sum, int K, int odist, int idist,
+                             int Q, cudaStream_t s);
+// FP64 direct re-score of poses.
+cudaError_t launch_rescore_fp64(int n, int K, float spacing, const float* grids,
+                                const float* coords, const AtomParam* params,
+                                const ConfDesc* confs, const RotDesc* rots, const int* tidx,
+                                int npose, double* energy, cudaStream_t s);
+
+// Number of kernel launches one wave issues.
+constexpr int kLaunchesPerWave = 5;
+
+void set_error(const std::string& msg);
+
+}  // namespace cdk

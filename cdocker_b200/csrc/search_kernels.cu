@@ -1,0 +1,558 @@
+// search_kernels.cu -- the FP32 FFT translational-rotational search on sm_100a.
+//
+// One wave of rotations runs five kernels, all on one stream:
+//   prep          rotate atoms (reference op order, no contraction), bounding box, windows,
+//                 per-channel x-plane ranges          (src/Rotate.cpp, GetMin/MaxCoors.cpp)
+//   spread_yz     per (rotation, channel, x plane): spread the atoms that touch the plane
+//                 into shared memory (trilinear weights in FillLigandGrid's arithmetic), then
+//                 the 2-D real-to-complex FFT over (y,z) -> A      (src/FillLigandGrid.cpp)
+//   xpass         per spectral column tile: FFT along x of every channel, the conjugate
+//                 product with the resident receptor spectra summed over channels, and the
+//                 inverse FFT along x, keeping only the translation window -> B
+//                                                       (src/kernel.cu ConjMult + SumGrids)
+//   yz_inv_argmin per (rotation, x in window): inverse FFT over y, complex-to-real over z,
+//                 min / first argmin over the window, folded into one 64-bit key per rotation
+//                                         (src/TranRotaConfSearchNoMini.cu:429-464)
+//   finalize      keys -> minE, (i,j,k)
+// The energy grid never leaves shared memory. Spectra stay in the digit-reversed order the
+// in-place FFT stages produce; the receptor spectra are computed by the same stages, so
+// the pointwise product lines up without any permutation.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "cdk_internal.h"
+#include "fft.cuh"
+
+namespace cdk {
+
+namespace {
+
+// ---------------------------------------------------------------------------------------
+// exact-order float rotation (src/QuaternionMultiply.cpp:3-11, src/Rotate.cpp:4-27)
+__device__ __forceinline__ void qmul_rn(const float* l, const float* r, float* o) {
+  o[0] = __fsub_rn(__fsub_rn(__fsub_rn(__fmul_rn(l[0], r[0]), __fmul_rn(l[1], r[1])),
+                             __fmul_rn(l[2], r[2])),
+                   __fmul_rn(l[3], r[3]));
+  o[1] = __fsub_rn(__fadd_rn(__fadd_rn(__fmul_rn(l[0], r[1]), __fmul_rn(l[1], r[0])),
+                             __fmul_rn(l[2], r[3])),
+                   __fmul_rn(l[3], r[2]));
+  o[2] = __fadd_rn(__fadd_rn(__fsub_rn(__fmul_rn(l[0], r[2]), __fmul_rn(l[1], r[3])),
+                             __fmul_rn(l[2], r[0])),
+                   __fmul_rn(l[3], r[1]));
+  o[3] = __fadd_rn(__fsub_rn(__fadd_rn(__fmul_rn(l[0], r[3]), __fmul_rn(l[1], r[2])),
+                             __fmul_rn(l[2], r[1])),
+                   __fmul_rn(l[3], r[0]));
+}
+
+__device__ __forceinline__ void rotate_rn(const float* q, float vx, float vy, float vz,
+                                          float* out) {
+  float qc[4] = {q[0], -q[1], -q[2], -q[3]};
+  float qv[4] = {0.0f, vx, vy, vz};
+  float t1[4], t2[4];
+  qmul_rn(q, qv, t1);
+  qmul_rn(t1, qc, t2);
+  out[0] = t2[1];
+  out[1] = t2[2];
+  out[2] = t2[3];
+}
+
+// cell index of a coordinate, FillLigandGrid's double arithmetic (src/FillLigandGrid.cpp:28-30)
+__device__ __forceinline__ int cell_of(float x, float mn, float h) {
+  return (int)__ddiv_rn(__dsub_rn((double)x, (double)mn), (double)h);
+}
+// ratio within the cell (src/FillLigandGrid.cpp:33-35): `index * spacing` is a float product
+__device__ __forceinline__ double ratio_of(float x, float mn, float h, int i) {
+  return __ddiv_rn(__dsub_rn(__dsub_rn((double)x, (double)mn), (double)__fmul_rn((float)i, h)),
+                   (double)h);
+}
+
+__device__ __forceinline__ unsigned int order_key(float f) {
+  unsigned int u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key_to_float(unsigned int k) {
+  unsigned int u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+  return __uint_as_float(u);
+}
+
+// ---------------------------------------------------------------------------------------
+// prep: one warp per rotation
+__global__ void __launch_bounds__(128) k_prep(WaveArgs a) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = blockIdx.x * 4 + warp;
+  __shared__ int s_lo[4][KMAX], s_hi[4][KMAX], s_ext[4][3];
+  if (lane < KMAX) {
+    s_lo[warp][lane] = 0x7fff;
+    s_hi[warp][lane] = -1;
+  }
+  if (lane < 3) s_ext[warp][lane] = 0;
+  __syncwarp();
+  if (r >= a.nrot) return;
+  const RotDesc rd = a.rots[r];
+  const ConfDesc cd = a.confs[rd.conf];
+  const int nA = min(cd.n_atoms, a.max_atoms);
+  const float* xyz = a.coords + (size_t)cd.coord_off * 3;
+  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int i = lane; i < nA; i += 32) {
+    float p[3];
+    rotate_rn(rd.q, xyz[i * 3 + 0], xyz[i * 3 + 1], xyz[i * 3 + 2], p);
+    a.rot_xyz[(size_t)r * a.max_atoms + i] = make_float4(p[0], p[1], p[2], 0.0f);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      mn[d] = fminf(mn[d], p[d]);
+      mx[d] = fmaxf(mx[d], p[d]);
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[d] = fminf(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+      mx[d] = fmaxf(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+    }
+  const float h = a.spacing;
+  int W[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) W[d] = a.n - (int)__fdiv_rn(__fsub_rn(mx[d], mn[d]), h) - 2;
+  const bool valid = nA > 0 && W[0] > 0 && W[1] > 0 && W[2] > 0;
+  __syncwarp();
+  // per-channel x range and touched extents
+  const AtomParam* prm = a.params + cd.param_off;
+  const int elec = a.K - 1;
+  for (int i = lane; i < nA; i += 32) {
+    float4 p = a.rot_xyz[(size_t)r * a.max_atoms + i];
+    int ci[3] = {cell_of(p.x, mn[0], h), cell_of(p.y, mn[1], h), cell_of(p.z, mn[2], h)};
+    const int sl = prm[i].slot;
+    if (sl >= 0 && sl < elec) {
+      atomicMin(&s_lo[warp][sl], ci[0]);
+      atomicMax(&s_hi[warp][sl], ci[0] + 1);
+    }
+    atomicMin(&s_lo[warp][elec], ci[0]);
+    atomicMax(&s_hi[warp][elec], ci[0] + 1);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) atomicMax(&s_ext[warp][d], ci[d] + 2);
+  }
+  __syncwarp();
+  RotRec* rec = a.rec + r;
+  if (lane < KMAX) {
+    const bool used = lane < a.K && s_hi[warp][lane] >= 0;
+    rec->xlo[lane] = used ? (short)s_lo[warp][lane] : (short)1;
+    rec->xhi[lane] = used ? (short)s_hi[warp][lane] : (short)0;
+  }
+  if (lane == 0) {
+    int err = 0;
+    // the x planes of every channel must fit the planned box, y/z cells the grid
+    if (valid && (s_ext[warp][0] - 1 >= a.Lb || s_ext[warp][1] > a.n || s_ext[warp][2] > a.n))
+      err = 1;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      rec->mn[d] = mn[d];
+      rec->W[d] = W[d];
+      rec->ext[d] = s_ext[warp][d];
+    }
+    rec->valid = (valid && !err) ? 1 : 0;
+    rec->err = err;
+    rec->nA = nA;
+    a.keys[r] = ~0ull;
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// shared helpers for the (y,z) plane transforms
+//   P: packed real rows, pair p holds rows 2p (real part) and 2p+1 (imag part), stride n+1
+//   O: half spectrum over z, [y][kz] with stride nzh (row y, col kz)
+
+// z: R2C of `npairs` packed row pairs in P, then split into O rows (2p, 2p+1)
+template <int N>
+__device__ __forceinline__ void plane_forward(float2* P, float2* O, int npairs,
+                                              const float2* tw) {
+  constexpr int NZH = N / 2 + 1;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  fft_lines<N, false>(P, npairs, N + 1, 1, tw, tid, nthr);
+  for (int i = tid; i < (N / 2) * NZH; i += nthr) {
+    const int p = i / NZH, kz = i - p * NZH;
+    float2 A = make_float2(0.f, 0.f), Bv = make_float2(0.f, 0.f);
+    if (p < npairs) {
+      const float2 zk = P[p * (N + 1) + fft_pos<N>(kz)];
+      const float2 zn = P[p * (N + 1) + fft_pos<N>((N - kz) % N)];
+      A = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+      Bv = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+    }
+    O[(2 * p) * NZH + kz] = A;
+    O[(2 * p + 1) * NZH + kz] = Bv;
+  }
+  __syncthreads();
+  // y: complex FFT on the nzh columns
+  fft_lines<N, false>(O, NZH, 1, NZH, tw, tid, nthr);
+}
+
+// ---------------------------------------------------------------------------------------
+// spread + forward (y,z) transform of one (rotation, channel, x plane)
+template <int N>
+__global__ void __launch_bounds__(256) k_spread_yz(WaveArgs a) {
+  constexpr int NZH = N / 2 + 1;
+  constexpr int NCOL = N * NZH;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tw = reinterpret_cast<float2*>(smem_raw);
+  float2* O = tw + N;
+  float2* P = O + N * NZH;
+  const int x = blockIdx.x, k = blockIdx.y, r = blockIdx.z;
+  const RotRec* rec = a.rec + r;
+  if (!rec->valid) return;
+  const int xlo = rec->xlo[k], xhi = rec->xhi[k];
+  if (x < xlo || x > xhi) return;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  for (int i = tid; i < N; i += nthr) tw[i] = a.tw[i];
+  const int npairs = min(N / 2, (rec->ext[1] + 1) / 2);
+  float* Pf = reinterpret_cast<float*>(P);
+  for (int i = tid; i < npairs * (N + 1); i += nthr) P[i] = make_float2(0.f, 0.f);
+  __syncthreads();
+  // spread the atoms touching plane x (src/FillLigandGrid.cpp:24-66 vdW, :75-118 elec)
+  const RotDesc rd = a.rots[r];
+  const ConfDesc cd = a.confs[rd.conf];
+  const AtomParam* prm = a.params + cd.param_off;
+  const float mn0 = rec->mn[0], mn1 = rec->mn[1], mn2 = rec->mn[2];
+  const float h = a.spacing;
+  const bool elec = (k == a.K - 1);
+  const int nA = rec->nA;
+  for (int i = tid; i < nA; i += nthr) {
+    const AtomParam ap = prm[i];
+    if (!elec && ap.slot != k) continue;
+    const float4 p = a.rot_xyz[(size_t)r * a.max_atoms + i];
+    const int xi = cell_of(p.x, mn0, h);
+    double wx;
+    if (xi == x) wx = 1.0 - ratio_of(p.x, mn0, h, xi);
+    else if (xi + 1 == x) wx = ratio_of(p.x, mn0, h, xi);
+    else continue;
+    const int yi = cell_of(p.y, mn1, h), zi = cell_of(p.z, mn2, h);
+    const double yr = ratio_of(p.y, mn1, h, yi), zr = ratio_of(p.z, mn2, h, zi);
+    const double s = elec ? (double)ap.charge : (double)ap.w_vdw;
+    const double sx = s * wx;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int dy = c >> 1, dz = c & 1;
+      const double w = sx * (dy ? yr : 1.0 - yr) * (dz ? zr : 1.0 - zr);
+      const int y = yi + dy, z = zi + dz;
+      if (y < N && z < N) atomicAdd(&Pf[((y >> 1) * (N + 1) + z) * 2 + (y & 1)], (float)w);
+    }
+  }
+  __syncthreads();
+  plane_forward<N>(P, O, npairs, tw);
+  // write the plane's half spectrum (16-byte stores)
+  float4* dst = reinterpret_cast<float4*>(a.A + (((size_t)r * a.K + k) * a.Lb + x) * NCOL);
+  const float4* src = reinterpret_cast<const float4*>(O);
+  for (int i = tid; i < NCOL / 2; i += nthr) dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------------------------------
+// x pass: forward along x, conj-multiply-sum with the receptor spectra, inverse along x.
+// CTA = one tile of `ct` spectral columns x a contiguous chunk of rotations.
+template <int N>
+__global__ void __launch_bounds__(256) k_xpass(WaveArgs a, int rot_per_cta) {
+  constexpr int NZH = N / 2 + 1;
+  constexpr int NCOL = N * NZH;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tw = reinterpret_cast<float2*>(smem_raw);
+  int* s_ch = reinterpret_cast<int*>(tw + N);
+  float2* Wb = reinterpret_cast<float2*>(s_ch + 2 * KMAX);
+  const int ct = a.col_tile;
+  const int c0 = blockIdx.x * ct;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  for (int i = tid; i < N; i += nthr) tw[i] = a.tw[i];
+  const int r_begin = blockIdx.y * rot_per_cta;
+  const int r_end = min(a.nrot, r_begin + rot_per_cta);
+  const int K = a.K;
+  for (int r = r_begin; r < r_end; ++r) {
+    const RotRec* rec = a.rec + r;
+    if (!rec->valid) continue;
+    __syncthreads();  // previous rotation done with s_ch / Wb
+    if (tid == 0) {
+      int nk = 0;
+      for (int k = 0; k < K; ++k)
+        if (rec->xlo[k] <= rec->xhi[k]) s_ch[nk++] = k;
+      s_ch[KMAX] = nk;
+    }
+    __syncthreads();
+    const int nk = s_ch[KMAX];
+    const int nl = nk * ct;  // lines
+    // load A (zero outside each channel's x range)
+    for (int i = tid; i < N * nl; i += nthr) {
+      const int c = i % ct;
+      const int t = i / ct;
+      const int kk = t % nk;
+      const int x = t / nk;
+      const int k = s_ch[kk];
+      float2 v = make_float2(0.f, 0.f);
+      if (x >= rec->xlo[k] && x <= rec->xhi[k] && c0 + c < NCOL)
+        v = a.A[(((size_t)r * K + k) * a.Lb + x) * NCOL + c0 + c];
+      Wb[i] = v;
+    }
+    __syncthreads();
+    fft_lines<N, false>(Wb, nl, 1, nl, tw, tid, nthr);
+    // S = sum_k conj(L_k) * P_k, into the kk = 0 lines
+    for (int i = tid; i < N * ct; i += nthr) {
+      const int c = i % ct;
+      const int xp = i / ct;
+      float2 s = make_float2(0.f, 0.f);
+      if (c0 + c < NCOL) {
+        for (int kk = 0; kk < nk; ++kk) {
+          const float2 l = Wb[xp * nl + kk * ct + c];
+          const float2 p = a.phat[((size_t)xp * K + s_ch[kk]) * NCOL + c0 + c];
+          const float2 t = c_conjmul(l, p);
+          s.x += t.x;
+          s.y += t.y;
+        }
+      }
+      Wb[xp * nl + c] = s;
+    }
+    __syncthreads();
+    fft_lines<N, true>(Wb, ct, 1, nl, tw, tid, nthr);
+    const int Wx = rec->W[0];
+    for (int i = tid; i < Wx * ct; i += nthr) {
+      const int c = i % ct;
+      const int x = i / ct;
+      if (c0 + c < NCOL) a.B[((size_t)r * N + x) * NCOL + c0 + c] = Wb[x * nl + c];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// inverse (y,z) of one (rotation, x in window) plane + min / first argmin
+template <int N>
+__global__ void __launch_bounds__(256) k_yz_inv_argmin(WaveArgs a) {
+  constexpr int NZH = N / 2 + 1;
+  constexpr int NCOL = N * NZH;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tw = reinterpret_cast<float2*>(smem_raw);
+  float2* O = tw + N;
+  float2* P = O + N * NZH;
+  __shared__ unsigned long long s_best[8];
+  const int x = blockIdx.x, r = blockIdx.y;
+  const RotRec* rec = a.rec + r;
+  if (!rec->valid) return;
+  const int Wx = rec->W[0], Wy = rec->W[1], Wz = rec->W[2];
+  if (x >= Wx) return;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  for (int i = tid; i < N; i += nthr) tw[i] = a.tw[i];
+  const float4* src = reinterpret_cast<const float4*>(a.B + ((size_t)r * N + x) * NCOL);
+  float4* dst = reinterpret_cast<float4*>(O);
+  for (int i = tid; i < NCOL / 2; i += nthr) dst[i] = src[i];
+  __syncthreads();
+  fft_lines<N, true>(O, NZH, 1, NZH, tw, tid, nthr);  // y: positions -> natural rows
+  const int npairs = (Wy + 1) / 2;
+  // pack rows (2p, 2p+1) as one complex line with Hermitian extension over z
+  for (int i = tid; i < npairs * N; i += nthr) {
+    const int p = i / N, k = i - p * N;
+    const float2* A = O + (2 * p) * NZH;
+    const float2* Bv = O + (2 * p + 1) * NZH;
+    float2 z;
+    if (k == 0 || k == N / 2) {
+      z = make_float2(A[k].x, Bv[k].x);
+    } else if (k < N / 2) {
+      z = make_float2(A[k].x - Bv[k].y, A[k].y + Bv[k].x);
+    } else {
+      const int m = N - k;
+      z = make_float2(A[m].x + Bv[m].y, -A[m].y + Bv[m].x);
+    }
+    P[p * (N + 1) + fft_pos<N>(k)] = z;
+  }
+  __syncthreads();
+  fft_lines<N, true>(P, npairs, N + 1, 1, tw, tid, nthr);
+  const float inv = 1.0f / (float)((double)N * N * N);
+  unsigned long long best = ~0ull;
+  for (int i = tid; i < Wy * Wz; i += nthr) {
+    const int y = i / Wz, z = i - y * Wz;
+    const float2 v = P[(y >> 1) * (N + 1) + z];
+    const float e = ((y & 1) ? v.y : v.x) * inv;
+    const unsigned int lin = (unsigned int)((x * N + y) * N + z);
+    const unsigned long long key = ((unsigned long long)order_key(e) << 32) | lin;
+    best = key < best ? key : best;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
+    best = other < best ? other : best;
+  }
+  if ((tid & 31) == 0) s_best[tid >> 5] = best;
+  __syncthreads();
+  if (tid == 0) {
+    for (int w = 1; w < (nthr >> 5); ++w) best = s_best[w] < best ? s_best[w] : best;
+    best = s_best[0] < best ? s_best[0] : best;
+    atomicMin(a.keys + r, best);
+  }
+}
+
+__global__ void k_finalize(WaveArgs a) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= a.nrot) return;
+  const int out = a.rots[r].out;
+  const RotRec* rec = a.rec + r;
+  if (rec->err) atomicAdd(a.err_count, 1);
+  const unsigned long long key = a.keys[r];
+  if (!rec->valid || key == ~0ull) {
+    a.minE[out] = INFINITY;
+    a.idx[out * 3 + 0] = a.idx[out * 3 + 1] = a.idx[out * 3 + 2] = -1;
+    return;
+  }
+  const unsigned int lin = (unsigned int)(key & 0xffffffffu);
+  const int n = a.n;
+  a.minE[out] = key_to_float((unsigned int)(key >> 32));
+  a.idx[out * 3 + 0] = lin / (n * n);
+  a.idx[out * 3 + 1] = (lin / n) % n;
+  a.idx[out * 3 + 2] = lin % n;
+}
+
+// ---------------------------------------------------------------------------------------
+// receptor spectra: dense (y,z) forward of every plane, then x forward per column tile
+template <int N>
+__global__ void __launch_bounds__(256) k_receptor_yz(const float* grids, float2* out,
+                                                      const float2* twg) {
+  constexpr int NZH = N / 2 + 1;
+  constexpr int NCOL = N * NZH;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tw = reinterpret_cast<float2*>(smem_raw);
+  float2* O = tw + N;
+  float2* P = O + N * NZH;
+  const int x = blockIdx.x, k = blockIdx.y;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  for (int i = tid; i < N; i += nthr) tw[i] = twg[i];
+  const float* g = grids + ((size_t)k * N + x) * N * N;
+  for (int i = tid; i < N * N; i += nthr) {
+    const int y = i / N, z = i - y * N;
+    reinterpret_cast<float*>(P)[((y >> 1) * (N + 1) + z) * 2 + (y & 1)] = g[i];
+  }
+  __syncthreads();
+  plane_forward<N>(P, O, N / 2, tw);
+  float2* dst = out + ((size_t)k * N + x) * NCOL;
+  for (int i = tid; i < NCOL; i += nthr) dst[i] = O[i];
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_receptor_x(const float2* in, float2* phat, int K,
+                                                     int ct, const float2* twg) {
+  constexpr int NZH = N / 2 + 1;
+  constexpr int NCOL = N * NZH;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tw = reinterpret_cast<float2*>(smem_raw);
+  float2* Wb = tw + N;
+  const int c0 = blockIdx.x * ct;
+  const int k = blockIdx.y;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  for (int i = tid; i < N; i += nthr) tw[i] = twg[i];
+  for (int i = tid; i < N * ct; i += nthr) {
+    const int c = i % ct, x = i / ct;
+    Wb[i] = (c0 + c < NCOL) ? in[((size_t)k * N + x) * NCOL + c0 + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  fft_lines<N, false>(Wb, ct, 1, ct, tw, tid, nthr);
+  for (int i = tid; i < N * ct; i += nthr) {
+    const int c = i % ct, xp = i / ct;
+    if (c0 + c < NCOL) phat[((size_t)xp * K + k) * NCOL + c0 + c] = Wb[i];
+  }
+}
+
+template <int N>
+constexpr size_t plane_smem() {
+  return sizeof(float2) * (N + N * (N / 2 + 1) + (N / 2) * (N + 1));
+}
+
+template <int N>
+cudaError_t launch_spread_yz_t(const WaveArgs& a, cudaStream_t s) {
+  const size_t sm = plane_smem<N>();
+  cudaError_t e = cudaFuncSetAttribute(k_spread_yz<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  dim3 grid(a.Lb, a.K, a.nrot);
+  k_spread_yz<N><<<grid, 256, sm, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t launch_yz_inv_t(const WaveArgs& a, cudaStream_t s) {
+  const size_t sm = plane_smem<N>();
+  cudaError_t e = cudaFuncSetAttribute(k_yz_inv_argmin<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  dim3 grid(N, a.nrot);
+  k_yz_inv_argmin<N><<<grid, 256, sm, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t launch_xpass_t(const WaveArgs& a, cudaStream_t s) {
+  const size_t sm = xpass_smem_bytes(N, a.K, a.col_tile);
+  cudaError_t e = cudaFuncSetAttribute(k_xpass<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  constexpr int NCOL = N * (N / 2 + 1);
+  const int tiles = (NCOL + a.col_tile - 1) / a.col_tile;
+  // enough CTAs to fill the machine a few times over; each walks a chunk of rotations
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int chunks = (sms * 8 + tiles - 1) / tiles;
+  if (chunks > a.nrot) chunks = a.nrot;
+  if (chunks < 1) chunks = 1;
+  const int per = (a.nrot + chunks - 1) / chunks;
+  chunks = (a.nrot + per - 1) / per;
+  dim3 grid(tiles, chunks);
+  k_xpass<N><<<grid, 256, sm, s>>>(a, per);
+  return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t launch_receptor_t(int K, const float* grids, float2* scratch, float2* phat,
+                              const float2* tw, int ct, cudaStream_t s) {
+  const size_t sm = plane_smem<N>();
+  cudaError_t e = cudaFuncSetAttribute(k_receptor_yz<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  k_receptor_yz<N><<<dim3(N, K), 256, sm, s>>>(grids, scratch, tw);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  constexpr int NCOL = N * (N / 2 + 1);
+  const size_t sm2 = sizeof(float2) * (N + (size_t)N * ct);
+  e = cudaFuncSetAttribute(k_receptor_x<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+  if (e != cudaSuccess) return e;
+  k_receptor_x<N><<<dim3((NCOL + ct - 1) / ct, K), 256, sm2, s>>>(scratch, phat, K, ct, tw);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t xpass_smem_bytes(int n, int K, int col_tile) {
+  return sizeof(float2) * n + sizeof(int) * 2 * KMAX + sizeof(float2) * (size_t)n * K * col_tile;
+}
+
+int pick_col_tile(int n, int K) {
+  // largest tile (<= 16 columns) whose work buffer stays within 100 KB of shared memory
+  int ct = 16;
+  while (ct > 2 && xpass_smem_bytes(n, K, ct) > 100 * 1024) ct >>= 1;
+  return ct;
+}
+
+#define CDK_DISPATCH_N(n, fn, ...)                 \
+  switch (n) {                                     \
+    case 32: return fn<32>(__VA_ARGS__);           \
+    case 64: return fn<64>(__VA_ARGS__);           \
+    case 96: return fn<96>(__VA_ARGS__);           \
+    case 128: return fn<128>(__VA_ARGS__);         \
+    default: return cudaErrorInvalidValue;         \
+  }
+
+cudaError_t launch_prep(const WaveArgs& a, cudaStream_t s) {
+  k_prep<<<(a.nrot + 3) / 4, 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t launch_spread_yz(const WaveArgs& a, cudaStream_t s) {
+  CDK_DISPATCH_N(a.n, launch_spread_yz_t, a, s);
+}
+cudaError_t launch_xpass(const WaveArgs& a, cudaStream_t s) {
+  CDK_DISPATCH_N(a.n, launch_xpass_t, a, s);
+}
+cudaError_t launch_yz_inv_argmin(const WaveArgs& a, cudaStream_t s) {
+  CDK_DISPATCH_N(a.n, launch_yz_inv_t, a, s);
+}
+cudaError_t launch_finalize(const WaveArgs& a, cudaStream_t s) {
+  k_finalize<<<(a.nrot + 255) / 256, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t launch_receptor_fft(int n, int K, const float* grids, float2* scratch,
+                                float2* phat, const float2* tw, int ct, cudaStream_t s) {
+  CDK_DISPATCH_N(n, launch_receptor_t, K, grids, scratch, phat, tw, ct, s);
+}
+
+}  // namespace cdk

@@ -1,0 +1,161 @@
+/* cdock_b200.h -- C-ABI of the B200 FFT translational-rotational search.
+ *
+ * The reference (CDOCKER) has no library boundary for this path: the search runs inline in
+ * each driver's main() (src/TranRotaConfSearchNoMini.cu:156-464, and the same block in
+ * src/TranRotaSearch.cu:111-350), and its only declared GPU interface is include/kernel.h
+ * (ConjMult, SumGrids). The entry points below are that path cut at its natural seams, with
+ * plain pointers and sizes; each comment names the reference code it replaces.
+ *
+ * Conventions
+ *  - Every function returns an int status (CDK_OK = 0) and never exits the process;
+ *    cdk_last_error() returns the message of the last failure on the calling thread.
+ *  - Grids are float [K][nx][ny][nz], z fastest, the reference's usedGridValues layout
+ *    (src/TranRotaConfSearchNoMini.cu:135-146): K-1 vdW grids, then the electrostatic grid.
+ *  - Atom slots are the position of each atom's vdW grid among the K-1 used vdW grids, as
+ *    produced by GetIdxOfAtomsForVdwRadius (src/GetIdxOfAtomsForVdwRadius.cpp:4-35).
+ *  - A context owns all device memory it uses. Contexts are independent; one context must not
+ *    be driven from two host threads at once.
+ *  - stream arguments are cudaStream_t passed as void* (NULL = the context's own stream).
+ */
+#ifndef CDOCK_B200_H
+#define CDOCK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CDK_OK 0
+#define CDK_ERR_INVALID 1     /* bad argument */
+#define CDK_ERR_CUDA 2        /* a CUDA call failed */
+#define CDK_ERR_NOMEM 3       /* device allocation failed */
+#define CDK_ERR_UNSUPPORTED 4 /* grid size / K outside what the kernels are built for */
+#define CDK_ERR_OVERFLOW 5    /* a rotation's ligand box exceeded the planned box */
+#define CDK_ERR_IO 6          /* file could not be read or parsed */
+#define CDK_ERR_BUSY 7        /* serving queue full / admission refused */
+
+#define CDK_FORM_FP32 0   /* FP32 radix FFT passes (the plain form) */
+#define CDK_FORM_BF16X3 1 /* split-BF16 (hi*hi + hi*lo + lo*hi) DFT contractions, FP32 acc. */
+
+typedef struct cdk_ctx cdk_ctx;
+
+typedef struct cdk_opts {
+  int device;          /* CUDA device ordinal */
+  int form;            /* CDK_FORM_* */
+  int wave_rotations;  /* rotations per launch wave; 0 = pick automatically */
+  int max_atoms;       /* largest ligand (atoms) this context will see; 0 = 256 */
+  int col_tile;        /* spectral columns per CTA in the x pass; 0 = autotuned default */
+  int use_graphs;      /* 1 = replay each wave through a captured CUDA graph */
+  int reserved[8];
+} cdk_opts;
+
+/* Library version string. */
+const char* cdk_version(void);
+
+/* Message of the last failure on this thread (empty if none). Returns the message length. */
+int cdk_last_error(char* buf, size_t cap);
+
+/* Fills *opts with defaults. */
+void cdk_opts_default(cdk_opts* opts);
+
+/* Upload the K receptor grids and transform them once; the K spectra stay resident.
+ * Replaces src/TranRotaConfSearchNoMini.cu:156-199 (cufftPlanMany R2C + H2D + ExecR2C).
+ * nx == ny == nz in {32, 64, 96, 128}; 2 <= K <= 16. grids: host pointer. */
+int cdk_ctx_create(int nx, int ny, int nz, float spacing, int K, const float* grids,
+                   const cdk_opts* opts, cdk_ctx** out);
+int cdk_ctx_destroy(cdk_ctx* ctx);
+
+/* Whole search over nConf conformers x nQ rotations, host buffers in and out.
+ * Replaces src/TranRotaConfSearchNoMini.cu:352-464 (rotate, bounding box, FillLigandGrid,
+ * H2D, R2C, ConjMult, SumGrids, C2R, D2H, host min/argmin). Rotation i of conformer c is
+ * quats[(c*nQ + i)*4 .. +4]; results minE[c*nQ+i] and idx[(c*nQ+i)*3 .. +3] follow the
+ * reference: minimum over the window [0, n - int(len/h) - 2) per axis of the correlation
+ * energy, first minimum in x-major order; +inf and -1 for an empty window.
+ * coor: [nConf][nAtom][3]; charge, eps: [nAtom]; slot: [nAtom] in 0..K-2. */
+int cdk_search(cdk_ctx* ctx, int nAtom, int nConf, const float* coor, const float* charge,
+               const float* eps, const int* slot, int nQ, const float* quats, float* minE,
+               int* idx, void* stream);
+
+/* Same search with every buffer already in device memory (d_ prefix = device pointer);
+ * no host<->device copies and no synchronisation beyond stream order. */
+int cdk_search_device(cdk_ctx* ctx, int nAtom, int nConf, const float* d_coor,
+                      const float* d_charge, const float* d_eps, const int* d_slot, int nQ,
+                      const float* d_quats, float* d_minE, int* d_idx, void* stream);
+
+/* FP64 direct re-score of given poses (rotation + translation index) against the resident
+ * receptor grids: E = sum_k sum_atoms sum_corners w * P_k(g + t), accumulated in double.
+ * Host buffers. rot_conf[i] picks the conformer, quats[i*4..], tidx[i*3..] the translation. */
+int cdk_rescore_fp64(cdk_ctx* ctx, int nAtom, int nConf, const float* coor,
+                     const float* charge, const float* eps, const int* slot, int nPose,
+                     const int* rot_conf, const float* quats, const int* tidx, double* energy,
+                     void* stream);
+
+/* Dense ligand-grid fill on the GPU with FillLigandGrid's semantics
+ * (src/FillLigandGrid.cpp:7-120): rotated coords [nQ][nAtom][3] and their min corners
+ * [nQ][3] in, out[nQ][nVdwUsed+1][x][y][z] (host, overwritten; the reference wants it
+ * pre-zeroed, this call zeroes it). */
+int cdk_fill_ligand_grid(int nQ, int nAtom, const float* coors, const float* mincoors,
+                         const float* charge, const float* eps, const int* slot, int nVdwUsed,
+                         int x, int y, int z, float spacing, float* out);
+
+/* kernel.h-compatible spectral kernels on device pointers (include/kernel.h:9-11), with
+ * bounds checks. d_potential_F: [K][odist] complex; d_ligand_F: [Q][K][odist] complex.
+ * cdk_conj_mult: d_ligand_F[q,k,f] <- conj(d_ligand_F[q,k,f]) * d_potential_F[k,f]
+ *   (src/kernel.cu:5-14).
+ * cdk_sum_grids: d_sum_F[q,f] = sum_k d_ligand_F[q,k,f] / sqrtf(idist) (src/kernel.cu:16-30). */
+int cdk_conj_mult(const void* d_potential_F, void* d_ligand_F, int odist, int K, int Q,
+                  void* stream);
+int cdk_sum_grids(const void* d_ligand_F, void* d_sum_F, int K, int odist, int idist, int Q,
+                  void* stream);
+
+/* Host helpers with the reference's semantics (bit-exact). */
+
+/* nConf x nQ Shoemake quaternions from one std::mt19937_64 seeded with `seed`, drawn in turn
+ * (src/QuaternionUniformSampling.cpp:5-24; the driver's shared generator, :203-204, :323). */
+int cdk_quaternion_uniform_sampling(uint64_t seed, int nConf, int nQ, float* out);
+
+/* FilterQuaternions (src/FilterQuaternions.cpp:11-83): keeps rotations whose rotated box is
+ * shorter than the grid lengths; if more than maxN pass, std::random_shuffle (driven by the
+ * process-wide rand()) and keep the first maxN. out: nQ*4 capacity; returns the count via
+ * *count. */
+int cdk_filter_quaternions(const float* coor, int nAtom, int nQ, const float* quats,
+                           float gridLenX, float gridLenY, float gridLenZ, int maxN,
+                           float* out, int* count);
+
+/* GetIdxOfAtomsForVdwRadius (src/GetIdxOfAtomsForVdwRadius.cpp:4-35) + the driver's grid
+ * compaction (src/TranRotaConfSearchNoMini.cu:126-146): per-atom slot among the used vdW
+ * grids, the used grid indices (ascending), and their count via *nUsed. */
+int cdk_vdw_slots(int nAtom, const float* radii, int nVdw, const float* gridRadii,
+                  int* usedIdx, int* atomSlot, int* nUsed);
+
+/* ReadGrids (src/ReadGrids.cpp:6-68): header ints [numGrids, x, y, z], floats
+ * [midx, midy, midz, xlen, ylen, zlen, spacing, restraint_k]; radii (numGrids-1) and values
+ * (numGrids*x*y*z) are written when the capacities suffice. Pass NULL buffers to size first. */
+int cdk_read_grids(const char* path, int* hdr_i, float* hdr_f, float* radii, long radii_cap,
+                   float* values, long values_cap);
+
+/* Writes grids in the same text format (3 title lines, header, radii, per grid a header line
+ * and x y z value lines, z fastest). */
+int cdk_write_grids(const char* path, int numGrids, int x, int y, int z, const float* mid,
+                    const float* len, float spacing, float restraint_k, const float* radii,
+                    const float* values);
+
+/* Seeded synthetic receptor potential grids: nVdw soft-core capped LJ grids at the given probe
+ * radii and one distance-dependent-dielectric Coulomb grid (eps(r) = 4r, capped at +-elecCap),
+ * from receptor atoms xyz[nAtom][3], radius, sqrt-epsilon and charge. Grid point (i,j,k) is
+ * origin + (i,j,k)*spacing. out: [nVdw+1][n][n][n]. Host, multithreaded. */
+int cdk_synth_receptor_grids(int n, float spacing, const float* origin, int nAtom,
+                             const float* xyz, const float* radius, const float* sqrtEps,
+                             const float* charge, int nVdw, const float* probeRadii,
+                             float vdwCap, float elecCap, float cutoff, float* out);
+
+/* Counters of the last search on this context: [0] kernel launches, [1] waves,
+ * [2] rotations, [3] device ms of the last search (events on the search stream). */
+int cdk_ctx_stats(cdk_ctx* ctx, double* out, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CDOCK_B200_H */

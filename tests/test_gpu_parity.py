@@ -1,0 +1,113 @@
+"""GPU parity of the FP32 search against the oracle, through the C-ABI (cdk_search)."""
+import numpy as np
+import pytest
+
+from cdocker_b200 import Receptor, synth, fill_ligand_grid
+from oracle import oracle as O
+from tests.parity import check_search
+
+pytestmark = pytest.mark.gpu
+
+
+def _emap(w, conf_of, quat_of):
+    def f(r):
+        return O.energy_map(w.grids, w.spacing, w.coor[conf_of(r)], w.charge, w.eps, w.slot,
+                            quat_of(r))
+    return f
+
+
+def test_c0_full_vs_fp64_direct(c0):
+    """Config 0 (32^3, K=9, 24 atoms, 500 rotations): every rotation vs the FP64 oracle."""
+    w = c0
+    with Receptor(w.grids, w.spacing) as rec:
+        minE, idx = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+    _, ridx, r64 = O.search_direct(w.grids, w.spacing, w.coor, w.charge, w.eps, w.slot, w.quats,
+                                   prec=1)
+    q = w.quats.reshape(-1, 4)
+    st = check_search(minE, idx, r64, ridx, _emap(w, lambda r: 0, lambda r: q[r]))
+    assert st["n"] == 500
+
+
+def test_c0_vs_fp32_cpunaive(c0):
+    """Same inputs vs cpuNaive's float accumulation (src/cpuNaive.cpp:194-216)."""
+    w = c0
+    q = w.quats[:, :100]
+    with Receptor(w.grids, w.spacing) as rec:
+        minE, idx = rec.search(w.coor, w.charge, w.eps, w.slot, q)
+    r32, ridx, _ = O.search_direct(w.grids, w.spacing, w.coor, w.charge, w.eps, w.slot, q, prec=0)
+    qq = q.reshape(-1, 4)
+    check_search(minE, idx, r32, ridx, _emap(w, lambda r: 0, lambda r: qq[r]))
+
+
+@pytest.mark.parametrize("name,nconf,nq", [("c1_64", 3, 16), ("c3_96", 1, 6), ("c4_128", 1, 4)])
+def test_larger_grids_vs_fp64(name, nconf, nq, grids_cache):
+    w = synth.make_workload(name, seed=1, n_conf=nconf, n_q=nq, grids_cache=grids_cache)
+    with Receptor(w.grids, w.spacing) as rec:
+        minE, idx = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+    _, ridx, r64 = O.search_direct(w.grids, w.spacing, w.coor, w.charge, w.eps, w.slot, w.quats,
+                                   prec=1)
+    qq = w.quats.reshape(-1, 4)
+    check_search(minE, idx, r64, ridx, _emap(w, lambda r: r // nq, lambda r: qq[r]))
+
+
+def test_waves_and_tiles_agree(c0):
+    """Different wave sizes and column tiles give identical results (work split only)."""
+    w = c0
+    q = w.quats[:, :64]
+    outs = []
+    for wave, ct in [(0, 0), (7, 4), (64, 8), (13, 16)]:
+        with Receptor(w.grids, w.spacing, wave_rotations=wave, col_tile=ct) as rec:
+            outs.append(rec.search(w.coor, w.charge, w.eps, w.slot, q))
+    for m, i in outs[1:]:
+        np.testing.assert_array_equal(i, outs[0][1])
+        np.testing.assert_allclose(m, outs[0][0], rtol=1e-6, atol=1e-5)
+
+
+def test_fill_bitexact_vs_reference(c0):
+    """cdk_fill_ligand_grid == the reference's FillLigandGrid, bit for bit."""
+    w = c0
+    rot, mn, ln = O.rotate_bbox(w.coor[0], w.quats[0, :4])
+    gpu = fill_ligand_grid(rot, mn, w.charge, w.eps, w.slot, w.K - 1, (w.n,) * 3, w.spacing)
+    if O.ref_available():
+        R = O.ref()
+        ref = np.zeros_like(gpu)
+        R.ref_fill_ligand_grid(4, rot.shape[1], O._pf(rot), O._pf(mn), O._pf(O._f32(w.charge)),
+                               O._pf(O._f32(w.eps)), O._pf(O._f32(w.radii)), 8,
+                               O._pf(O._f32(w.grid_radii)), w.n, w.n, w.n, w.spacing, O._pf(ref))
+    else:
+        ref = O.fill_ligand_grid(rot, mn, w.charge, w.eps, w.slot, w.K - 1, (w.n,) * 3, w.spacing)
+    assert np.array_equal(gpu.view(np.uint32), ref.view(np.uint32))
+
+
+def test_empty_window_and_zero_rotations(c0):
+    """A ligand longer than the grid leaves the window empty: +inf and -1 (the reference
+    leaves INFINITY and unset indices); nQ = 0 is a no-op."""
+    w = c0
+    big = w.coor[0] * 4.0  # ~32 A across on a 15.5 A grid
+    with Receptor(w.grids, w.spacing) as rec:
+        minE, idx = rec.search(big, w.charge, w.eps, w.slot, w.quats[:, :5])
+        assert np.all(np.isinf(minE)) and np.all(idx == -1)
+        m0, i0 = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats[:, :0])
+        assert m0.size == 0
+
+
+def test_invalid_slot_rejected(c0):
+    from cdocker_b200 import CdkError
+    w = c0
+    bad = w.slot.copy()
+    bad[0] = w.K - 1  # the elec channel is not a vdW slot
+    with Receptor(w.grids, w.spacing) as rec:
+        with pytest.raises(CdkError):
+            rec.search(w.coor, w.charge, w.eps, bad, w.quats[:, :3])
+
+
+def test_rescore_fp64_matches_oracle_map(c0):
+    w = c0
+    q = w.quats[0, :8]
+    with Receptor(w.grids, w.spacing) as rec:
+        minE, idx = rec.search(w.coor, w.charge, w.eps, w.slot, q[None])
+        e64 = rec.rescore_fp64(w.coor, w.charge, w.eps, w.slot, np.zeros(8, np.int32), q, idx)
+    for r in range(8):
+        emap = O.energy_map(w.grids, w.spacing, w.coor[0], w.charge, w.eps, w.slot, q[r])
+        ref = emap[tuple(idx[r])]
+        assert abs(e64[r] - ref) <= 1e-9 * max(1.0, abs(ref))
