@@ -362,6 +362,37 @@ def run_ours(args, rank, world, local_rank):
     rec.close()
 
 
+def profile_run(args):
+    """One warm-up and one timed search of `--profile-run` rotations (first conformers of the
+    config-1 workload), per-kernel device times from events around every launch."""
+    import torch
+    from cdocker_b200 import Receptor
+    w = make_rank_workload(0, 1)
+    n_q = N_Q
+    n_conf = max(1, min(N_CONF, (args.profile_run + n_q - 1) // n_q))
+    if args.profile_run < n_q:
+        n_q = args.profile_run
+    dev = torch.device("cuda", 0)
+    coor = torch.from_numpy(np.ascontiguousarray(w.coor[:n_conf])).to(dev)
+    q = torch.from_numpy(np.ascontiguousarray(w.quats[:n_conf, :n_q])).to(dev)
+    ch = torch.from_numpy(w.charge).to(dev)
+    ep = torch.from_numpy(w.eps).to(dev)
+    sl = torch.from_numpy(w.slot).to(dev)
+    n_rot = n_conf * n_q
+    e = torch.empty(n_rot, device=dev)
+    i = torch.empty(n_rot, 3, dtype=torch.int32, device=dev)
+    out = {}
+    with Receptor(w.grids, w.spacing, wave_rotations=args.wave, col_tile=args.col_tile,
+                  profile=True) as rec:
+        for it in range(2):
+            rec.search_device(w.coor.shape[1], n_conf, coor.data_ptr(), ch.data_ptr(),
+                              ep.data_ptr(), sl.data_ptr(), n_q, q.data_ptr(), e.data_ptr(),
+                              i.data_ptr(), 0)
+        out = rec.stats()
+    out["rotations_per_s"] = n_rot / (out["device_ms"] / 1e3)
+    print(json.dumps({"profile_run": n_rot, **out}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -376,6 +407,9 @@ def main():
     ap.add_argument("--ref-cufft", type=int, default=1)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--roofline-json", default="")
+    ap.add_argument("--profile-run", type=int, default=0,
+                    help="run one search of this many rotations with per-kernel events and "
+                         "print the timings (the small case used for ncu captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = _env_int("WORLD_SIZE", 1)
@@ -383,6 +417,9 @@ def main():
     local_rank = _env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.profile_run:
+        profile_run(args)
         return
     import torch
     import torch.distributed as dist

@@ -128,7 +128,7 @@ class Receptor:
 
     def __init__(self, grids, spacing: float, device: int = 0, wave_rotations: int = 0,
                  max_atoms: int = 256, col_tile: int = 0, form: int = L.CDK_FORM_FP32,
-                 use_graphs: int = 0):
+                 use_graphs: int = 0, profile: bool = False):
         g = _f32(grids)
         if g.ndim != 4:
             raise ValueError("grids must be [K, n, n, n]")
@@ -143,6 +143,7 @@ class Receptor:
         opts.max_atoms = max_atoms
         opts.col_tile = col_tile
         opts.use_graphs = use_graphs
+        opts.reserved[0] = 1 if profile else 0
         h = C.c_void_p()
         L.check(lib.cdk_ctx_create(g.shape[1], g.shape[2], g.shape[3], self.spacing, self.K,
                                    _pf(g), C.byref(opts), C.byref(h)))
@@ -210,7 +211,10 @@ class Receptor:
         return out
 
     def stats(self) -> dict:
-        out = np.zeros(4, np.float64)
-        L.check(L.lib().cdk_ctx_stats(self._h, out.ctypes.data_as(_dp), 4))
+        out = np.zeros(16, np.float64)
+        L.check(L.lib().cdk_ctx_stats(self._h, out.ctypes.data_as(_dp), 16))
+        names = ["prep", "spread_yz", "xpass", "yz_inv_argmin", "finalize"]
         return {"launches": int(out[0]), "waves": int(out[1]), "rotations": int(out[2]),
-                "device_ms": float(out[3])}
+                "device_ms": float(out[3]), "box": int(out[4]), "wave_rotations": int(out[5]),
+                "planes_spread": int(out[6]), "planes_window": int(out[7]),
+                "kernel_ms": {k: float(v) for k, v in zip(names, out[8:13])}}

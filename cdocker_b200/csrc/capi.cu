@@ -111,9 +111,14 @@ struct cdk_ctx {
   Arena tables;               // per-search tables
   Arena io;                   // staging of host-buffer searches
   unsigned int* d_misc = nullptr;  // [0] diameter bits, [1] flags, [2] error count
+  unsigned long long* d_work = nullptr;  // [0] x planes spread (A), [1] window planes (B)
+  unsigned long long* h_work = nullptr;
   unsigned int* h_misc = nullptr;  // pinned mirror
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  double stats[4] = {0, 0, 0, 0};
+  // per-kernel timing (opts.reserved[0] != 0): events around every launch of every wave
+  std::vector<cudaEvent_t> kev;
+  int kev_used = 0;
+  double stats[CDK_NSTATS] = {};
 };
 
 namespace {
@@ -174,26 +179,50 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   a.idx = d_idx;
   a.err_count = reinterpret_cast<int*>(c->d_misc + 2);
   a.col_tile = c->opts.col_tile > 0 ? c->opts.col_tile : pick_col_tile(n, K);
-  if (xpass_smem_bytes(n, K, a.col_tile) > 227 * 1024) {
+  if ((n <= 64 ? xpass2_smem_bytes(n, K, a.col_tile) : xpass_smem_bytes(n, K, a.col_tile)) > 227 * 1024 ||
+      (n <= 64 && a.col_tile > 16)) {
     set_error("column tile too large for shared memory");
     return CDK_ERR_INVALID;
   }
   CDK_CUDA(cudaMemsetAsync(c->d_misc + 2, 0, sizeof(unsigned int), s));
+  CDK_CUDA(cudaMemsetAsync(c->d_work, 0, 2 * sizeof(unsigned long long), s));
+  a.work = c->d_work;
+  const bool prof = c->opts.reserved[0] != 0;
+  const long nwaves = (nRot + wave - 1) / wave;
+  if (prof) {
+    const size_t need = (size_t)nwaves * (kLaunchesPerWave + 1);
+    while (c->kev.size() < need) {
+      cudaEvent_t e;
+      CDK_CUDA(cudaEventCreate(&e));
+      c->kev.push_back(e);
+    }
+  }
+  c->kev_used = 0;
   long launches = 1, waves = 0;
   for (long r0 = 0; r0 < nRot; r0 += wave) {
     a.nrot = (int)std::min<long>(wave, nRot - r0);
     a.rots = d_rots + r0;
+    cudaEvent_t* ev = prof ? &c->kev[(size_t)waves * (kLaunchesPerWave + 1)] : nullptr;
+    if (prof) CDK_CUDA(cudaEventRecord(ev[0], s));
     CDK_CUDA(launch_prep(a, s));
+    if (prof) CDK_CUDA(cudaEventRecord(ev[1], s));
     CDK_CUDA(launch_spread_yz(a, s));
+    if (prof) CDK_CUDA(cudaEventRecord(ev[2], s));
     CDK_CUDA(launch_xpass(a, s));
+    if (prof) CDK_CUDA(cudaEventRecord(ev[3], s));
     CDK_CUDA(launch_yz_inv_argmin(a, s));
+    if (prof) CDK_CUDA(cudaEventRecord(ev[4], s));
     CDK_CUDA(launch_finalize(a, s));
+    if (prof) CDK_CUDA(cudaEventRecord(ev[5], s));
     launches += kLaunchesPerWave;
     ++waves;
   }
+  c->kev_used = prof ? (int)waves : 0;
   c->stats[0] = (double)launches;
   c->stats[1] = (double)waves;
   c->stats[2] = (double)nRot;
+  c->stats[4] = (double)Lb;
+  c->stats[5] = (double)wave;
   return CDK_OK;
 }
 
@@ -277,6 +306,17 @@ int check_errors_after(cdk_ctx* c, cudaStream_t s) {
   CDK_CUDA(cudaStreamSynchronize(s));
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, c->ev0, c->ev1) == cudaSuccess) c->stats[3] = ms;
+  CDK_CUDA(cudaMemcpy(c->h_work, c->d_work, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  c->stats[6] = (double)c->h_work[0];
+  c->stats[7] = (double)c->h_work[1];
+  for (int k = 0; k < kLaunchesPerWave; ++k) c->stats[8 + k] = 0.0;
+  for (int w = 0; w < c->kev_used; ++w) {
+    cudaEvent_t* ev = &c->kev[(size_t)w * (kLaunchesPerWave + 1)];
+    for (int k = 0; k < kLaunchesPerWave; ++k) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, ev[k], ev[k + 1]) == cudaSuccess) c->stats[8 + k] += t;
+    }
+  }
   if (c->h_misc[2] != 0) {
     set_error(std::to_string(c->h_misc[2]) +
               " rotation(s) overflowed the planned ligand box; results for them are invalid");
@@ -367,6 +407,8 @@ int cdk_ctx_create(int nx, int ny, int nz, float spacing, int K, const float* gr
   CTX_CUDA(cudaMalloc(&c->d_tw, sizeof(float2) * n));
   CTX_CUDA(cudaMalloc(&c->d_misc, 4 * sizeof(unsigned int)));
   CTX_CUDA(cudaMallocHost(&c->h_misc, 4 * sizeof(unsigned int)));
+  CTX_CUDA(cudaMalloc(&c->d_work, 2 * sizeof(unsigned long long)));
+  CTX_CUDA(cudaMallocHost(&c->h_work, 2 * sizeof(unsigned long long)));
   std::vector<float2> tw(n);
   for (int j = 0; j < n; ++j) {
     const double ang = -2.0 * M_PI * j / n;
@@ -398,6 +440,9 @@ int cdk_ctx_destroy(cdk_ctx* c) {
   cudaFree(c->d_tw);
   cudaFree(c->d_misc);
   if (c->h_misc) cudaFreeHost(c->h_misc);
+  cudaFree(c->d_work);
+  if (c->h_work) cudaFreeHost(c->h_work);
+  for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
   cudaFree(c->wave.base);
   cudaFree(c->tables.base);
   cudaFree(c->io.base);
@@ -618,7 +663,7 @@ int cdk_sum_grids(const void* d_ligand_F, void* d_sum_F, int K, int odist, int i
 
 int cdk_ctx_stats(cdk_ctx* c, double* out, int n) {
   if (!c || !out) return CDK_ERR_INVALID;
-  for (int i = 0; i < n && i < 4; ++i) out[i] = c->stats[i];
+  for (int i = 0; i < n && i < CDK_NSTATS; ++i) out[i] = c->stats[i];
   return CDK_OK;
 }
 

@@ -69,6 +69,7 @@ struct WaveArgs {
   float* minE;               // output base (indexed by RotDesc.out)
   int* idx;
   int* err_count;
+  unsigned long long* work;  // [0] x planes spread, [1] window planes (work counters)
   int col_tile;
 };
 
@@ -83,6 +84,7 @@ cudaError_t launch_receptor_fft(int n, int K, const float* grids, float2* scratc
                                 float2* phat, const float2* tw, int col_tile, cudaStream_t s);
 // Shared memory per CTA of the x pass for given n, K, column tile.
 size_t xpass_smem_bytes(int n, int K, int col_tile);
+size_t xpass2_smem_bytes(int n, int K, int col_tile);
 int pick_col_tile(int n, int K);
 // Dense FillLigandGrid on the GPU.
 cudaError_t launch_fill_dense(int nQ, int nAtom, const float* coors, const float* mincoors,

@@ -316,6 +316,151 @@ __global__ void __launch_bounds__(256) k_xpass(WaveArgs a, int rot_per_cta) {
 }
 
 // ---------------------------------------------------------------------------------------
+// x pass for two-stage plans (N = R0*R1), fused stage by stage:
+//   phase A  first forward stage straight from A in global memory (only the x planes a
+//            channel touches are read; the rest are known zeros), two channels at a time
+//   phase B  second forward stage + conj(L_k) * P_k accumulated in registers over all
+//            channels (receptor tile resident in shared memory for the CTA's rotations),
+//            then the first inverse stage on the sum
+//   phase C  last inverse stage, written straight to B for x inside the window
+// Thread t of a pair (t, t^1) handles the even / odd channel of each pair; the pair's
+// partial sums meet through one shuffle.
+template <int N>
+__global__ void __launch_bounds__(256) k_xpass2(WaveArgs a, int rot_per_cta) {
+  constexpr int NZH = N / 2 + 1;
+  constexpr int NCOL = N * NZH;
+  constexpr int R0 = FFTPlan<N>::R0, R1 = FFTPlan<N>::R1, M1 = N / R0;
+  static_assert(FFTPlan<N>::NS == 2, "two-stage plans only");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ct = a.col_tile;
+  const int K = a.K;
+  float2* tw = reinterpret_cast<float2*>(smem_raw);
+  int* s_ch = reinterpret_cast<int*>(tw + N);          // [KMAX + 2]
+  float2* Ps = reinterpret_cast<float2*>(s_ch + 2 * KMAX);  // [N][K][ct]
+  float2* Wb = Ps + (size_t)N * K * ct;                 // [N][2][ct]
+  float2* S = Wb + (size_t)N * 2 * ct;                  // [N][ct]
+  const int c0 = blockIdx.x * ct;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  for (int i = tid; i < N; i += nthr) tw[i] = a.tw[i];
+  // receptor spectra of this column tile, all channels, resident for every rotation
+  for (int i = tid; i < N * K * ct; i += nthr) {
+    const int c = i % ct, t = i / ct;  // t = pos*K + k
+    Ps[i] = (c0 + c < NCOL) ? a.phat[(size_t)t * NCOL + c0 + c] : make_float2(0.f, 0.f);
+  }
+  const int r_begin = blockIdx.y * rot_per_cta;
+  const int r_end = min(a.nrot, r_begin + rot_per_cta);
+  for (int r = r_begin; r < r_end; ++r) {
+    const RotRec* rec = a.rec + r;
+    if (!rec->valid) continue;
+    __syncthreads();
+    if (tid == 0) {
+      int nk = 0;
+      for (int k = 0; k < K; ++k)
+        if (rec->xlo[k] <= rec->xhi[k]) s_ch[nk++] = k;
+      s_ch[KMAX] = nk;
+    }
+    __syncthreads();
+    const int nk = s_ch[KMAX];
+    // phase-B ownership: (half, c, b) with half fastest so that pairs share a warp
+    float2 acc[R1];
+#pragma unroll
+    for (int j = 0; j < R1; ++j) acc[j] = make_float2(0.f, 0.f);
+    const int nB = 2 * ct * R0;
+    for (int k0 = 0; k0 < nk; k0 += 2) {
+      // phase A: first forward stage for channels s_ch[k0], s_ch[k0+1]
+      for (int i = tid; i < 2 * ct * M1; i += nthr) {
+        const int c = i % ct;
+        const int t = i / ct;
+        const int half = t % 2;
+        const int np = t / 2;
+        float2 v[R0];
+        const int kk = k0 + half;
+        if (kk < nk && c0 + c < NCOL) {
+          const int k = s_ch[kk];
+          const int lo = rec->xlo[k], hi = rec->xhi[k];
+          const float2* src = a.A + (((size_t)r * K + k) * a.Lb) * NCOL + c0 + c;
+#pragma unroll
+          for (int j = 0; j < R0; ++j) {
+            const int x = np + j * M1;
+            v[j] = (x >= lo && x <= hi) ? src[(size_t)x * NCOL] : make_float2(0.f, 0.f);
+          }
+          Radix<R0, -1>::run(v);
+#pragma unroll
+          for (int q = 1; q < R0; ++q) v[q] = c_mul(v[q], tw[np * q]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < R0; ++j) v[j] = make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int q = 0; q < R0; ++q) Wb[((np + q * M1) * 2 + half) * ct + c] = v[q];
+      }
+      __syncthreads();
+      // phase B: second forward stage and the conjugate product, accumulated; thread tid
+      // owns item tid (the launcher keeps 2*ct*R0 <= blockDim.x)
+      if (tid < nB) {
+        const int half = tid & 1;
+        const int c = (tid >> 1) % ct;
+        const int b = (tid >> 1) / ct;
+        const int kk = k0 + half;
+        if (kk < nk) {
+          const int k = s_ch[kk];
+          float2 v[R1];
+#pragma unroll
+          for (int j = 0; j < R1; ++j) v[j] = Wb[((b * R1 + j) * 2 + half) * ct + c];
+          Radix<R1, -1>::run(v);
+#pragma unroll
+          for (int q = 0; q < R1; ++q) {
+            const float2 p = Ps[((b * R1 + q) * K + k) * ct + c];
+            const float2 t = c_conjmul(v[q], p);
+            acc[q].x += t.x;
+            acc[q].y += t.y;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // combine the pair (lanes tid, tid^1), first inverse stage, into S; whole warps take part
+    if (tid < ((nB + 31) & ~31)) {
+      float2 v[R1];
+#pragma unroll
+      for (int j = 0; j < R1; ++j) {
+        v[j].x = acc[j].x + __shfl_xor_sync(0xffffffffu, acc[j].x, 1);
+        v[j].y = acc[j].y + __shfl_xor_sync(0xffffffffu, acc[j].y, 1);
+      }
+      if (tid < nB && (tid & 1) == 0) {
+        const int c = (tid >> 1) % ct;
+        const int b = (tid >> 1) / ct;
+        Radix<R1, +1>::run(v);
+#pragma unroll
+        for (int j = 0; j < R1; ++j) S[(b * R1 + j) * ct + c] = v[j];
+      }
+    }
+    __syncthreads();
+    // phase C: last inverse stage, window rows only
+    const int Wx = rec->W[0];
+    for (int i = tid; i < ct * M1; i += nthr) {
+      const int c = i % ct;
+      const int np = i / ct;
+      float2 v[R0];
+#pragma unroll
+      for (int q = 0; q < R0; ++q) {
+        v[q] = S[(np + q * M1) * ct + c];
+        if (q > 0) v[q] = c_mulc(v[q], tw[np * q]);
+      }
+      Radix<R0, +1>::run(v);
+      if (c0 + c < NCOL) {
+        float2* dst = a.B + (size_t)r * N * NCOL + c0 + c;
+#pragma unroll
+        for (int j = 0; j < R0; ++j) {
+          const int x = np + j * M1;
+          if (x < Wx) dst[(size_t)x * NCOL] = v[j];
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
 // inverse (y,z) of one (rotation, x in window) plane + min / first argmin
 template <int N>
 __global__ void __launch_bounds__(256) k_yz_inv_argmin(WaveArgs a) {
@@ -386,6 +531,13 @@ __global__ void k_finalize(WaveArgs a) {
   const int out = a.rots[r].out;
   const RotRec* rec = a.rec + r;
   if (rec->err) atomicAdd(a.err_count, 1);
+  if (rec->valid) {
+    unsigned long long planes = 0;
+    for (int k = 0; k < a.K; ++k)
+      if (rec->xlo[k] <= rec->xhi[k]) planes += (unsigned long long)(rec->xhi[k] - rec->xlo[k] + 1);
+    atomicAdd(a.work, planes);
+    atomicAdd(a.work + 1, (unsigned long long)rec->W[0]);
+  }
   const unsigned long long key = a.keys[r];
   if (!rec->valid || key == ~0ull) {
     a.minE[out] = INFINITY;
@@ -476,23 +628,37 @@ cudaError_t launch_yz_inv_t(const WaveArgs& a, cudaStream_t s) {
 
 template <int N>
 cudaError_t launch_xpass_t(const WaveArgs& a, cudaStream_t s) {
-  const size_t sm = xpass_smem_bytes(N, a.K, a.col_tile);
-  cudaError_t e = cudaFuncSetAttribute(k_xpass<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  if (e != cudaSuccess) return e;
   constexpr int NCOL = N * (N / 2 + 1);
   const int tiles = (NCOL + a.col_tile - 1) / a.col_tile;
-  // enough CTAs to fill the machine a few times over; each walks a chunk of rotations
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  int chunks = (sms * 8 + tiles - 1) / tiles;
-  if (chunks > a.nrot) chunks = a.nrot;
-  if (chunks < 1) chunks = 1;
-  const int per = (a.nrot + chunks - 1) / chunks;
-  chunks = (a.nrot + per - 1) / per;
-  dim3 grid(tiles, chunks);
-  k_xpass<N><<<grid, 256, sm, s>>>(a, per);
-  return cudaGetLastError();
+  if constexpr (FFTPlan<N>::NS == 2) {
+    if (2 * a.col_tile * FFTPlan<N>::R0 > 256) return cudaErrorInvalidValue;
+    // rotations per CTA: as many as keeps >= 2 CTAs per SM busy, so that the receptor tile
+    // loaded into shared memory is reused across many rotations
+    const size_t sm = xpass2_smem_bytes(N, a.K, a.col_tile);
+    cudaError_t e = cudaFuncSetAttribute(k_xpass2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    int chunks = (sms * 2 + tiles - 1) / tiles;
+    if (chunks > a.nrot) chunks = a.nrot;
+    if (chunks < 1) chunks = 1;
+    const int per = (a.nrot + chunks - 1) / chunks;
+    chunks = (a.nrot + per - 1) / per;
+    k_xpass2<N><<<dim3(tiles, chunks), 256, sm, s>>>(a, per);
+    return cudaGetLastError();
+  } else {
+    const size_t sm = xpass_smem_bytes(N, a.K, a.col_tile);
+    cudaError_t e = cudaFuncSetAttribute(k_xpass<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    int chunks = (sms * 8 + tiles - 1) / tiles;
+    if (chunks > a.nrot) chunks = a.nrot;
+    if (chunks < 1) chunks = 1;
+    const int per = (a.nrot + chunks - 1) / chunks;
+    chunks = (a.nrot + per - 1) / per;
+    k_xpass<N><<<dim3(tiles, chunks), 256, sm, s>>>(a, per);
+    return cudaGetLastError();
+  }
 }
 
 template <int N>
@@ -513,14 +679,24 @@ cudaError_t launch_receptor_t(int K, const float* grids, float2* scratch, float2
 
 }  // namespace
 
+size_t xpass2_smem_bytes(int n, int K, int col_tile) {
+  return sizeof(float2) * n + sizeof(int) * 2 * KMAX +
+         sizeof(float2) * (size_t)n * col_tile * (K + 2 + 1);
+}
+
 size_t xpass_smem_bytes(int n, int K, int col_tile) {
   return sizeof(float2) * n + sizeof(int) * 2 * KMAX + sizeof(float2) * (size_t)n * K * col_tile;
 }
 
 int pick_col_tile(int n, int K) {
-  // largest tile (<= 16 columns) whose work buffer stays within 100 KB of shared memory
+  // largest tile (<= 16 columns) whose buffers stay within ~110 KB of shared memory, so that
+  // two CTAs share an SM
   int ct = 16;
-  while (ct > 2 && xpass_smem_bytes(n, K, ct) > 100 * 1024) ct >>= 1;
+  if (n == 32 || n == 64) {
+    while (ct > 2 && xpass2_smem_bytes(n, K, ct) > 110 * 1024) ct >>= 1;
+  } else {
+    while (ct > 2 && xpass_smem_bytes(n, K, ct) > 100 * 1024) ct >>= 1;
+  }
   return ct;
 }
 

@@ -48,7 +48,7 @@ typedef struct cdk_opts {
   int max_atoms;       /* largest ligand (atoms) this context will see; 0 = 256 */
   int col_tile;        /* spectral columns per CTA in the x pass; 0 = autotuned default */
   int use_graphs;      /* 1 = replay each wave through a captured CUDA graph */
-  int reserved[8];
+  int reserved[8];     /* [0] = 1: time every kernel with events (cdk_ctx_stats [8..12]) */
 } cdk_opts;
 
 /* Library version string. */
@@ -151,8 +151,13 @@ int cdk_synth_receptor_grids(int n, float spacing, const float* origin, int nAto
                              const float* charge, int nVdw, const float* probeRadii,
                              float vdwCap, float elecCap, float cutoff, float* out);
 
-/* Counters of the last search on this context: [0] kernel launches, [1] waves,
- * [2] rotations, [3] device ms of the last search (events on the search stream). */
+/* Counters of the last search on this context (n <= CDK_NSTATS values):
+ * [0] kernel launches, [1] waves, [2] rotations, [3] device ms of the search (events on the
+ * search stream), [4] planned ligand box edge, [5] rotations per wave, [6] (y,z) planes the
+ * spread kernel transformed, [7] window planes the x pass wrote, [8..12] device ms per kernel
+ * kind (prep, spread_yz, xpass, yz_inv_argmin, finalize) when the context was created with
+ * opts.reserved[0] = 1 (events around every launch), else 0. */
+#define CDK_NSTATS 16
 int cdk_ctx_stats(cdk_ctx* ctx, double* out, int n);
 
 #ifdef __cplusplus

@@ -110,4 +110,7 @@ def test_rescore_fp64_matches_oracle_map(c0):
     for r in range(8):
         emap = O.energy_map(w.grids, w.spacing, w.coor[0], w.charge, w.eps, w.slot, q[r])
         ref = emap[tuple(idx[r])]
-        assert abs(e64[r] - ref) <= 1e-9 * max(1.0, abs(ref))
+        # the oracle map sums the float-rounded ligand grid; the re-score keeps the trilinear
+        # weights in double, so the two differ by float rounding of the weights (~1e-8)
+        assert abs(e64[r] - ref) <= 1e-7 * max(1.0, abs(ref))
+        assert abs(e64[r] - minE[r]) <= 1e-4 * max(1.0, abs(ref))
