@@ -325,8 +325,8 @@ def run_ours(args, rank, world, local_rank):
 
     if rank == 0:
         hbm, peak_kind = _peaks()
-        ncol = 64 * 33
-        b_rot = 8 * 9 * 64 ** 3 + 16 * 9 * ncol + 16 * ncol + 8 * 64 ** 3
+        nc = 64 * 64 * 33  # half-spectrum points of one grid
+        b_rot = 8 * 9 * 64 ** 3 + 16 * 9 * nc + 16 * nc + 8 * 64 ** 3
         rps = value / world
         line = {
             "metric": METRIC, "value": value, "unit": "rotations/s", "n_gpus": world,

@@ -76,6 +76,7 @@ SIGNATURES = {
     "cdk_synth_receptor_grids": (C.c_int, [C.c_int, C.c_float, _fp, C.c_int, _fp, _fp, _fp, _fp,
                                            C.c_int, _fp, C.c_float, C.c_float, C.c_float, _fp]),
     "cdk_ctx_stats": (C.c_int, [_vp, _dp, C.c_int]),
+    "cdk_pose_coordinates": (C.c_int, [C.c_int, _fp, _fp, _dp, C.c_float, _ip, _dp]),
 }
 
 _lib = None

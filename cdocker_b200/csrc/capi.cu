@@ -180,8 +180,8 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   a.err_count = reinterpret_cast<int*>(c->d_misc + 2);
   a.col_tile = c->opts.col_tile > 0 ? c->opts.col_tile : pick_col_tile(n, K);
   if ((n <= 64 ? xpass2_smem_bytes(n, K, a.col_tile) : xpass_smem_bytes(n, K, a.col_tile)) > 227 * 1024 ||
-      (n <= 64 && a.col_tile > 16)) {
-    set_error("column tile too large for shared memory");
+      (n <= 64 && a.col_tile != 8 && a.col_tile != 16)) {
+    set_error("column tile must be 8 or 16 for n <= 64 and fit shared memory");
     return CDK_ERR_INVALID;
   }
   CDK_CUDA(cudaMemsetAsync(c->d_misc + 2, 0, sizeof(unsigned int), s));
@@ -326,6 +326,23 @@ int check_errors_after(cdk_ctx* c, cudaStream_t s) {
 }
 
 }  // namespace
+
+namespace cdk {
+bool ctx_view(const cdk_ctx* c, CtxView* v) {
+  if (!c || !v) return false;
+  v->dev = c->dev;
+  v->n = c->n;
+  v->K = c->K;
+  v->spacing = c->spacing;
+  v->col_tile_opt = c->opts.col_tile;
+  v->max_atoms = c->opts.max_atoms;
+  v->phat = c->d_phat;
+  v->tw = c->d_tw;
+  v->h_misc = c->h_misc;
+  v->stream = c->stream;
+  return true;
+}
+}  // namespace cdk
 
 extern "C" {
 

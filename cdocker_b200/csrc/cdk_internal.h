@@ -105,4 +105,21 @@ constexpr int kLaunchesPerWave = 5;
 
 void set_error(const std::string& msg);
 
+// Read-only view of a context's resident state, for entry points that live outside capi.cu.
+struct CtxView {
+  int dev, n, K;
+  float spacing;
+  int col_tile_opt, max_atoms;
+  const float2* phat;
+  const float2* tw;
+  unsigned int* h_misc;  // pinned host scratch of the context (4 words)
+  cudaStream_t stream;
+};
+
+}  // namespace cdk
+
+struct cdk_ctx;
+namespace cdk {
+// Fills *v from the context; returns false for a null context.
+bool ctx_view(const cdk_ctx* c, CtxView* v);
 }  // namespace cdk

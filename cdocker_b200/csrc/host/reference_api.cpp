@@ -292,6 +292,28 @@ using namespace cdk;
 
 extern "C" {
 
+// Pose of a rotation at its best translation, as the driver rebuilds it
+// (src/TranRotaConfSearchNoMini.cu:473-487): the rotated float coordinates widened to double,
+// plus (gridMin - mincoor + idx * spacing) per axis, where gridMin = mid - len/2 (:149-151)
+// and idx * spacing is the float product of the reference.
+int cdk_pose_coordinates(int nAtom, const float* coor, const float* quat, const double* gridMin,
+                         float spacing, const int* idx, double* out) {
+  if (nAtom <= 0 || !coor || !quat || !gridMin || !idx || !out) {
+    set_error("invalid argument");
+    return CDK_ERR_INVALID;
+  }
+  std::vector<float> rc((size_t)nAtom * 3);
+  for (int a = 0; a < nAtom; ++a) Rotate(quat, coor + 3 * a, &rc[3 * a]);
+  float mn[3];
+  GetMinCoors(1, nAtom, rc.data(), mn);
+  for (int a = 0; a < nAtom; ++a)
+    for (int d = 0; d < 3; ++d) {
+      const float step = (float)idx[d] * spacing;
+      out[3 * a + d] = (double)rc[3 * a + d] + (gridMin[d] - (double)mn[d] + (double)step);
+    }
+  return CDK_OK;
+}
+
 int cdk_quaternion_uniform_sampling(uint64_t seed, int nConf, int nQ, float* out) {
   if (!out || nConf < 0 || nQ < 0) {
     set_error("invalid argument");

@@ -206,7 +206,11 @@ __global__ void __launch_bounds__(256) k_spread_yz(WaveArgs a) {
   float* Pf = reinterpret_cast<float*>(P);
   for (int i = tid; i < npairs * (N + 1); i += nthr) P[i] = make_float2(0.f, 0.f);
   __syncthreads();
-  // spread the atoms touching plane x (src/FillLigandGrid.cpp:24-66 vdW, :75-118 elec)
+  // spread the atoms touching plane x (src/FillLigandGrid.cpp:24-66 vdW, :75-118 elec).
+  // Warp 0 adds the atoms one after another in ascending atom order, the four (y,z) corners
+  // of an atom in four lanes (they never share a cell), each add rounded back to float from
+  // double as in the reference: the plane is bit-identical to FillLigandGrid's and the
+  // search is deterministic whatever the batch around a rotation.
   const RotDesc rd = a.rots[r];
   const ConfDesc cd = a.confs[rd.conf];
   const AtomParam* prm = a.params + cd.param_off;
@@ -214,25 +218,42 @@ __global__ void __launch_bounds__(256) k_spread_yz(WaveArgs a) {
   const float h = a.spacing;
   const bool elec = (k == a.K - 1);
   const int nA = rec->nA;
-  for (int i = tid; i < nA; i += nthr) {
-    const AtomParam ap = prm[i];
-    if (!elec && ap.slot != k) continue;
-    const float4 p = a.rot_xyz[(size_t)r * a.max_atoms + i];
-    const int xi = cell_of(p.x, mn0, h);
-    double wx;
-    if (xi == x) wx = 1.0 - ratio_of(p.x, mn0, h, xi);
-    else if (xi + 1 == x) wx = ratio_of(p.x, mn0, h, xi);
-    else continue;
-    const int yi = cell_of(p.y, mn1, h), zi = cell_of(p.z, mn2, h);
-    const double yr = ratio_of(p.y, mn1, h, yi), zr = ratio_of(p.z, mn2, h, zi);
-    const double s = elec ? (double)ap.charge : (double)ap.w_vdw;
-    const double sx = s * wx;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const int dy = c >> 1, dz = c & 1;
-      const double w = sx * (dy ? yr : 1.0 - yr) * (dz ? zr : 1.0 - zr);
-      const int y = yi + dy, z = zi + dz;
-      if (y < N && z < N) atomicAdd(&Pf[((y >> 1) * (N + 1) + z) * 2 + (y & 1)], (float)w);
+  if (tid < 32) {
+    const int lane = tid;
+    for (int base = 0; base < nA; base += 32) {
+      const int i = base + lane;
+      bool touch = false;
+      if (i < nA) {
+        const AtomParam ap = prm[i];
+        if (elec || ap.slot == k) {
+          const int xi = cell_of(a.rot_xyz[(size_t)r * a.max_atoms + i].x, mn0, h);
+          touch = (xi == x) || (xi + 1 == x);
+        }
+      }
+      unsigned int m = __ballot_sync(0xffffffffu, touch);
+      while (m) {
+        const int at = base + __ffs(m) - 1;
+        m &= m - 1;
+        if (lane < 4) {
+          const AtomParam ap = prm[at];
+          const float4 p = a.rot_xyz[(size_t)r * a.max_atoms + at];
+          const int xi = cell_of(p.x, mn0, h);
+          const double xr = ratio_of(p.x, mn0, h, xi);
+          const double wx = (xi == x) ? __dsub_rn(1.0, xr) : xr;
+          const int yi = cell_of(p.y, mn1, h), zi = cell_of(p.z, mn2, h);
+          const double yr = ratio_of(p.y, mn1, h, yi), zr = ratio_of(p.z, mn2, h, zi);
+          const double sc = elec ? (double)ap.charge : (double)ap.w_vdw;
+          const int dy = lane >> 1, dz = lane & 1;
+          const double w = __dmul_rn(__dmul_rn(__dmul_rn(sc, wx), dy ? yr : __dsub_rn(1.0, yr)),
+                                     dz ? zr : __dsub_rn(1.0, zr));
+          const int y = yi + dy, z = zi + dz;
+          if (y < N && z < N) {
+            float* cell = &Pf[((y >> 1) * (N + 1) + z) * 2 + (y & 1)];
+            *cell = (float)__dadd_rn((double)*cell, w);
+          }
+        }
+        __syncwarp();
+      }
     }
   }
   __syncthreads();
@@ -316,145 +337,142 @@ __global__ void __launch_bounds__(256) k_xpass(WaveArgs a, int rot_per_cta) {
 }
 
 // ---------------------------------------------------------------------------------------
-// x pass for two-stage plans (N = R0*R1), fused stage by stage:
+// x pass for two-stage plans (N = R0*R1), fused stage by stage; CT spectral columns per CTA:
 //   phase A  first forward stage straight from A in global memory (only the x planes a
-//            channel touches are read; the rest are known zeros), two channels at a time
+//            channel touches are read; the rest are known zeros), two channels per round;
+//            the next round's loads are issued before this round's phase B to hide latency
 //   phase B  second forward stage + conj(L_k) * P_k accumulated in registers over all
-//            channels (receptor tile resident in shared memory for the CTA's rotations),
-//            then the first inverse stage on the sum
+//            channels (receptor tile resident in shared memory for the CTA's rotations)
+//   combine  pair sum through one shuffle, first inverse stage
 //   phase C  last inverse stage, written straight to B for x inside the window
-// Thread t of a pair (t, t^1) handles the even / odd channel of each pair; the pair's
-// partial sums meet through one shuffle.
-template <int N>
-__global__ void __launch_bounds__(256) k_xpass2(WaveArgs a, int rot_per_cta) {
+template <int N, int CT>
+__global__ void __launch_bounds__(256, 2) k_xpass2(WaveArgs a, int rot_per_cta) {
   constexpr int NZH = N / 2 + 1;
   constexpr int NCOL = N * NZH;
   constexpr int R0 = FFTPlan<N>::R0, R1 = FFTPlan<N>::R1, M1 = N / R0;
+  constexpr int NA = 2 * CT * M1;  // phase-A items
+  constexpr int NB = 2 * CT * R0;  // phase-B items
   static_assert(FFTPlan<N>::NS == 2, "two-stage plans only");
+  static_assert(NA <= 256 && NB <= 256, "one item per thread");
+  static_assert(NCOL % CT == 0, "column tiles must divide the half spectrum");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int ct = a.col_tile;
   const int K = a.K;
   float2* tw = reinterpret_cast<float2*>(smem_raw);
-  int* s_ch = reinterpret_cast<int*>(tw + N);          // [KMAX + 2]
-  float2* Ps = reinterpret_cast<float2*>(s_ch + 2 * KMAX);  // [N][K][ct]
-  float2* Wb = Ps + (size_t)N * K * ct;                 // [N][2][ct]
-  float2* S = Wb + (size_t)N * 2 * ct;                  // [N][ct]
-  const int c0 = blockIdx.x * ct;
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  for (int i = tid; i < N; i += nthr) tw[i] = a.tw[i];
-  // receptor spectra of this column tile, all channels, resident for every rotation
-  for (int i = tid; i < N * K * ct; i += nthr) {
-    const int c = i % ct, t = i / ct;  // t = pos*K + k
-    Ps[i] = (c0 + c < NCOL) ? a.phat[(size_t)t * NCOL + c0 + c] : make_float2(0.f, 0.f);
+  int* s_ch = reinterpret_cast<int*>(tw + N);               // [KMAX] channel ids, [KMAX] count
+  short* s_rng = reinterpret_cast<short*>(s_ch + 2 * KMAX);  // [KMAX][2] x range per slot
+  float2* Ps = reinterpret_cast<float2*>(s_rng + 4 * KMAX);  // [N][K][CT]
+  float2* Wb = Ps + (size_t)N * K * CT;                      // [N][2][CT]
+  float2* S = Wb + (size_t)N * 2 * CT;                       // [N][CT]
+  const int c0 = blockIdx.x * CT;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < N; i += 256) tw[i] = a.tw[i];
+  for (int i = tid; i < N * K * CT; i += 256) {
+    const int c = i % CT, t = i / CT;  // t = pos*K + k
+    Ps[i] = a.phat[(size_t)t * NCOL + c0 + c];
   }
+  // per-thread roles
+  const int a_c = tid % CT, a_half = (tid / CT) & 1, a_np = tid / (2 * CT);
+  const int b_half = tid & 1, b_c = (tid >> 1) % CT, b_b = (tid >> 1) / CT;
   const int r_begin = blockIdx.y * rot_per_cta;
   const int r_end = min(a.nrot, r_begin + rot_per_cta);
   for (int r = r_begin; r < r_end; ++r) {
     const RotRec* rec = a.rec + r;
     if (!rec->valid) continue;
-    __syncthreads();
+    __syncthreads();  // previous rotation is done with s_ch / Wb / S
     if (tid == 0) {
       int nk = 0;
       for (int k = 0; k < K; ++k)
-        if (rec->xlo[k] <= rec->xhi[k]) s_ch[nk++] = k;
+        if (rec->xlo[k] <= rec->xhi[k]) {
+          s_rng[2 * nk] = rec->xlo[k];
+          s_rng[2 * nk + 1] = rec->xhi[k];
+          s_ch[nk++] = k;
+        }
       s_ch[KMAX] = nk;
     }
     __syncthreads();
     const int nk = s_ch[KMAX];
-    // phase-B ownership: (half, c, b) with half fastest so that pairs share a warp
+    const float2* Ar = a.A + ((size_t)r * K) * a.Lb * NCOL + c0 + a_c;
+    // raw loads of one round (channels kk0, kk0+1) for this thread's phase-A item
+    auto load_round = [&](int kk0, float2* v) {
+      const int kk = kk0 + a_half;
+      if (tid < NA && kk < nk) {
+        const int k = s_ch[kk];
+        const int lo = s_rng[2 * kk], hi = s_rng[2 * kk + 1];
+        const float2* src = Ar + (size_t)k * a.Lb * NCOL;
+#pragma unroll
+        for (int j = 0; j < R0; ++j) {
+          const int x = a_np + j * M1;
+          v[j] = (x >= lo && x <= hi) ? src[(size_t)x * NCOL] : make_float2(0.f, 0.f);
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < R0; ++j) v[j] = make_float2(0.f, 0.f);
+      }
+    };
     float2 acc[R1];
 #pragma unroll
     for (int j = 0; j < R1; ++j) acc[j] = make_float2(0.f, 0.f);
-    const int nB = 2 * ct * R0;
+    float2 va[R0];
+    load_round(0, va);
     for (int k0 = 0; k0 < nk; k0 += 2) {
-      // phase A: first forward stage for channels s_ch[k0], s_ch[k0+1]
-      for (int i = tid; i < 2 * ct * M1; i += nthr) {
-        const int c = i % ct;
-        const int t = i / ct;
-        const int half = t % 2;
-        const int np = t / 2;
-        float2 v[R0];
-        const int kk = k0 + half;
-        if (kk < nk && c0 + c < NCOL) {
-          const int k = s_ch[kk];
-          const int lo = rec->xlo[k], hi = rec->xhi[k];
-          const float2* src = a.A + (((size_t)r * K + k) * a.Lb) * NCOL + c0 + c;
+      // phase A: first forward stage into Wb
+      if (tid < NA) {
+        Radix<R0, -1>::run(va);
 #pragma unroll
-          for (int j = 0; j < R0; ++j) {
-            const int x = np + j * M1;
-            v[j] = (x >= lo && x <= hi) ? src[(size_t)x * NCOL] : make_float2(0.f, 0.f);
-          }
-          Radix<R0, -1>::run(v);
+        for (int q = 1; q < R0; ++q) va[q] = c_mul(va[q], tw[a_np * q]);
 #pragma unroll
-          for (int q = 1; q < R0; ++q) v[q] = c_mul(v[q], tw[np * q]);
-        } else {
-#pragma unroll
-          for (int j = 0; j < R0; ++j) v[j] = make_float2(0.f, 0.f);
-        }
-#pragma unroll
-        for (int q = 0; q < R0; ++q) Wb[((np + q * M1) * 2 + half) * ct + c] = v[q];
+        for (int q = 0; q < R0; ++q) Wb[((a_np + q * M1) * 2 + a_half) * CT + a_c] = va[q];
       }
       __syncthreads();
-      // phase B: second forward stage and the conjugate product, accumulated; thread tid
-      // owns item tid (the launcher keeps 2*ct*R0 <= blockDim.x)
-      if (tid < nB) {
-        const int half = tid & 1;
-        const int c = (tid >> 1) % ct;
-        const int b = (tid >> 1) / ct;
-        const int kk = k0 + half;
-        if (kk < nk) {
-          const int k = s_ch[kk];
-          float2 v[R1];
+      if (k0 + 2 < nk) load_round(k0 + 2, va);  // in flight during phase B
+      // phase B: second forward stage and the conjugate product, accumulated
+      const int kk = k0 + b_half;
+      if (tid < NB && kk < nk) {
+        const int k = s_ch[kk];
+        float2 v[R1];
 #pragma unroll
-          for (int j = 0; j < R1; ++j) v[j] = Wb[((b * R1 + j) * 2 + half) * ct + c];
-          Radix<R1, -1>::run(v);
+        for (int j = 0; j < R1; ++j) v[j] = Wb[((b_b * R1 + j) * 2 + b_half) * CT + b_c];
+        Radix<R1, -1>::run(v);
 #pragma unroll
-          for (int q = 0; q < R1; ++q) {
-            const float2 p = Ps[((b * R1 + q) * K + k) * ct + c];
-            const float2 t = c_conjmul(v[q], p);
-            acc[q].x += t.x;
-            acc[q].y += t.y;
-          }
+        for (int q = 0; q < R1; ++q) {
+          const float2 p = Ps[((b_b * R1 + q) * K + k) * CT + b_c];
+          acc[q].x += v[q].x * p.x + v[q].y * p.y;
+          acc[q].y += v[q].x * p.y - v[q].y * p.x;
         }
       }
       __syncthreads();
     }
-    // combine the pair (lanes tid, tid^1), first inverse stage, into S; whole warps take part
-    if (tid < ((nB + 31) & ~31)) {
+    // combine the pair (lanes tid, tid^1), first inverse stage, into S
+    if (tid < ((NB + 31) & ~31)) {
       float2 v[R1];
 #pragma unroll
       for (int j = 0; j < R1; ++j) {
         v[j].x = acc[j].x + __shfl_xor_sync(0xffffffffu, acc[j].x, 1);
         v[j].y = acc[j].y + __shfl_xor_sync(0xffffffffu, acc[j].y, 1);
       }
-      if (tid < nB && (tid & 1) == 0) {
-        const int c = (tid >> 1) % ct;
-        const int b = (tid >> 1) / ct;
+      if (tid < NB && b_half == 0) {
         Radix<R1, +1>::run(v);
 #pragma unroll
-        for (int j = 0; j < R1; ++j) S[(b * R1 + j) * ct + c] = v[j];
+        for (int j = 0; j < R1; ++j) S[(b_b * R1 + j) * CT + b_c] = v[j];
       }
     }
     __syncthreads();
     // phase C: last inverse stage, window rows only
     const int Wx = rec->W[0];
-    for (int i = tid; i < ct * M1; i += nthr) {
-      const int c = i % ct;
-      const int np = i / ct;
+    if (tid < CT * M1) {
+      const int c = tid % CT, np = tid / CT;
       float2 v[R0];
 #pragma unroll
       for (int q = 0; q < R0; ++q) {
-        v[q] = S[(np + q * M1) * ct + c];
+        v[q] = S[(np + q * M1) * CT + c];
         if (q > 0) v[q] = c_mulc(v[q], tw[np * q]);
       }
       Radix<R0, +1>::run(v);
-      if (c0 + c < NCOL) {
-        float2* dst = a.B + (size_t)r * N * NCOL + c0 + c;
+      float2* dst = a.B + (size_t)r * N * NCOL + c0 + c;
 #pragma unroll
-        for (int j = 0; j < R0; ++j) {
-          const int x = np + j * M1;
-          if (x < Wx) dst[(size_t)x * NCOL] = v[j];
-        }
+      for (int j = 0; j < R0; ++j) {
+        const int x = np + j * M1;
+        if (x < Wx) dst[(size_t)x * NCOL] = v[j];
       }
     }
   }
@@ -634,18 +652,22 @@ cudaError_t launch_xpass_t(const WaveArgs& a, cudaStream_t s) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if constexpr (FFTPlan<N>::NS == 2) {
-    if (2 * a.col_tile * FFTPlan<N>::R0 > 256) return cudaErrorInvalidValue;
-    // rotations per CTA: as many as keeps >= 2 CTAs per SM busy, so that the receptor tile
-    // loaded into shared memory is reused across many rotations
+    // fixed 16-column tiles; chunks of up to 32 rotations per CTA keep the receptor tile
+    // reused while giving the scheduler many CTAs per SM slot
+    constexpr int CT = 16;
+    if (a.col_tile != CT && a.col_tile != 8) return cudaErrorInvalidValue;
     const size_t sm = xpass2_smem_bytes(N, a.K, a.col_tile);
-    cudaError_t e = cudaFuncSetAttribute(k_xpass2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    int chunks = (sms * 2 + tiles - 1) / tiles;
-    if (chunks > a.nrot) chunks = a.nrot;
-    if (chunks < 1) chunks = 1;
-    const int per = (a.nrot + chunks - 1) / chunks;
-    chunks = (a.nrot + per - 1) / per;
-    k_xpass2<N><<<dim3(tiles, chunks), 256, sm, s>>>(a, per);
+    const int per = 32;
+    const int chunks = (a.nrot + per - 1) / per;
+    if (a.col_tile == CT) {
+      cudaError_t e = cudaFuncSetAttribute(k_xpass2<N, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      if (e != cudaSuccess) return e;
+      k_xpass2<N, 16><<<dim3(NCOL / 16, chunks), 256, sm, s>>>(a, per);
+    } else {
+      cudaError_t e = cudaFuncSetAttribute(k_xpass2<N, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      if (e != cudaSuccess) return e;
+      k_xpass2<N, 8><<<dim3(NCOL / 8, chunks), 256, sm, s>>>(a, per);
+    }
     return cudaGetLastError();
   } else {
     const size_t sm = xpass_smem_bytes(N, a.K, a.col_tile);
@@ -680,7 +702,7 @@ cudaError_t launch_receptor_t(int K, const float* grids, float2* scratch, float2
 }  // namespace
 
 size_t xpass2_smem_bytes(int n, int K, int col_tile) {
-  return sizeof(float2) * n + sizeof(int) * 2 * KMAX +
+  return sizeof(float2) * n + sizeof(int) * 2 * KMAX + sizeof(short) * 4 * KMAX +
          sizeof(float2) * (size_t)n * col_tile * (K + 2 + 1);
 }
 
@@ -693,7 +715,7 @@ int pick_col_tile(int n, int K) {
   // two CTAs share an SM
   int ct = 16;
   if (n == 32 || n == 64) {
-    while (ct > 2 && xpass2_smem_bytes(n, K, ct) > 110 * 1024) ct >>= 1;
+    if (xpass2_smem_bytes(n, K, 16) > 110 * 1024) ct = 8;
   } else {
     while (ct > 2 && xpass_smem_bytes(n, K, ct) > 100 * 1024) ct >>= 1;
   }

@@ -130,6 +130,12 @@ int cdk_filter_quaternions(const float* coor, int nAtom, int nQ, const float* qu
 int cdk_vdw_slots(int nAtom, const float* radii, int nVdw, const float* gridRadii,
                   int* usedIdx, int* atomSlot, int* nUsed);
 
+/* Pose of one rotation at its best translation (src/TranRotaConfSearchNoMini.cu:473-487):
+ * out[a] = Rotate(quat, coor[a]) + gridMin - mincoor + idx * spacing, in double.
+ * gridMin = mid - len/2 of the grid file (:149-151). */
+int cdk_pose_coordinates(int nAtom, const float* coor, const float* quat, const double* gridMin,
+                         float spacing, const int* idx, double* out);
+
 /* ReadGrids (src/ReadGrids.cpp:6-68): header ints [numGrids, x, y, z], floats
  * [midx, midy, midz, xlen, ylen, zlen, spacing, restraint_k]; radii (numGrids-1) and values
  * (numGrids*x*y*z) are written when the capacities suffice. Pass NULL buffers to size first. */

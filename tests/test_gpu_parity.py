@@ -55,12 +55,13 @@ def test_waves_and_tiles_agree(c0):
     w = c0
     q = w.quats[:, :64]
     outs = []
-    for wave, ct in [(0, 0), (7, 4), (64, 8), (13, 16)]:
+    for wave, ct in [(0, 0), (7, 8), (64, 8), (13, 16)]:
         with Receptor(w.grids, w.spacing, wave_rotations=wave, col_tile=ct) as rec:
             outs.append(rec.search(w.coor, w.charge, w.eps, w.slot, q))
     for m, i in outs[1:]:
+        # the channel sum runs in the same order whatever the split: bit-identical
         np.testing.assert_array_equal(i, outs[0][1])
-        np.testing.assert_allclose(m, outs[0][0], rtol=1e-6, atol=1e-5)
+        np.testing.assert_array_equal(m, outs[0][0])
 
 
 def test_fill_bitexact_vs_reference(c0):
