@@ -60,6 +60,8 @@ SIGNATURES = {
                              _vp]),
     "cdk_search_device": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp,
                                     _vp, _vp]),
+    "cdk_search_device_noalloc": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_int,
+                                            _vp, _vp, _vp, _vp]),
     "cdk_rescore_fp64": (C.c_int, [_vp, C.c_int, C.c_int, _fp, _fp, _fp, _ip, C.c_int, _ip, _fp,
                                    _ip, _dp, _vp]),
     "cdk_fill_ligand_grid": (C.c_int, [C.c_int, C.c_int, _fp, _fp, _fp, _fp, _ip, C.c_int, C.c_int,

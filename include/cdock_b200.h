@@ -84,6 +84,22 @@ int cdk_search_device(cdk_ctx* ctx, int nAtom, int nConf, const float* d_coor,
                       const float* d_charge, const float* d_eps, const int* d_slot, int nQ,
                       const float* d_quats, float* d_minE, int* d_idx, void* stream);
 
+/* cdk_search_device without any device allocation. It has no counterpart in the reference.
+ * For callers that cannot call cudaMalloc when they search (recording into a CUDA graph,
+ * real-time loops that must not hit the allocator, memory owned by a pool): the wave and
+ * table scratch that cdk_search_device grows with cudaMalloc comes instead from one
+ * file-scope device array of CDK_NOALLOC_SCRATCH_BYTES (64 MiB), held by every GPU that loads
+ * the library until exit. Rotations run in waves that fit it; a search whose single rotation
+ * does not fit returns CDK_ERR_UNSUPPORTED. The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress) and must come before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race; serialise them. Same arguments,
+ * results and errors as cdk_search_device. */
+#define CDK_NOALLOC_SCRATCH_BYTES (64u << 20)
+int cdk_search_device_noalloc(cdk_ctx* ctx, int nAtom, int nConf, const float* d_coor,
+                              const float* d_charge, const float* d_eps, const int* d_slot,
+                              int nQ, const float* d_quats, float* d_minE, int* d_idx,
+                              void* stream);
+
 /* FP64 direct re-score of given poses (rotation + translation index) against the resident
  * receptor grids: E = sum_k sum_atoms sum_corners w * P_k(g + t), accumulated in double.
  * Host buffers. rot_conf[i] picks the conformer, quats[i*4..], tidx[i*3..] the translation. */
