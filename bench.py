@@ -208,19 +208,65 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def _kernel_roofline(stats: dict, n: int, K: int, hbm: float, peak_kind: str, traffic: dict):
+    """Roofline of the dominant kernel of the last search: algorithmic bytes per launch (from
+    the library's exact work counters) over its average launch time (events in the timed
+    region)."""
+    ncol = n * (n // 2 + 1)
+    waves = max(1, stats["waves"])
+    km = stats["kernel_ms"]
+    dom = max(km, key=km.get)
+    plane = ncol * 8
+    rot = stats["rotations"]
+    alg = {
+        "xpass": (stats["planes_spread"] + stats["planes_window"]) * plane + waves * K * n * plane,
+        "spread_yz": stats["planes_spread"] * plane,
+        "yz_inv_argmin": stats["planes_window"] * plane,
+        "prep": rot * 1024,
+        "finalize": rot * 32,
+    }
+    per_launch = alg[dom] / waves
+    t = km[dom] / waves / 1e3
+    achieved = per_launch / t / 1e9
+    tr = traffic.get(dom)
+    out = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+           "frac": achieved / hbm, "peak_kind": peak_kind,
+           "traffic": (tr * rot / waves) if tr is not None else None,
+           "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": t * 1e3,
+           "share_of_device_time": km[dom] / max(1e-9, sum(km.values())),
+           "kernel_ms": km}
+    return out
+
+
+def _accuracy_sample(w, e, i, n_sample=24):
+    """Per-rotation errors of a sample of the timed results against the FP64 oracle."""
+    from oracle import oracle as O
+    from tests.parity import rel_err
+    n_rot = e.shape[0]
+    sel = np.linspace(0, n_rot - 1, n_sample).astype(int)
+    q = w.quats.reshape(-1, 4)
+    r64 = np.empty(len(sel))
+    ri = np.empty((len(sel), 3), np.int32)
+    for j, r in enumerate(sel):
+        _, ii, m = O.search_direct(w.grids, w.spacing, w.coor[r // N_Q], w.charge, w.eps, w.slot,
+                                   q[r][None, None], prec=1)
+        r64[j], ri[j] = m[0], ii[0]
+    err = rel_err(e[sel], r64)
+    return {"rotations_checked": int(len(sel)), "max_rel_err_vs_fp64": float(err.max()),
+            "median_rel_err_vs_fp64": float(np.median(err)),
+            "best_translation_agreement": float(np.mean(np.all(i[sel] == ri, axis=1)))}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
-    from cdocker_b200 import Receptor
+    from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP32, Receptor
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     w = make_rank_workload(rank, world)
     n_conf, n_atom = w.coor.shape[0], w.coor.shape[1]
     n_rot = n_conf * N_Q
-    rec = Receptor(w.grids, w.spacing, device=local_rank, wave_rotations=args.wave,
-                   col_tile=args.col_tile, use_graphs=args.graphs)
-    # resident inputs
     d_coor = torch.from_numpy(w.coor).to(dev)
     d_charge = torch.from_numpy(w.charge).to(dev)
     d_eps = torch.from_numpy(w.eps).to(dev)
@@ -230,11 +276,6 @@ def run_ours(args, rank, world, local_rank):
     d_i = torch.empty(n_rot, 3, dtype=torch.int32, device=dev)
     stream = torch.cuda.Stream(device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-
-    def step_device():
-        rec.search_device(n_atom, n_conf, d_coor.data_ptr(), d_charge.data_ptr(),
-                          d_eps.data_ptr(), d_slot.data_ptr(), N_Q, d_q.data_ptr(),
-                          d_e.data_ptr(), d_i.data_ptr(), stream.cuda_stream)
 
     def barrier():
         if world > 1:
@@ -248,32 +289,55 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    for _ in range(args.warmup):
-        step_device()
-    torch.cuda.synchronize(dev)
-    sampler = ClockSampler(local_rank)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
-    barrier()
-    sampler.start()
-    time.sleep(0.3)
-    for s in range(args.steps):
-        with torch.cuda.stream(stream):
-            evs[s][0].record(stream)
-            step_device()
-            evs[s][1].record(stream)
-            flush.fill_(s & 0xff)
-    barrier()
-    clocks = sampler.stop()
-    dev_ms = sum(a.elapsed_time(b) for a, b in evs)
-    dev_ms = max_over_ranks(dev_ms)
-    stats = rec.stats()
-    launches_per_step = stats["launches"]
-    value = world * n_rot * args.steps / (dev_ms / 1e3)
+    def timed_form(form):
+        rec = Receptor(w.grids, w.spacing, device=local_rank, wave_rotations=args.wave,
+                       col_tile=args.col_tile, form=form, profile=True)
 
-    # per-kernel timing of one search on the same stream (events around each launch group are
-    # not available through the C-ABI, so the roofline kernel is timed by the profile pass)
-    # e2e: host buffers through cdk_search, pinned memory, copies inside the timed region
+        def step():
+            rec.search_device(n_atom, n_conf, d_coor.data_ptr(), d_charge.data_ptr(),
+                              d_eps.data_ptr(), d_slot.data_ptr(), N_Q, d_q.data_ptr(),
+                              d_e.data_ptr(), d_i.data_ptr(), stream.cuda_stream)
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize(dev)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        barrier()
+        sampler = ClockSampler(local_rank)
+        sampler.start()
+        time.sleep(0.3)
+        for s in range(args.steps):
+            with torch.cuda.stream(stream):
+                evs[s][0].record(stream)
+                step()
+                evs[s][1].record(stream)
+                flush.fill_(s & 0xff)
+        barrier()
+        clocks = sampler.stop()
+        ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs))
+        stats = rec.stats()
+        e = d_e.cpu().numpy()
+        i = d_i.cpu().numpy()
+        return rec, ms, stats, clocks, e, i
+
+    forms = {}
+    for name, form in (("fp32", CDK_FORM_FP32), ("bf16x3_tensor_core", CDK_FORM_BF16X3)):
+        if args.forms != "both" and args.forms != name:
+            continue
+        rec, ms, stats, clocks, e, i = timed_form(form)
+        acc = _accuracy_sample(w, e, i) if (rank == 0 and not args.no_check) else None
+        forms[name] = {"rec": rec, "ms": ms, "stats": stats, "clocks": clocks, "acc": acc,
+                       "value": world * n_rot * args.steps / (ms / 1e3)}
+    # headline: the fastest form that meets its error bar on the checked sample
+    bars = {"fp32": 1e-4, "bf16x3_tensor_core": 1e-3}
+    ok = [k for k, v in forms.items()
+          if v["acc"] is None or v["acc"]["max_rel_err_vs_fp64"] <= bars[k]]
+    head = max(ok or list(forms), key=lambda k: forms[k]["value"])
+    H = forms[head]
+    rec = H["rec"]
+
+    # e2e through cdk_search with pinned host buffers, copies inside the timed region
     h_coor = torch.from_numpy(w.coor).pin_memory()
     h_q = torch.from_numpy(w.quats).pin_memory()
     h_e = torch.empty(n_rot, dtype=torch.float32).pin_memory()
@@ -310,63 +374,85 @@ def run_ours(args, rank, world, local_rank):
     e2e_val = world * n_rot * args.steps / (e2e_ms / 1e3)
     h2d = w.coor.nbytes + w.quats.nbytes + charge.nbytes + eps.nbytes + slot.nbytes
     d2h = n_rot * 4 + n_rot * 12
-    # correctness spot check of the timed results (rank 0, a few rotations vs the oracle)
-    check = None
-    if rank == 0 and not args.no_check:
-        from oracle import oracle as O
-        sel = np.arange(0, n_rot, max(1, n_rot // 8))[:8]
-        qs = w.quats.reshape(-1, 4)[sel]
-        errs = []
-        for j, r in enumerate(sel):
-            _, ri, r64 = O.search_direct(w.grids, w.spacing, w.coor[r // N_Q], w.charge, w.eps,
-                                         w.slot, qs[j][None, None], prec=1)
-            errs.append(abs(float(h_e[r]) - r64[0]) / max(1.0, abs(r64[0])))
-        check = {"rotations_checked": int(len(sel)), "max_rel_err_vs_fp64": max(errs)}
+
+    serving = None
+    if rank == 0 and args.serve_secs > 0:
+        serving = serving_sample(w, rec, args.serve_secs)
 
     if rank == 0:
         hbm, peak_kind = _peaks()
         nc = 64 * 64 * 33  # half-spectrum points of one grid
         b_rot = 8 * 9 * 64 ** 3 + 16 * 9 * nc + 16 * nc + 8 * 64 ** 3
+        traffic = {}
+        tp = os.path.join(ROOT, "profiles", "dram_bytes_per_rotation.json")
+        if os.path.exists(tp):
+            with open(tp) as f:
+                traffic = json.load(f).get(head, {})
+        value = H["value"]
         rps = value / world
         line = {
             "metric": METRIC, "value": value, "unit": "rotations/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "ms_per_step": H["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if head == "fp32" else "bf16x3 (f32 accumulate)",
+            "data": "synthetic",
             "config": {"workload": "config 1: 64^3 grid at 0.5 A, K=9, 2,500-atom synthetic "
                                    "receptor, 40-atom ligand, 100 conformers x 1,000 "
                                    "quaternions = 1e5 rotations per rank per step",
-                       "form": "fp32", "grid": 64, "K": 9, "rotations_per_step": n_rot * world,
-                       "l2": "256 MiB written between timed steps; per-step scratch "
-                             f"{rec.stats().get('waves', 0)} waves, far above L2",
-                       "wave_rotations": args.wave, "parallelism": f"rotation shards x{world}"},
-            "gpu_launches": int(launches_per_step * args.steps),
-            "clocks": clocks,
+                       "form": head, "grid": 64, "K": 9, "rotations_per_step": n_rot * world,
+                       "l2": "256 MiB written between timed steps (and every step's wave "
+                             "scratch is GBs, far above L2)",
+                       "wave_rotations": H["stats"]["wave_rotations"],
+                       "parallelism": f"rotation shards x{world}"},
+            "gpu_launches": int(H["stats"]["launches"] * args.steps),
+            "clocks": H["clocks"],
             "e2e": {"value": e2e_val, "unit": "rotations/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
+                    "d2h_bytes_per_step": int(d2h), "form": head},
+            "roofline": _kernel_roofline(H["stats"], 64, 9, hbm, peak_kind, traffic),
             "fft_roofline": {"bytes_per_rotation": b_rot, "achieved_gbs": rps * b_rot / 1e9,
                              "peak_gbs": hbm, "frac": rps * b_rot / 1e9 / hbm,
                              "peak_kind": peak_kind,
                              "note": "staged-pipeline algorithmic bytes B_rot = 8KN + 16K*Nc + "
-                                     "16Nc + 8N per rotation, per GPU"},
-            "check": check,
+                                     "16Nc + 8N per rotation (Nc = n*n*(n/2+1)), per GPU"},
+            "forms": {k: {"value": v["value"], "ms_per_step": v["ms"] / args.steps,
+                          "accuracy": v["acc"], "kernel_ms_last_step": v["stats"]["kernel_ms"]}
+                      for k, v in forms.items()},
         }
-        if args.roofline_json and os.path.exists(args.roofline_json):
-            with open(args.roofline_json) as f:
-                line["roofline"] = json.load(f)
+        if serving is not None:
+            line["serving"] = serving
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(w, budget_s=args.cpu_budget)
         if args.ref_cufft:
             line["reference_cufft"] = reference_cufft_sample(w)
         print(json.dumps(line), flush=True)
-    rec.close()
+    for v in forms.values():
+        v["rec"].close()
+
+
+def serving_sample(w, rec_unused, secs: float) -> dict:
+    """Continuous-batching server on the same 64^3 receptor (all 8 vdW grids + elec): Poisson
+    arrivals of requests with ligands of 10-80 atoms, 10-50 conformers, 500-2,000 rotations."""
+    from cdocker_b200 import Receptor, synth
+    from cdocker_b200.serving import Server, make_requests, poisson_arrivals, run_load
+    rate = 40.0
+    arr = poisson_arrivals(rate, secs, seed=7)
+    reqs = make_requests(len(arr), 21, w.spacing, w.length, synth.PROBE_RADII, atoms=(10, 80),
+                         confs=(10, 50), rots=(500, 2000))
+    with Receptor(w.all_grids, w.spacing, max_atoms=128) as r:
+        with Server(r, arena_bytes=512 << 20, wave_rotations=1024, max_atoms=128) as srv:
+            res = run_load(srv, reqs, arr)
+            st = srv.stats()
+    res.update({"rate_hz": rate, "grid": 64, "waves": st["waves"],
+                "request_mix": "ligand U(10,80) atoms, conformers U(10,50), rotations "
+                               "U(500,2000), Poisson arrivals"})
+    return res
 
 
 def profile_run(args):
     """One warm-up and one timed search of `--profile-run` rotations (first conformers of the
     config-1 workload), per-kernel device times from events around every launch."""
     import torch
-    from cdocker_b200 import Receptor
+    from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP32, Receptor
     w = make_rank_workload(0, 1)
     n_q = N_Q
     n_conf = max(1, min(N_CONF, (args.profile_run + n_q - 1) // n_q))
@@ -382,8 +468,9 @@ def profile_run(args):
     e = torch.empty(n_rot, device=dev)
     i = torch.empty(n_rot, 3, dtype=torch.int32, device=dev)
     out = {}
+    form = CDK_FORM_BF16X3 if args.forms == "bf16x3_tensor_core" else CDK_FORM_FP32
     with Receptor(w.grids, w.spacing, wave_rotations=args.wave, col_tile=args.col_tile,
-                  profile=True) as rec:
+                  profile=True, form=form) as rec:
         for it in range(2):
             rec.search_device(w.coor.shape[1], n_conf, coor.data_ptr(), ch.data_ptr(),
                               ep.data_ptr(), sl.data_ptr(), n_q, q.data_ptr(), e.data_ptr(),
@@ -406,7 +493,8 @@ def main():
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--ref-cufft", type=int, default=1)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
-    ap.add_argument("--roofline-json", default="")
+    ap.add_argument("--forms", default="both", choices=["both", "fp32", "bf16x3_tensor_core"])
+    ap.add_argument("--serve-secs", type=float, default=3.0)
     ap.add_argument("--profile-run", type=int, default=0,
                     help="run one search of this many rotations with per-kernel events and "
                          "print the timings (the small case used for ncu captures)")

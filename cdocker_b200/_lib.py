@@ -37,6 +37,18 @@ class CdkOpts(C.Structure):
     ]
 
 
+class CdkServerOpts(C.Structure):
+    _fields_ = [
+        ("arena_bytes", C.c_size_t),
+        ("wave_rotations", C.c_int),
+        ("max_box", C.c_int),
+        ("max_atoms", C.c_int),
+        ("max_conformers", C.c_int),
+        ("max_waiting", C.c_int),
+        ("reserved", C.c_int * 4),
+    ]
+
+
 class CdkError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"cdk error {code}: {msg}")
@@ -78,6 +90,13 @@ SIGNATURES = {
     "cdk_synth_receptor_grids": (C.c_int, [C.c_int, C.c_float, _fp, C.c_int, _fp, _fp, _fp, _fp,
                                            C.c_int, _fp, C.c_float, C.c_float, C.c_float, _fp]),
     "cdk_ctx_stats": (C.c_int, [_vp, _dp, C.c_int]),
+    "cdk_server_opts_default": (None, [C.POINTER(CdkServerOpts)]),
+    "cdk_server_create": (C.c_int, [_vp, C.POINTER(CdkServerOpts), C.POINTER(_vp)]),
+    "cdk_server_submit": (C.c_int, [_vp, C.c_int, C.c_int, _fp, _fp, _fp, _ip, C.c_int, _fp,
+                                    C.POINTER(C.c_uint64)]),
+    "cdk_server_poll": (C.c_int, [_vp, C.c_uint64, C.c_int, _fp, _ip, _dp]),
+    "cdk_server_stats": (C.c_int, [_vp, _dp, C.c_int]),
+    "cdk_server_destroy": (C.c_int, [_vp]),
     "cdk_pose_coordinates": (C.c_int, [C.c_int, _fp, _fp, _dp, C.c_float, _ip, _dp]),
 }
 

@@ -106,6 +106,7 @@ struct cdk_ctx {
   cudaStream_t stream = nullptr;
   float* d_grids = nullptr;   // [K][n^3], kept for the FP64 re-score
   float2* d_phat = nullptr;   // [n][K][ncol]
+  float2* d_ptilde = nullptr; // [ncol][K][n] receptor transformed over (y,z) only, x n (BF16X3 form)
   float2* d_tw = nullptr;     // [n]
   Arena wave;                 // per-wave scratch
   Arena tables;               // per-search tables
@@ -179,6 +180,11 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   a.idx = d_idx;
   a.err_count = reinterpret_cast<int*>(c->d_misc + 2);
   a.col_tile = c->opts.col_tile > 0 ? c->opts.col_tile : pick_col_tile(n, K);
+  const bool tc = c->opts.form == CDK_FORM_BF16X3;
+  if (tc && xpass_tc_smem_bytes(n, K, Lb) > 227 * 1024) {
+    set_error("ligand box too large for the tensor-core x pass at this grid size and K");
+    return CDK_ERR_UNSUPPORTED;
+  }
   if ((n <= 64 ? xpass2_smem_bytes(n, K, a.col_tile) : xpass_smem_bytes(n, K, a.col_tile)) > 227 * 1024 ||
       (n <= 64 && a.col_tile != 8 && a.col_tile != 16)) {
     set_error("column tile must be 8 or 16 for n <= 64 and fit shared memory");
@@ -208,7 +214,8 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     if (prof) CDK_CUDA(cudaEventRecord(ev[1], s));
     CDK_CUDA(launch_spread_yz(a, s));
     if (prof) CDK_CUDA(cudaEventRecord(ev[2], s));
-    CDK_CUDA(launch_xpass(a, s));
+    if (tc) CDK_CUDA(launch_xpass_tc(a, c->d_ptilde, s));
+    else CDK_CUDA(launch_xpass(a, s));
     if (prof) CDK_CUDA(cudaEventRecord(ev[3], s));
     CDK_CUDA(launch_yz_inv_argmin(a, s));
     if (prof) CDK_CUDA(cudaEventRecord(ev[4], s));
@@ -392,9 +399,9 @@ int cdk_ctx_create(int nx, int ny, int nz, float spacing, int K, const float* gr
   if (opts) c->opts = *opts;
   else cdk_opts_default(&c->opts);
   if (c->opts.max_atoms <= 0) c->opts.max_atoms = 256;
-  if (c->opts.form != CDK_FORM_FP32) {
+  if (c->opts.form != CDK_FORM_FP32 && c->opts.form != CDK_FORM_BF16X3) {
     delete c;
-    set_error("only the FP32 form is built in this library");
+    set_error("unknown form");
     return CDK_ERR_UNSUPPORTED;
   }
   c->dev = c->opts.device;
@@ -439,6 +446,10 @@ int cdk_ctx_create(int nx, int ny, int nz, float spacing, int K, const float* gr
   CTX_CUDA(cudaMalloc(&scratch, sizeof(float2) * K * n * ncol));
   cudaError_t e = launch_receptor_fft(n, K, c->d_grids, scratch, c->d_phat, c->d_tw,
                                       pick_col_tile(n, 1), c->stream);
+  if (e == cudaSuccess && c->opts.form == CDK_FORM_BF16X3) {
+    e = cudaMalloc(&c->d_ptilde, sizeof(float2) * K * n * ncol);
+    if (e == cudaSuccess) e = launch_ptilde(n, K, scratch, c->d_ptilde, c->stream);
+  }
   cudaError_t e2 = cudaStreamSynchronize(c->stream);
   cudaFree(scratch);
   CTX_CUDA(e);
@@ -454,6 +465,7 @@ int cdk_ctx_destroy(cdk_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   cudaFree(c->d_grids);
   cudaFree(c->d_phat);
+  cudaFree(c->d_ptilde);
   cudaFree(c->d_tw);
   cudaFree(c->d_misc);
   if (c->h_misc) cudaFreeHost(c->h_misc);

@@ -79,6 +79,9 @@ cudaError_t launch_spread_yz(const WaveArgs& a, cudaStream_t s);
 cudaError_t launch_xpass(const WaveArgs& a, cudaStream_t s);
 cudaError_t launch_yz_inv_argmin(const WaveArgs& a, cudaStream_t s);
 cudaError_t launch_finalize(const WaveArgs& a, cudaStream_t s);
+// Finalize for waves whose rotations belong to different requests: minE goes to
+// ebase[RotDesc.out], the three indices to ibase[RotDesc.pad0 .. +2].
+cudaError_t launch_finalize_server(const WaveArgs& a, float* ebase, int* ibase, cudaStream_t s);
 // Dense forward transform of K receptor grids [K][n][n][n] -> phat [n][K][ncol].
 cudaError_t launch_receptor_fft(int n, int K, const float* grids, float2* scratch,
                                 float2* phat, const float2* tw, int col_tile, cudaStream_t s);
@@ -99,6 +102,11 @@ cudaError_t launch_rescore_fp64(int n, int K, float spacing, const float* grids,
                                 const float* coords, const AtomParam* params,
                                 const ConfDesc* confs, const RotDesc* rots, const int* tidx,
                                 int npose, double* energy, cudaStream_t s);
+
+// Precision form: x pass as a split-BF16 circulant contraction on the tensor cores.
+cudaError_t launch_ptilde(int n, int K, const float2* yz, float2* pt, cudaStream_t s);
+cudaError_t launch_xpass_tc(const WaveArgs& a, const float2* pt, cudaStream_t s);
+size_t xpass_tc_smem_bytes(int n, int K, int Lb);
 
 // Number of kernel launches one wave issues.
 constexpr int kLaunchesPerWave = 5;

@@ -570,6 +570,27 @@ __global__ void k_finalize(WaveArgs a) {
   a.idx[out * 3 + 2] = lin % n;
 }
 
+__global__ void k_finalize_server(WaveArgs a, float* ebase, int* ibase) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= a.nrot) return;
+  const RotDesc rd = a.rots[r];
+  const RotRec* rec = a.rec + r;
+  if (rec->err) atomicAdd(a.err_count, 1);
+  const unsigned long long key = a.keys[r];
+  int* idx = ibase + rd.pad0;
+  if (!rec->valid || key == ~0ull) {
+    ebase[rd.out] = INFINITY;
+    idx[0] = idx[1] = idx[2] = -1;
+    return;
+  }
+  const unsigned int lin = (unsigned int)(key & 0xffffffffu);
+  const int n = a.n;
+  ebase[rd.out] = key_to_float((unsigned int)(key >> 32));
+  idx[0] = lin / (n * n);
+  idx[1] = (lin / n) % n;
+  idx[2] = lin % n;
+}
+
 // ---------------------------------------------------------------------------------------
 // receptor spectra: dense (y,z) forward of every plane, then x forward per column tile
 template <int N>
@@ -746,6 +767,10 @@ cudaError_t launch_yz_inv_argmin(const WaveArgs& a, cudaStream_t s) {
 }
 cudaError_t launch_finalize(const WaveArgs& a, cudaStream_t s) {
   k_finalize<<<(a.nrot + 255) / 256, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t launch_finalize_server(const WaveArgs& a, float* ebase, int* ibase, cudaStream_t s) {
+  k_finalize_server<<<(a.nrot + 255) / 256, 256, 0, s>>>(a, ebase, ibase);
   return cudaGetLastError();
 }
 cudaError_t launch_receptor_fft(int n, int K, const float* grids, float2* scratch,

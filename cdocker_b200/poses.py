@@ -61,3 +61,28 @@ def export_top(out_dir: str, conformer: int, coor, quats, minE, idx, grid_min, s
         if energy_file is not None:
             energy_file.write(f"{name},{conformer},{rank},{float(minE[r]):g}\n")
     return rows
+
+
+def rescore_top(receptor, coor, charge, eps, slot, quats, minE, idx, k: int = 8,
+                batch: int = 1000):
+    """FP64 re-score of the k lowest-energy rotations of every batch of `batch` consecutive
+    rotations (direct trilinear grid-energy sum on the GPU, cdk_rescore_fp64).
+    Returns (indices [n_batches, k] into the rotation list, energies [n_batches, k] float64)."""
+    coor = np.ascontiguousarray(coor, np.float32)
+    if coor.ndim == 2:
+        coor = coor[None]
+    q = np.ascontiguousarray(quats, np.float32).reshape(-1, 4)
+    n_q = q.shape[0] // coor.shape[0]
+    n = q.shape[0]
+    tops, confs, qs, ts = [], [], [], []
+    for b0 in range(0, n, batch):
+        order = sort_index(minE[b0:b0 + batch])[:k] + b0
+        tops.append(order)
+        for r in order:
+            confs.append(r // n_q)
+            qs.append(q[r])
+            ts.append(idx[r])
+    e = receptor.rescore_fp64(coor, charge, eps, slot, np.asarray(confs, np.int32),
+                              np.asarray(qs, np.float32), np.asarray(ts, np.int32))
+    kk = min(k, batch)
+    return np.asarray(tops).reshape(-1, kk), e.reshape(-1, kk)

@@ -173,6 +173,39 @@ int cdk_synth_receptor_grids(int n, float spacing, const float* origin, int nAto
                              const float* charge, int nVdw, const float* probeRadii,
                              float vdwCap, float elecCap, float cutoff, float* out);
 
+/* ---- serving: continuous batching over one resident receptor ----
+ * A server owns a worker thread and a stream on the context's device. Requests (a ligand
+ * with its conformers and rotations) are admitted when their inputs and outputs fit the
+ * server's device arena, in FIFO order; the worker packs the rotations of all admitted
+ * requests into shared waves, so requests that arrive while others run join the next wave.
+ * Results are the same as cdk_search on the request alone. The context must outlive the
+ * server. The reference has no serving layer (it searches one ligand per process run). */
+typedef struct cdk_server cdk_server;
+typedef struct cdk_server_opts {
+  size_t arena_bytes;  /* device memory for request inputs/outputs (admission budget) */
+  int wave_rotations;  /* rotations per shared wave */
+  int max_box;         /* largest ligand box edge (grid cells) a request may need */
+  int max_atoms;       /* largest ligand */
+  int max_conformers;  /* conformer slots across admitted requests */
+  int max_waiting;     /* queued (not yet admitted) requests before submit returns BUSY */
+  int reserved[4];
+} cdk_server_opts;
+void cdk_server_opts_default(cdk_server_opts* opts);
+int cdk_server_create(cdk_ctx* ctx, const cdk_server_opts* opts, cdk_server** out);
+/* Copies the request; returns a ticket. CDK_ERR_BUSY when the wait queue is full. */
+int cdk_server_submit(cdk_server* s, int nAtom, int nConf, const float* coor,
+                      const float* charge, const float* eps, const int* slot, int nQ,
+                      const float* quats, uint64_t* ticket);
+/* Waits up to wait_ms (-1: forever, 0: no wait). CDK_OK: results copied (minE[nConf*nQ],
+ * idx[nConf*nQ][3]) and timing[0..2] = queue, run, total ms; the ticket is then released.
+ * CDK_ERR_BUSY: still running. */
+int cdk_server_poll(cdk_server* s, uint64_t ticket, int wait_ms, float* minE, int* idx,
+                    double* timing);
+/* [0] waves, [1] rotations, [2] kernel launches, [3] completed requests, [4] p50 latency ms,
+ * [5] p99 latency ms, [6] waiting requests, [7] admitted requests in flight. */
+int cdk_server_stats(cdk_server* s, double* out, int n);
+int cdk_server_destroy(cdk_server* s);
+
 /* Counters of the last search on this context (n <= CDK_NSTATS values):
  * [0] kernel launches, [1] waves, [2] rotations, [3] device ms of the search (events on the
  * search stream), [4] planned ligand box edge, [5] rotations per wave, [6] (y,z) planes the

@@ -1,0 +1,54 @@
+"""Precision form (CDK_FORM_BF16X3): the x pass as a split-BF16 circulant contraction on the
+tensor cores. Bar: per-rotation minimum energy within 1e-3 relative of the FP64 oracle (floor
+1 kcal/mol), best translation identical except at near-ties of that tolerance; FP64 re-score
+of the top poses."""
+import numpy as np
+import pytest
+
+from cdocker_b200 import CDK_FORM_BF16X3, Receptor, synth
+from cdocker_b200.poses import rescore_top
+from oracle import oracle as O
+from tests.parity import check_search, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL_TC = 1e-3
+
+
+@pytest.mark.parametrize("name,nconf,nq", [("c0_32", 1, 500), ("c1_64", 4, 25), ("c4_128", 1, 4)])
+def test_tc_form_vs_fp64(name, nconf, nq, grids_cache):
+    w = synth.make_workload(name, seed=5, n_conf=nconf, n_q=nq, grids_cache=grids_cache)
+    with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3) as rec:
+        minE, idx = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+    _, ridx, r64 = O.search_direct(w.grids, w.spacing, w.coor, w.charge, w.eps, w.slot, w.quats,
+                                   prec=1)
+    qq = w.quats.reshape(-1, 4)
+    st = check_search(minE, idx, r64, ridx,
+                      lambda r: O.energy_map(w.grids, w.spacing, w.coor[r // nq], w.charge, w.eps,
+                                             w.slot, qq[r]), rel_tol=TOL_TC)
+    assert st["max_rel"] <= TOL_TC
+
+
+def test_tc_and_fp32_forms_agree(c0):
+    w = c0
+    q = w.quats[:, :200]
+    with Receptor(w.grids, w.spacing) as r32, Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3) as rtc:
+        e32, i32 = r32.search(w.coor, w.charge, w.eps, w.slot, q)
+        etc, itc = rtc.search(w.coor, w.charge, w.eps, w.slot, q)
+    assert rel_err(etc, e32).max() <= TOL_TC
+    assert np.mean(np.all(itc == i32, axis=1)) >= 0.98
+
+
+def test_fp64_rescore_of_top_poses(c0):
+    w = c0
+    q = w.quats[:, :100]
+    with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3) as rec:
+        minE, idx = rec.search(w.coor, w.charge, w.eps, w.slot, q)
+        top, e64 = rescore_top(rec, w.coor, w.charge, w.eps, w.slot, q, minE, idx, k=8,
+                               batch=100)
+    assert top.shape == (1, 8) and e64.shape == (1, 8)
+    qq = q.reshape(-1, 4)
+    for j, r in enumerate(top[0]):
+        emap = O.energy_map(w.grids, w.spacing, w.coor[0], w.charge, w.eps, w.slot, qq[r])
+        ref = emap[tuple(idx[r])]
+        assert abs(e64[0, j] - ref) <= 1e-7 * max(1.0, abs(ref))
