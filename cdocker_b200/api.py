@@ -128,7 +128,8 @@ class Receptor:
 
     def __init__(self, grids, spacing: float, device: int = 0, wave_rotations: int = 0,
                  max_atoms: int = 256, col_tile: int = 0, form: int = L.CDK_FORM_FP32,
-                 use_graphs: int = 0, profile: bool = False):
+                 use_graphs: int = 0, profile: bool = False, fft_planes: bool = False,
+                 autotune: bool = False):
         g = _f32(grids)
         if g.ndim != 4:
             raise ValueError("grids must be [K, n, n, n]")
@@ -144,6 +145,8 @@ class Receptor:
         opts.col_tile = col_tile
         opts.use_graphs = use_graphs
         opts.reserved[0] = 1 if profile else 0
+        opts.reserved[1] = 1 if fft_planes else 0
+        opts.reserved[2] = 1 if autotune else 0
         h = C.c_void_p()
         L.check(lib.cdk_ctx_create(g.shape[1], g.shape[2], g.shape[3], self.spacing, self.K,
                                    _pf(g), C.byref(opts), C.byref(h)))
@@ -217,4 +220,6 @@ class Receptor:
         return {"launches": int(out[0]), "waves": int(out[1]), "rotations": int(out[2]),
                 "device_ms": float(out[3]), "box": int(out[4]), "wave_rotations": int(out[5]),
                 "planes_spread": int(out[6]), "planes_window": int(out[7]),
-                "kernel_ms": {k: float(v) for k, v in zip(names, out[8:13])}}
+                "kernel_ms": {k: float(v) for k, v in zip(names, out[8:13])},
+                "col_tile": int(out[13]), "rotations_per_cta": int(out[14]),
+                "graph_state": int(out[15])}

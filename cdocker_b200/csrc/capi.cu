@@ -108,6 +108,7 @@ struct cdk_ctx {
   float2* d_phat = nullptr;   // [n][K][ncol]
   float2* d_ptilde = nullptr; // [ncol][K][n] receptor transformed over (y,z) only, x n (BF16X3 form)
   float2* d_tw = nullptr;     // [n]
+  int* d_kyof = nullptr;      // [n] natural frequency at each digit-reversed position
   Arena wave;                 // per-wave scratch
   Arena tables;               // per-search tables
   Arena io;                   // staging of host-buffer searches
@@ -119,6 +120,23 @@ struct cdk_ctx {
   // per-kernel timing (opts.reserved[0] != 0): events around every launch of every wave
   std::vector<cudaEvent_t> kev;
   int kev_used = 0;
+  // CUDA graph of the last search shape (opts.use_graphs)
+  struct GraphKey {
+    const void* p[7];
+    int nAtom, nConf, nQ, Lb;
+    cudaStream_t s;
+    bool operator==(const GraphKey& o) const {
+      for (int i = 0; i < 7; ++i)
+        if (p[i] != o.p[i]) return false;
+      return nAtom == o.nAtom && nConf == o.nConf && nQ == o.nQ && Lb == o.Lb && s == o.s;
+    }
+  } gkey{};
+  int gkey_seen = 0;  // 1 after one plain run with gkey, 2 once the graph exists
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  // autotuned x-pass configuration (opts.reserved[2] = 1), per (Lb)
+  int tuned_Lb = -1, tuned_col_tile = 0, tuned_chunk = 0;
+  double tune_ms[8] = {};
   double stats[CDK_NSTATS] = {};
 };
 
@@ -134,6 +152,64 @@ namespace {
   } while (0)
 
 bool supported_n(int n) { return n == 32 || n == 64 || n == 96 || n == 128; }
+
+// Times the x pass (the dominant kernel) on the search's first wave under each candidate
+// configuration -- column tile and rotations per CTA for the FP32 form, rotations per CTA for
+// the tensor-core form -- and keeps the fastest for this ligand box. The candidates all compute
+// the same numbers (deterministic kernels), so the timing runs leave no trace in the results.
+int autotune_xpass(cdk_ctx* c, WaveArgs a, const RotDesc* d_rots, long nRot, int wave, bool tc,
+                   cudaStream_t s) {
+  a.nrot = (int)std::min<long>(wave, nRot);
+  a.rots = d_rots;
+  CDK_CUDA(launch_prep(a, s));
+  CDK_CUDA(launch_spread_yz(a, s));
+  struct Cand { int ct, chunk; };
+  std::vector<Cand> cands;
+  if (tc) {
+    for (int ch : {32, 64, 128, 256}) cands.push_back({a.col_tile, ch});
+  } else if (c->n <= 64) {
+    for (int ct : {16, 8})
+      for (int ch : {16, 32, 64}) {
+        if (xpass2_smem_bytes(c->n, c->K, ct) > 227 * 1024) continue;
+        cands.push_back({ct, ch});
+      }
+  } else {
+    cands.push_back({a.col_tile, 0});
+  }
+  cudaEvent_t e0, e1;
+  CDK_CUDA(cudaEventCreate(&e0));
+  CDK_CUDA(cudaEventCreate(&e1));
+  double best = 1e30;
+  Cand pick = cands[0];
+  int i = 0;
+  for (const Cand& cd : cands) {
+    WaveArgs t = a;
+    t.col_tile = cd.ct;
+    t.chunk = cd.chunk;
+    float ms = 0.f, total = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {
+      CDK_CUDA(cudaEventRecord(e0, s));
+      if (tc) CDK_CUDA(launch_xpass_tc(t, c->d_ptilde, s));
+      else CDK_CUDA(launch_xpass(t, s));
+      CDK_CUDA(cudaEventRecord(e1, s));
+      CDK_CUDA(cudaEventSynchronize(e1));
+      CDK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (rep == 1) total = ms;  // second run: warm caches
+    }
+    if (i < 8) c->tune_ms[i] = total;
+    ++i;
+    if (total < best) {
+      best = total;
+      pick = cd;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->tuned_Lb = a.Lb;
+  c->tuned_col_tile = pick.ct;
+  c->tuned_chunk = pick.chunk;
+  return CDK_OK;
+}
 
 // the search proper on device tables; nRot rotations, outputs indexed by RotDesc.out
 int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const ConfDesc* d_confs,
@@ -180,6 +256,12 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   a.idx = d_idx;
   a.err_count = reinterpret_cast<int*>(c->d_misc + 2);
   a.col_tile = c->opts.col_tile > 0 ? c->opts.col_tile : pick_col_tile(n, K);
+  a.kyof = (c->opts.reserved[1] == 0) ? c->d_kyof : nullptr;  // reserved[1] = 1: FFT planes
+  a.chunk = 0;
+  if (c->tuned_Lb == Lb) {
+    if (c->tuned_col_tile) a.col_tile = c->tuned_col_tile;
+    a.chunk = c->tuned_chunk;
+  }
   const bool tc = c->opts.form == CDK_FORM_BF16X3;
   if (tc && xpass_tc_smem_bytes(n, K, Lb) > 227 * 1024) {
     set_error("ligand box too large for the tensor-core x pass at this grid size and K");
@@ -204,6 +286,12 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     }
   }
   c->kev_used = 0;
+  if (c->opts.reserved[2] && c->tuned_Lb != Lb) {
+    int rc = autotune_xpass(c, a, d_rots, nRot, wave, tc, s);
+    if (rc) return rc;
+    a.col_tile = c->tuned_col_tile ? c->tuned_col_tile : a.col_tile;
+    a.chunk = c->tuned_chunk;
+  }
   long launches = 1, waves = 0;
   for (long r0 = 0; r0 < nRot; r0 += wave) {
     a.nrot = (int)std::min<long>(wave, nRot - r0);
@@ -230,6 +318,9 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   c->stats[2] = (double)nRot;
   c->stats[4] = (double)Lb;
   c->stats[5] = (double)wave;
+  c->stats[13] = (double)a.col_tile;
+  c->stats[14] = (double)(a.chunk > 0 ? a.chunk : (tc ? 64 : 32));
+  c->stats[15] = (double)(c->gkey_seen);
   return CDK_OK;
 }
 
@@ -298,11 +389,50 @@ int search_device_impl(cdk_ctx* c, int nAtom, int nConf, const float* d_coor,
   AtomParam* params = reinterpret_cast<AtomParam*>(tb + b_conf + b_rot);
   CDK_CUDA(cudaEventRecord(c->ev0, s));
   const long tmax = std::max<long>(nRot, std::max(nConf, nAtom));
+  // CUDA graph: the first search of a shape runs plainly (growing the scratch), the second
+  // captures build-tables + every wave into one graph, later ones replay it
+  cdk_ctx::GraphKey key{{d_coor, d_charge, d_eps, d_slot, d_quats, d_minE, d_idx}, nAtom, nConf, nQ, Lb, s};
+  const bool graphs = c->opts.use_graphs != 0 && !(c->opts.reserved[2] && c->tuned_Lb != Lb);
+  if (graphs && c->gkey_seen == 2 && c->gkey == key) {
+    CDK_CUDA(cudaGraphLaunch(c->gexec, s));
+    CDK_CUDA(cudaEventRecord(c->ev1, s));
+    return CDK_OK;
+  }
+  const bool capture = graphs && c->gkey_seen == 1 && c->gkey == key;
+  if (capture) CDK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   k_build_tables<<<(unsigned)((tmax + 255) / 256), 256, 0, s>>>(
       nAtom, nConf, nQ, d_quats, d_charge, d_eps, d_slot, confs, rots, params);
-  CDK_CUDA(cudaGetLastError());
-  rc = run_waves(c, d_coor, params, confs, rots, nRot, nAtom, Lb, d_minE, d_idx, s);
-  if (rc) return rc;
+  cudaError_t le = cudaGetLastError();
+  rc = (le == cudaSuccess) ? run_waves(c, d_coor, params, confs, rots, nRot, nAtom, Lb, d_minE, d_idx, s)
+                           : CDK_ERR_CUDA;
+  if (capture) {
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(s, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ce != cudaSuccess) {
+      set_error(std::string("graph capture: ") + cudaGetErrorString(ce));
+      return CDK_ERR_CUDA;
+    }
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->graph = g;
+    CDK_CUDA(cudaGraphInstantiate(&c->gexec, g, 0));
+    CDK_CUDA(cudaGraphLaunch(c->gexec, s));
+    c->gkey_seen = 2;
+  } else {
+    if (rc) return rc;
+    if (graphs) {
+      c->gkey = key;
+      c->gkey_seen = 1;
+    }
+  }
+  if (le != cudaSuccess) {
+    set_error(std::string("k_build_tables: ") + cudaGetErrorString(le));
+    return CDK_ERR_CUDA;
+  }
   CDK_CUDA(cudaEventRecord(c->ev1, s));
   return CDK_OK;
 }
@@ -345,6 +475,7 @@ bool ctx_view(const cdk_ctx* c, CtxView* v) {
   v->max_atoms = c->opts.max_atoms;
   v->phat = c->d_phat;
   v->tw = c->d_tw;
+  v->kyof = (c->opts.reserved[1] == 0) ? c->d_kyof : nullptr;
   v->h_misc = c->h_misc;
   v->stream = c->stream;
   return true;
@@ -440,6 +571,12 @@ int cdk_ctx_create(int nx, int ny, int nz, float spacing, int K, const float* gr
   }
   CTX_CUDA(cudaMemcpyAsync(c->d_tw, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice,
                            c->stream));
+  {
+    std::vector<int> kyof(n);
+    for (int k = 0; k < n; ++k) kyof[fft_position(n, k)] = k;
+    CTX_CUDA(cudaMalloc(&c->d_kyof, sizeof(int) * n));
+    CTX_CUDA(cudaMemcpy(c->d_kyof, kyof.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  }
   CTX_CUDA(cudaMemcpyAsync(c->d_grids, grids, sizeof(float) * K * N, cudaMemcpyHostToDevice,
                            c->stream));
   float2* scratch = nullptr;
@@ -467,11 +604,14 @@ int cdk_ctx_destroy(cdk_ctx* c) {
   cudaFree(c->d_phat);
   cudaFree(c->d_ptilde);
   cudaFree(c->d_tw);
+  cudaFree(c->d_kyof);
   cudaFree(c->d_misc);
   if (c->h_misc) cudaFreeHost(c->h_misc);
   cudaFree(c->d_work);
   if (c->h_work) cudaFreeHost(c->h_work);
   for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  if (c->graph) cudaGraphDestroy(c->graph);
   cudaFree(c->wave.base);
   cudaFree(c->tables.base);
   cudaFree(c->io.base);

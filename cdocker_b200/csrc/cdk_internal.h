@@ -71,6 +71,9 @@ struct WaveArgs {
   int* err_count;
   unsigned long long* work;  // [0] x planes spread, [1] window planes (work counters)
   int col_tile;
+  int chunk;                 // rotations per CTA in the x pass (0 = default)
+  const int* kyof;           // [n] natural frequency at each digit-reversed position; when set
+                             // (and ligands have <= 96 atoms) planes are evaluated directly
 };
 
 // Launchers (stream-ordered, no synchronisation). Return cudaError_t of the launch.
@@ -108,6 +111,9 @@ cudaError_t launch_ptilde(int n, int K, const float2* yz, float2* pt, cudaStream
 cudaError_t launch_xpass_tc(const WaveArgs& a, const float2* pt, cudaStream_t s);
 size_t xpass_tc_smem_bytes(int n, int K, int Lb);
 
+// Digit-reversed position of natural frequency k for the radix plan of length n.
+int fft_position(int n, int k);
+
 // Number of kernel launches one wave issues.
 constexpr int kLaunchesPerWave = 5;
 
@@ -120,6 +126,7 @@ struct CtxView {
   int col_tile_opt, max_atoms;
   const float2* phat;
   const float2* tw;
+  const int* kyof;
   unsigned int* h_misc;  // pinned host scratch of the context (4 words)
   cudaStream_t stream;
 };

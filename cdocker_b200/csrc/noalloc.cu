@@ -223,6 +223,7 @@ extern "C" int cdk_search_device_noalloc(cdk_ctx* ctx, int nAtom, int nConf,
   a.err_count = reinterpret_cast<int*>(misc + 2);
   a.work = reinterpret_cast<unsigned long long*>(misc + 4);
   a.col_tile = v.col_tile_opt > 0 ? v.col_tile_opt : pick_col_tile(n, K);
+  a.kyof = v.kyof;
   for (long r0 = 0; r0 < nRot; r0 += wave) {
     a.nrot = (int)std::min<long>(wave, nRot - r0);
     a.rots = rots;

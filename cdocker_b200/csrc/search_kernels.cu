@@ -265,6 +265,127 @@ __global__ void __launch_bounds__(256) k_spread_yz(WaveArgs a) {
 }
 
 // ---------------------------------------------------------------------------------------
+// Direct (y,z) spectrum of the spread planes of one (rotation, channel).
+// The spread is a sum of separable cloud-in-cell kernels, so the 2-D DFT of plane x is
+//   A(x, ky, kz) = sum_{atoms a touching x} s_a wx_a(x) Fy_a(ky) Fz_a(kz),
+//   Fy_a(ky) = (1 - ry) w^(yi ky) + ry w^((yi+1) ky),   w = exp(-2 pi i / n)
+// (the same numbers the spread + radix FFT produce, without the float rounding of the plane).
+// CTA per (rotation, channel): per-atom factor tables in shared memory, then every touched
+// plane's n*(n/2+1) outputs, written in the (ky position, kz) order of the FFT path.
+// Atoms are visited per plane in ascending order: deterministic.
+constexpr int kDirectMaxAtoms = 96;
+
+template <int N>
+__global__ void __launch_bounds__(256) k_spread_yz_direct(WaveArgs a, const int* __restrict__ kyof,
+                                                           int cap) {
+  constexpr int NZH = N / 2 + 1;
+  constexpr int NCOL = N * NZH;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tw = reinterpret_cast<float2*>(smem_raw);          // [N]
+  float2* Fy = tw + N;                                        // [cap][N] by ky position
+  float2* Fz = Fy + (size_t)cap * N;                          // [cap][NZH]
+  int* s_list = reinterpret_cast<int*>(Fz + (size_t)cap * NZH);  // [2*cap]
+  float* s_w = reinterpret_cast<float*>(s_list + 2 * cap);       // [2*cap]
+  int* s_start = reinterpret_cast<int*>(s_w + 2 * cap);          // [N+2]
+  int* s_atom = s_start + N + 2;                                 // [cap]
+  __shared__ int s_cnt;
+  const int k = blockIdx.x, r = blockIdx.y;
+  const RotRec* rec = a.rec + r;
+  if (!rec->valid) return;
+  const int xlo = rec->xlo[k], xhi = rec->xhi[k];
+  if (xlo > xhi) return;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  for (int i = tid; i < N; i += nthr) tw[i] = a.tw[i];
+  const RotDesc rd = a.rots[r];
+  const ConfDesc cd = a.confs[rd.conf];
+  const AtomParam* prm = a.params + cd.param_off;
+  const float mn0 = rec->mn[0], mn1 = rec->mn[1], mn2 = rec->mn[2];
+  const float h = a.spacing;
+  const bool elec = (k == a.K - 1);
+  const int nA = rec->nA;
+  // channel atoms in ascending order (warp 0, ballot compaction)
+  if (tid < 32) {
+    int cnt = 0;
+    for (int base = 0; base < nA; base += 32) {
+      const int i = base + tid;
+      const bool in = i < nA && (elec || prm[i].slot == k);
+      const unsigned int m = __ballot_sync(0xffffffffu, in);
+      if (in) s_atom[cnt + __popc(m & ((1u << tid) - 1))] = i;
+      cnt += __popc(m);
+    }
+    if (tid == 0) s_cnt = cnt;
+  }
+  __syncthreads();
+  const int na = s_cnt;
+  // factor tables; the per-plane lists (thread 0, ascending atom order)
+  for (int i = tid; i < na * (N + NZH); i += nthr) {
+    const int j = i / (N + NZH), f = i - j * (N + NZH);
+    const int at = s_atom[j];
+    const float4 p = a.rot_xyz[(size_t)r * a.max_atoms + at];
+    if (f < N) {
+      const int yi = cell_of(p.y, mn1, h);
+      const float ry = (float)ratio_of(p.y, mn1, h, yi);
+      const int ky = kyof[f];  // natural frequency of position f
+      const float2 w0 = tw[(yi * ky) % N], w1 = tw[((yi + 1) * ky) % N];
+      Fy[(size_t)j * N + f] = make_float2((1.f - ry) * w0.x + ry * w1.x, (1.f - ry) * w0.y + ry * w1.y);
+    } else {
+      const int kz = f - N;
+      const int zi = cell_of(p.z, mn2, h);
+      const float rz = (float)ratio_of(p.z, mn2, h, zi);
+      const float2 w0 = tw[(zi * kz) % N], w1 = tw[((zi + 1) * kz) % N];
+      Fz[(size_t)j * NZH + kz] = make_float2((1.f - rz) * w0.x + rz * w1.x, (1.f - rz) * w0.y + rz * w1.y);
+    }
+  }
+  if (tid == 0) {
+    // counting sort of (plane, atom) entries by plane; atoms stay in ascending order
+    for (int x = 0; x <= N; ++x) s_start[x] = 0;
+    for (int j = 0; j < na; ++j) {
+      const int xi = cell_of(a.rot_xyz[(size_t)r * a.max_atoms + s_atom[j]].x, mn0, h);
+      s_start[xi + 1]++;
+      if (xi + 1 < N) s_start[xi + 2]++;
+    }
+    for (int x = 0; x < N; ++x) s_start[x + 1] += s_start[x];
+    for (int j = 0; j < na; ++j) {
+      const int at = s_atom[j];
+      const float4 p = a.rot_xyz[(size_t)r * a.max_atoms + at];
+      const int xi = cell_of(p.x, mn0, h);
+      const double xr = ratio_of(p.x, mn0, h, xi);
+      const double sc = elec ? (double)prm[at].charge : (double)prm[at].w_vdw;
+      // s_start[x] is advanced as entries land; rebuilt below
+      const int e0 = s_start[xi]++;
+      s_list[e0] = j;
+      s_w[e0] = (float)(sc * (1.0 - xr));
+      if (xi + 1 < N) {
+        const int e1 = s_start[xi + 1]++;
+        s_list[e1] = j;
+        s_w[e1] = (float)(sc * xr);
+      }
+    }
+    // s_start[x] now holds the end of plane x; shift back to starts
+    for (int x = N; x > 0; --x) s_start[x] = s_start[x - 1];
+    s_start[0] = 0;
+  }
+  __syncthreads();
+  for (int x = xlo; x <= xhi; ++x) {
+    const int e0 = s_start[x], e1 = s_start[x + 1];
+    float2* dst = a.A + (((size_t)r * a.K + k) * a.Lb + x) * NCOL;
+    for (int c = tid; c < NCOL; c += nthr) {
+      const int kyp = c / NZH, kz = c - kyp * NZH;
+      float accx = 0.f, accy = 0.f;
+      for (int e = e0; e < e1; ++e) {
+        const int j = s_list[e];
+        const float wv = s_w[e];
+        const float2 fy = Fy[(size_t)j * N + kyp];
+        const float2 fz = Fz[(size_t)j * NZH + kz];
+        accx += wv * (fy.x * fz.x - fy.y * fz.y);
+        accy += wv * (fy.x * fz.y + fy.y * fz.x);
+      }
+      dst[c] = make_float2(accx, accy);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
 // x pass: forward along x, conj-multiply-sum with the receptor spectra, inverse along x.
 // CTA = one tile of `ct` spectral columns x a contiguous chunk of rotations.
 template <int N>
@@ -646,7 +767,21 @@ constexpr size_t plane_smem() {
 }
 
 template <int N>
+size_t direct_smem(int cap) {
+  return sizeof(float2) * (N + (size_t)cap * (N + N / 2 + 1)) + sizeof(int) * 2 * cap +
+         sizeof(float) * 2 * cap + sizeof(int) * (N + 2 + cap);
+}
+
+template <int N>
 cudaError_t launch_spread_yz_t(const WaveArgs& a, cudaStream_t s) {
+  if (a.kyof && a.max_atoms <= kDirectMaxAtoms) {
+    const int cap = a.max_atoms;
+    const size_t sm = direct_smem<N>(cap);
+    cudaError_t e = cudaFuncSetAttribute(k_spread_yz_direct<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_spread_yz_direct<N><<<dim3(a.K, a.nrot), 256, sm, s>>>(a, a.kyof, cap);
+    return cudaGetLastError();
+  }
   const size_t sm = plane_smem<N>();
   cudaError_t e = cudaFuncSetAttribute(k_spread_yz<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
@@ -678,7 +813,7 @@ cudaError_t launch_xpass_t(const WaveArgs& a, cudaStream_t s) {
     constexpr int CT = 16;
     if (a.col_tile != CT && a.col_tile != 8) return cudaErrorInvalidValue;
     const size_t sm = xpass2_smem_bytes(N, a.K, a.col_tile);
-    const int per = 32;
+    const int per = a.chunk > 0 ? a.chunk : 32;
     const int chunks = (a.nrot + per - 1) / per;
     if (a.col_tile == CT) {
       cudaError_t e = cudaFuncSetAttribute(k_xpass2<N, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -721,6 +856,16 @@ cudaError_t launch_receptor_t(int K, const float* grids, float2* scratch, float2
 }
 
 }  // namespace
+
+int fft_position(int n, int k) {
+  switch (n) {
+    case 32: return fft_pos<32>(k);
+    case 64: return fft_pos<64>(k);
+    case 96: return fft_pos<96>(k);
+    case 128: return fft_pos<128>(k);
+    default: return k;
+  }
+}
 
 size_t xpass2_smem_bytes(int n, int K, int col_tile) {
   return sizeof(float2) * n + sizeof(int) * 2 * KMAX + sizeof(short) * 4 * KMAX +

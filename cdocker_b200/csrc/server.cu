@@ -273,6 +273,7 @@ void worker_loop(cdk_server* s) {
   a.err_count = reinterpret_cast<int*>(s->d_misc);
   a.work = reinterpret_cast<unsigned long long*>(s->d_misc + 2);
   a.col_tile = s->v.col_tile_opt > 0 ? s->v.col_tile_opt : pick_col_tile(n, K);
+  a.kyof = s->v.kyof;
   a.minE = nullptr;
   a.idx = nullptr;
   int cur = 0;

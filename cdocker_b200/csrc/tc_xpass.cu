@@ -140,33 +140,60 @@ __global__ void __launch_bounds__(256, 2) k_xpass_tc(WaveArgs a, const float2* _
       __syncthreads();
       // skip a channel no rotation of the group touches (uniform across the CTA)
       bool any = false;
-      for (int rr = 0; rr < TC_R; ++rr) any |= (s_rng[2 * rr] <= s_rng[2 * rr + 1]);
+      int s_wmax = 0;
+      for (int rr = 0; rr < TC_R; ++rr) {
+        any |= (s_rng[2 * rr] <= s_rng[2 * rr + 1]);
+        s_wmax = max(s_wmax, s_meta[rr]);
+      }
       if (!any) continue;
-      // ---- stage the ligand operand: rotations x x-planes x columns of channel k
-      for (int i = tid; i < TC_R * Lp * TC_CT; i += blockDim.x) {
-        const int c = i % TC_CT;
-        const int t = i / TC_CT;
-        const int x = t % Lp;
-        const int rr = t / Lp;
-        float2 v = make_float2(0.f, 0.f);
-        if (rr < nr && x >= s_rng[2 * rr] && x <= s_rng[2 * rr + 1])
-          v = a.A[(((size_t)(r0 + rr) * K + k) * a.Lb + x) * NCOL + c0 + c];
-        __nv_bfloat16 arh, arl, aih, ail, naih, nail;
-        split_bf16(v.x, arh, arl);
-        split_bf16(v.y, aih, ail);
-        split_bf16(-v.y, naih, nail);
-        // rows n = 2rr (re out): [x] = ar, [Lp + x] = ai ; n = 2rr+1 (im out): [x] = -ai, [Lp+x] = ar
-        unsigned short* bh = bop + ((size_t)(0 * TC_CT + c) * 2 * TC_R) * KS;
-        unsigned short* bl = bop + ((size_t)(1 * TC_CT + c) * 2 * TC_R) * KS;
-        const size_t n0 = (size_t)(2 * rr) * KS, n1 = (size_t)(2 * rr + 1) * KS;
-        bh[n0 + x] = __bfloat16_as_ushort(arh);
-        bl[n0 + x] = __bfloat16_as_ushort(arl);
-        bh[n0 + Lp + x] = __bfloat16_as_ushort(aih);
-        bl[n0 + Lp + x] = __bfloat16_as_ushort(ail);
-        bh[n1 + x] = __bfloat16_as_ushort(naih);
-        bl[n1 + x] = __bfloat16_as_ushort(nail);
-        bh[n1 + Lp + x] = __bfloat16_as_ushort(arh);
-        bl[n1 + Lp + x] = __bfloat16_as_ushort(arl);
+      // ---- stage the ligand operand: rotations x x-planes x columns of channel k.
+      // Thread = (rotation, pair of x planes): two 32-byte rows of A (the CTA's 4 columns) in
+      // four 16-byte loads, then one 32-bit word (x, x+1) per column, slot and hi/lo.
+      for (int i = tid; i < TC_R * (Lp / 2); i += blockDim.x) {
+        const int x2 = i % (Lp / 2);
+        const int rr = i / (Lp / 2);
+        const int x = 2 * x2;
+        float4 v[2][2];
+#pragma unroll
+        for (int d = 0; d < 2; ++d) {
+          const bool in = rr < nr && x + d >= s_rng[2 * rr] && x + d <= s_rng[2 * rr + 1];
+          if (in) {
+            const float4* src = reinterpret_cast<const float4*>(
+                a.A + (((size_t)(r0 + rr) * K + k) * a.Lb + x + d) * NCOL + c0);
+            v[d][0] = src[0];
+            v[d][1] = src[1];
+          } else {
+            v[d][0] = v[d][1] = make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < TC_CT; ++c) {
+          // column c of plane x+d: (re, im)
+          const float re0 = (c & 1) ? v[0][c >> 1].z : v[0][c >> 1].x;
+          const float im0 = (c & 1) ? v[0][c >> 1].w : v[0][c >> 1].y;
+          const float re1 = (c & 1) ? v[1][c >> 1].z : v[1][c >> 1].x;
+          const float im1 = (c & 1) ? v[1][c >> 1].w : v[1][c >> 1].y;
+          __nv_bfloat16 rh0, rl0, rh1, rl1, ih0, il0, ih1, il1, nh0, nl0, nh1, nl1;
+          split_bf16(re0, rh0, rl0);
+          split_bf16(re1, rh1, rl1);
+          split_bf16(im0, ih0, il0);
+          split_bf16(im1, ih1, il1);
+          split_bf16(-im0, nh0, nl0);
+          split_bf16(-im1, nh1, nl1);
+          // rows n = 2rr (re out): [x] = ar, [Lp + x] = ai ; n = 2rr+1 (im out): [x] = -ai, [Lp+x] = ar
+          unsigned int* bh = reinterpret_cast<unsigned int*>(bop + ((size_t)(0 * TC_CT + c) * 2 * TC_R) * KS);
+          unsigned int* bl = reinterpret_cast<unsigned int*>(bop + ((size_t)(1 * TC_CT + c) * 2 * TC_R) * KS);
+          const size_t n0 = (size_t)(2 * rr) * (KS / 2), n1 = (size_t)(2 * rr + 1) * (KS / 2);
+          const int xw = x2, xwi = (Lp / 2) + x2;
+          bh[n0 + xw] = pack2(rh0, rh1);
+          bl[n0 + xw] = pack2(rl0, rl1);
+          bh[n0 + xwi] = pack2(ih0, ih1);
+          bl[n0 + xwi] = pack2(il0, il1);
+          bh[n1 + xw] = pack2(nh0, nh1);
+          bl[n1 + xw] = pack2(nl0, nl1);
+          bh[n1 + xwi] = pack2(rh0, rh1);
+          bl[n1 + xwi] = pack2(rl0, rl1);
+        }
       }
       __syncthreads();
       // ---- MMAs: this warp's column, its m-tiles, 4 n-tiles, all k-steps of channel k
@@ -193,6 +220,7 @@ __global__ void __launch_bounds__(256, 2) k_xpass_tc(WaveArgs a, const float2* _
         }
 #pragma unroll
         for (int m = 0; m < MTW; ++m) {
+          if ((mh * MTW + m) * 16 >= s_wmax) continue;  // rows past every window of the group
           const int row = (mh * MTW + m) * 16 + g;  // x' of a0/a2; +8 for a1/a3
           const unsigned int ah0 = qa_h[xa + row], ah1 = qa_h[xa + row + 8];
           const unsigned int ah2 = qb_h[xb + row], ah3 = qb_h[xb + row + 8];
@@ -234,7 +262,7 @@ cudaError_t launch_tc_t(const WaveArgs& a, const float2* pt, cudaStream_t s) {
   const size_t sm = xpass_tc_smem_bytes(N, a.K, a.Lb);
   cudaError_t e = cudaFuncSetAttribute(k_xpass_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  const int per = 64;
+  const int per = a.chunk > 0 ? ((a.chunk + 15) / 16) * 16 : 64;
   const int chunks = (a.nrot + per - 1) / per;
   k_xpass_tc<N><<<dim3(NCOL / TC_CT, chunks), 32 * TC_WARPS, sm, s>>>(a, pt, Lp, per);
   return cudaGetLastError();

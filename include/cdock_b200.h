@@ -48,7 +48,10 @@ typedef struct cdk_opts {
   int max_atoms;       /* largest ligand (atoms) this context will see; 0 = 256 */
   int col_tile;        /* spectral columns per CTA in the x pass; 0 = autotuned default */
   int use_graphs;      /* 1 = replay each wave through a captured CUDA graph */
-  int reserved[8];     /* [0] = 1: time every kernel with events (cdk_ctx_stats [8..12]) */
+  int reserved[8];     /* [0] = 1: time every kernel with events (cdk_ctx_stats [8..12]);
+                          [1] = 1: spread planes through the radix FFT instead of the direct
+                          separable evaluation; [2] = 1: autotune the x pass on the first wave
+                          of each new ligand box */
 } cdk_opts;
 
 /* Library version string. */
@@ -211,7 +214,8 @@ int cdk_server_destroy(cdk_server* s);
  * search stream), [4] planned ligand box edge, [5] rotations per wave, [6] (y,z) planes the
  * spread kernel transformed, [7] window planes the x pass wrote, [8..12] device ms per kernel
  * kind (prep, spread_yz, xpass, yz_inv_argmin, finalize) when the context was created with
- * opts.reserved[0] = 1 (events around every launch), else 0. */
+ * opts.reserved[0] = 1 (events around every launch), else 0; [13] x-pass column tile,
+ * [14] x-pass rotations per CTA, [15] graph state (0 off, 1 shape seen, 2 replaying). */
 #define CDK_NSTATS 16
 int cdk_ctx_stats(cdk_ctx* ctx, double* out, int n);
 

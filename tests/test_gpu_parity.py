@@ -115,3 +115,60 @@ def test_rescore_fp64_matches_oracle_map(c0):
         # weights in double, so the two differ by float rounding of the weights (~1e-8)
         assert abs(e64[r] - ref) <= 1e-7 * max(1.0, abs(ref))
         assert abs(e64[r] - minE[r]) <= 1e-4 * max(1.0, abs(ref))
+
+
+def test_direct_planes_match_fft_planes(grids_cache):
+    """The direct separable plane spectrum and the spread + radix-FFT planes agree."""
+    w = synth.make_workload("c1_64", seed=6, n_conf=2, n_q=32, grids_cache=grids_cache)
+    with Receptor(w.grids, w.spacing) as rd, Receptor(w.grids, w.spacing, fft_planes=True) as rf:
+        e1, i1 = rd.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+        e2, i2 = rf.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+    from tests.parity import rel_err
+    assert rel_err(e1, e2).max() <= 1e-5
+    assert np.mean(np.all(i1 == i2, axis=1)) >= 0.98
+
+
+def _device_search(rec, w, torch, reps):
+    dev = torch.device("cuda", 0)
+    t = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev)
+         for k, v in (("coor", w.coor), ("charge", w.charge), ("eps", w.eps), ("slot", w.slot),
+                      ("quats", w.quats))}
+    out = []
+    for _ in range(reps):
+        e = torch.empty(w.n_rot, device=dev)
+        i = torch.empty(w.n_rot, 3, dtype=torch.int32, device=dev)
+        # same output buffers every time for the graph key: reuse the first pair
+        if out:
+            e, i = out[0][2], out[0][3]
+        rec.search_device(w.coor.shape[1], w.coor.shape[0], t["coor"].data_ptr(),
+                          t["charge"].data_ptr(), t["eps"].data_ptr(), t["slot"].data_ptr(),
+                          w.quats.shape[1], t["quats"].data_ptr(), e.data_ptr(), i.data_ptr(), 0)
+        torch.cuda.synchronize()
+        out.append((e.cpu().numpy().copy(), i.cpu().numpy().copy(), e, i))
+    return out
+
+
+def test_graph_replay_matches(c0):
+    import torch
+    w = c0
+    with Receptor(w.grids, w.spacing) as plain:
+        ref = _device_search(plain, w, torch, 1)[0]
+    with Receptor(w.grids, w.spacing, use_graphs=1, wave_rotations=100) as rec:
+        outs = _device_search(rec, w, torch, 4)
+        assert rec.stats()["graph_state"] == 2
+    for e, i, _, _ in outs:
+        np.testing.assert_array_equal(e, ref[0])
+        np.testing.assert_array_equal(i, ref[1])
+
+
+def test_autotune_same_results(c0):
+    w = c0
+    q = w.quats[:, :200]
+    with Receptor(w.grids, w.spacing) as plain:
+        e0, i0 = plain.search(w.coor, w.charge, w.eps, w.slot, q)
+    with Receptor(w.grids, w.spacing, autotune=True) as rec:
+        e1, i1 = rec.search(w.coor, w.charge, w.eps, w.slot, q)
+        st = rec.stats()
+    np.testing.assert_array_equal(e0, e1)
+    np.testing.assert_array_equal(i0, i1)
+    assert st["col_tile"] in (8, 16) and st["rotations_per_cta"] in (16, 32, 64)
