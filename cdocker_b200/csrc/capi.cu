@@ -165,16 +165,16 @@ int autotune_xpass(cdk_ctx* c, WaveArgs a, const RotDesc* d_rots, long nRot, int
   CDK_CUDA(launch_spread_yz(a, s));
   struct Cand { int ct, chunk; };
   std::vector<Cand> cands;
-  if (tc) {
+  if (tc && c->opts.reserved[3] == 0 && umma_supported(c->n, a.Lb)) {
+    cands.push_back({a.col_tile, 0});  // fixed 128-rotation tiles
+  } else if (tc) {
     for (int ch : {32, 64, 128, 256}) cands.push_back({a.col_tile, ch});
-  } else if (c->n <= 64) {
-    for (int ct : {16, 8})
+  } else {
+    for (int ct : (c->n <= 64 ? std::vector<int>{16, 8} : std::vector<int>{8}))
       for (int ch : {16, 32, 64}) {
         if (xpass2_smem_bytes(c->n, c->K, ct) > 227 * 1024) continue;
         cands.push_back({ct, ch});
       }
-  } else {
-    cands.push_back({a.col_tile, 0});
   }
   cudaEvent_t e0, e1;
   CDK_CUDA(cudaEventCreate(&e0));
@@ -189,7 +189,9 @@ int autotune_xpass(cdk_ctx* c, WaveArgs a, const RotDesc* d_rots, long nRot, int
     float ms = 0.f, total = 0.f;
     for (int rep = 0; rep < 2; ++rep) {
       CDK_CUDA(cudaEventRecord(e0, s));
-      if (tc) CDK_CUDA(launch_xpass_tc(t, c->d_ptilde, s));
+      if (tc && c->opts.reserved[3] == 0 && umma_supported(c->n, a.Lb))
+        CDK_CUDA(launch_xpass_umma(t, c->d_ptilde, s));
+      else if (tc) CDK_CUDA(launch_xpass_tc(t, c->d_ptilde, s));
       else CDK_CUDA(launch_xpass(t, s));
       CDK_CUDA(cudaEventRecord(e1, s));
       CDK_CUDA(cudaEventSynchronize(e1));
@@ -242,6 +244,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   a.Lb = Lb;
   a.spacing = c->spacing;
   a.max_atoms = maxAtoms;
+  a.atom_cap = maxAtoms;
   a.coords = d_coor;
   a.params = d_params;
   a.confs = d_confs;
@@ -255,6 +258,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   a.minE = d_minE;
   a.idx = d_idx;
   a.err_count = reinterpret_cast<int*>(c->d_misc + 2);
+  a.fault = reinterpret_cast<int*>(c->d_misc + 3);
   a.col_tile = c->opts.col_tile > 0 ? c->opts.col_tile : pick_col_tile(n, K);
   a.kyof = (c->opts.reserved[1] == 0) ? c->d_kyof : nullptr;  // reserved[1] = 1: FFT planes
   a.chunk = 0;
@@ -267,13 +271,14 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     set_error("ligand box too large for the tensor-core x pass at this grid size and K");
     return CDK_ERR_UNSUPPORTED;
   }
-  if ((n <= 64 ? xpass2_smem_bytes(n, K, a.col_tile) : xpass_smem_bytes(n, K, a.col_tile)) > 227 * 1024 ||
-      (n <= 64 && a.col_tile != 8 && a.col_tile != 16)) {
-    set_error("column tile must be 8 or 16 for n <= 64 and fit shared memory");
+  if (xpass2_smem_bytes(n, K, a.col_tile) > 227 * 1024 ||
+      (n <= 64 && a.col_tile != 8 && a.col_tile != 16) || (n > 64 && a.col_tile != 8)) {
+    set_error("column tile must be 8 or 16 (n <= 64) or 8 (n > 64) and fit shared memory");
     return CDK_ERR_INVALID;
   }
-  CDK_CUDA(cudaMemsetAsync(c->d_misc + 2, 0, sizeof(unsigned int), s));
+  CDK_CUDA(cudaMemsetAsync(c->d_misc + 2, 0, 2 * sizeof(unsigned int), s));
   CDK_CUDA(cudaMemsetAsync(c->d_work, 0, 2 * sizeof(unsigned long long), s));
+  const bool umma = tc && c->opts.reserved[3] == 0 && umma_supported(n, Lb);
   a.work = c->d_work;
   const bool prof = c->opts.reserved[0] != 0;
   const long nwaves = (nRot + wave - 1) / wave;
@@ -302,7 +307,8 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     if (prof) CDK_CUDA(cudaEventRecord(ev[1], s));
     CDK_CUDA(launch_spread_yz(a, s));
     if (prof) CDK_CUDA(cudaEventRecord(ev[2], s));
-    if (tc) CDK_CUDA(launch_xpass_tc(a, c->d_ptilde, s));
+    if (umma) CDK_CUDA(launch_xpass_umma(a, c->d_ptilde, s));
+    else if (tc) CDK_CUDA(launch_xpass_tc(a, c->d_ptilde, s));
     else CDK_CUDA(launch_xpass(a, s));
     if (prof) CDK_CUDA(cudaEventRecord(ev[3], s));
     CDK_CUDA(launch_yz_inv_argmin(a, s));
@@ -396,6 +402,7 @@ int search_device_impl(cdk_ctx* c, int nAtom, int nConf, const float* d_coor,
   if (graphs && c->gkey_seen == 2 && c->gkey == key) {
     CDK_CUDA(cudaGraphLaunch(c->gexec, s));
     CDK_CUDA(cudaEventRecord(c->ev1, s));
+    c->stats[15] = 2;
     return CDK_OK;
   }
   const bool capture = graphs && c->gkey_seen == 1 && c->gkey == key;
@@ -422,6 +429,7 @@ int search_device_impl(cdk_ctx* c, int nAtom, int nConf, const float* d_coor,
     CDK_CUDA(cudaGraphInstantiate(&c->gexec, g, 0));
     CDK_CUDA(cudaGraphLaunch(c->gexec, s));
     c->gkey_seen = 2;
+    c->stats[15] = 2;
   } else {
     if (rc) return rc;
     if (graphs) {
@@ -438,9 +446,13 @@ int search_device_impl(cdk_ctx* c, int nAtom, int nConf, const float* d_coor,
 }
 
 int check_errors_after(cdk_ctx* c, cudaStream_t s) {
-  CDK_CUDA(cudaMemcpyAsync(c->h_misc + 2, c->d_misc + 2, sizeof(unsigned int),
+  CDK_CUDA(cudaMemcpyAsync(c->h_misc + 2, c->d_misc + 2, 2 * sizeof(unsigned int),
                            cudaMemcpyDeviceToHost, s));
   CDK_CUDA(cudaStreamSynchronize(s));
+  if (c->h_misc[3] != 0) {
+    set_error("a bounded device wait (tensor-core commit) gave up; results are invalid");
+    return CDK_ERR_CUDA;
+  }
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, c->ev0, c->ev1) == cudaSuccess) c->stats[3] = ms;
   CDK_CUDA(cudaMemcpy(c->h_work, c->d_work, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));

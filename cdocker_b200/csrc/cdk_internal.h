@@ -55,6 +55,7 @@ struct WaveArgs {
   float spacing;
   int nrot;          // rotations in this wave
   int max_atoms;     // stride of rotated-atom storage
+  int atom_cap;      // largest ligand of this wave (sizes the direct plane kernel)
   const float* coords;       // [atoms][3]
   const AtomParam* params;   // [atom params]
   const ConfDesc* confs;
@@ -72,6 +73,7 @@ struct WaveArgs {
   unsigned long long* work;  // [0] x planes spread, [1] window planes (work counters)
   int col_tile;
   int chunk;                 // rotations per CTA in the x pass (0 = default)
+  int* fault;                // set when a bounded device wait gave up
   const int* kyof;           // [n] natural frequency at each digit-reversed position; when set
                              // (and ligands have <= 96 atoms) planes are evaluated directly
 };
@@ -110,6 +112,9 @@ cudaError_t launch_rescore_fp64(int n, int K, float spacing, const float* grids,
 cudaError_t launch_ptilde(int n, int K, const float2* yz, float2* pt, cudaStream_t s);
 cudaError_t launch_xpass_tc(const WaveArgs& a, const float2* pt, cudaStream_t s);
 size_t xpass_tc_smem_bytes(int n, int K, int Lb);
+// tcgen05 variant of the precision x pass (n = 64)
+bool umma_supported(int n, int Lb);
+cudaError_t launch_xpass_umma(const WaveArgs& a, const float2* pt, cudaStream_t s);
 
 // Digit-reversed position of natural frequency k for the radix plan of length n.
 int fft_position(int n, int k);

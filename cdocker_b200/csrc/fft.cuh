@@ -99,6 +99,63 @@ struct Radix<8, SIGN> {
   }
 };
 
+// exp(SIGN * 2 pi i m / R) for the composite radices below (constants from the unit circle:
+// cos/sin of multiples of pi/6 and pi/8)
+template <int R, int SIGN>
+__device__ __forceinline__ float2 unit_root(int m) {
+  constexpr float c8 = 0.92387953251128675613f, s8 = 0.38268343236508977173f;
+  constexpr float h2 = 0.70710678118654752440f, r3 = 0.86602540378443864676f;
+  float c = 1.f, sn = 0.f;
+  if (R == 16) {
+    const float cs[16] = {1.f, c8, h2, s8, 0.f, -s8, -h2, -c8, -1.f, -c8, -h2, -s8, 0.f, s8, h2, c8};
+    const float ss[16] = {0.f, s8, h2, c8, 1.f, c8, h2, s8, 0.f, -s8, -h2, -c8, -1.f, -c8, -h2, -s8};
+    c = cs[m & 15];
+    sn = ss[m & 15];
+  } else if (R == 12) {
+    const float cs[12] = {1.f, r3, .5f, 0.f, -.5f, -r3, -1.f, -r3, -.5f, 0.f, .5f, r3};
+    const float ss[12] = {0.f, .5f, r3, 1.f, r3, .5f, 0.f, -.5f, -r3, -1.f, -r3, -.5f};
+    c = cs[m % 12];
+    sn = ss[m % 12];
+  }
+  return make_float2(c, SIGN * sn);
+}
+
+// Composite radix R = A * B in registers: n = B*n1 + n2, k = k1 + A*k2;
+// y[k] = sum_n2 w_R^(n2 k1) w_B^(n2 k2) sum_n1 x[B n1 + n2] w_A^(n1 k1)
+template <int A, int B, int SIGN>
+__device__ __forceinline__ void radix_composite(float2* v) {
+  constexpr int R = A * B;
+  float2 u[B][A];
+#pragma unroll
+  for (int n2 = 0; n2 < B; ++n2) {
+#pragma unroll
+    for (int n1 = 0; n1 < A; ++n1) u[n2][n1] = v[B * n1 + n2];
+    Radix<A, SIGN>::run(u[n2]);
+#pragma unroll
+    for (int k1 = 1; k1 < A; ++k1)
+      if (n2 > 0) u[n2][k1] = c_mul(u[n2][k1], unit_root<R, SIGN>(n2 * k1));
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < A; ++k1) {
+    float2 w[B];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) w[n2] = u[n2][k1];
+    Radix<B, SIGN>::run(w);
+#pragma unroll
+    for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = w[k2];
+  }
+}
+
+template <int SIGN>
+struct Radix<12, SIGN> {
+  __device__ __forceinline__ static void run(float2* v) { radix_composite<4, 3, SIGN>(v); }
+};
+
+template <int SIGN>
+struct Radix<16, SIGN> {
+  __device__ __forceinline__ static void run(float2* v) { radix_composite<4, 4, SIGN>(v); }
+};
+
 // Radix sequences per transform length (R0 first in the forward transform).
 template <int N>
 struct FFTPlan;
@@ -112,11 +169,11 @@ struct FFTPlan<64> {
 };
 template <>
 struct FFTPlan<96> {
-  static constexpr int NS = 3, R0 = 8, R1 = 4, R2 = 3;
+  static constexpr int NS = 2, R0 = 8, R1 = 12, R2 = 1;
 };
 template <>
 struct FFTPlan<128> {
-  static constexpr int NS = 3, R0 = 8, R1 = 4, R2 = 4;
+  static constexpr int NS = 2, R0 = 8, R1 = 16, R2 = 1;
 };
 
 template <int N>

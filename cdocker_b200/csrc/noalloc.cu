@@ -213,6 +213,7 @@ extern "C" int cdk_search_device_noalloc(cdk_ctx* ctx, int nAtom, int nConf,
   a.Lb = Lb;
   a.spacing = v.spacing;
   a.max_atoms = nAtom;
+  a.atom_cap = nAtom;
   a.coords = d_coor;
   a.params = params;
   a.confs = confs;
@@ -221,6 +222,7 @@ extern "C" int cdk_search_device_noalloc(cdk_ctx* ctx, int nAtom, int nConf,
   a.minE = d_minE;
   a.idx = d_idx;
   a.err_count = reinterpret_cast<int*>(misc + 2);
+  a.fault = reinterpret_cast<int*>(misc + 3);
   a.work = reinterpret_cast<unsigned long long*>(misc + 4);
   a.col_tile = v.col_tile_opt > 0 ? v.col_tile_opt : pick_col_tile(n, K);
   a.kyof = v.kyof;

@@ -774,8 +774,8 @@ size_t direct_smem(int cap) {
 
 template <int N>
 cudaError_t launch_spread_yz_t(const WaveArgs& a, cudaStream_t s) {
-  if (a.kyof && a.max_atoms <= kDirectMaxAtoms) {
-    const int cap = a.max_atoms;
+  const int cap = a.atom_cap > 0 ? a.atom_cap : a.max_atoms;
+  if (a.kyof && cap <= kDirectMaxAtoms) {
     const size_t sm = direct_smem<N>(cap);
     cudaError_t e = cudaFuncSetAttribute(k_spread_yz_direct<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
@@ -812,13 +812,14 @@ cudaError_t launch_xpass_t(const WaveArgs& a, cudaStream_t s) {
     // reused while giving the scheduler many CTAs per SM slot
     constexpr int CT = 16;
     if (a.col_tile != CT && a.col_tile != 8) return cudaErrorInvalidValue;
+    if (N > 64 && a.col_tile != 8) return cudaErrorInvalidValue;
     const size_t sm = xpass2_smem_bytes(N, a.K, a.col_tile);
     const int per = a.chunk > 0 ? a.chunk : 32;
     const int chunks = (a.nrot + per - 1) / per;
-    if (a.col_tile == CT) {
-      cudaError_t e = cudaFuncSetAttribute(k_xpass2<N, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (N <= 64 && a.col_tile == CT) {
+      cudaError_t e = cudaFuncSetAttribute(k_xpass2<N, (N <= 64 ? 16 : 8)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       if (e != cudaSuccess) return e;
-      k_xpass2<N, 16><<<dim3(NCOL / 16, chunks), 256, sm, s>>>(a, per);
+      k_xpass2<N, (N <= 64 ? 16 : 8)><<<dim3(NCOL / (N <= 64 ? 16 : 8), chunks), 256, sm, s>>>(a, per);
     } else {
       cudaError_t e = cudaFuncSetAttribute(k_xpass2<N, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       if (e != cudaSuccess) return e;
@@ -882,6 +883,8 @@ int pick_col_tile(int n, int K) {
   int ct = 16;
   if (n == 32 || n == 64) {
     if (xpass2_smem_bytes(n, K, 16) > 110 * 1024) ct = 8;
+  } else if (n == 96 || n == 128) {
+    ct = 8;
   } else {
     while (ct > 2 && xpass_smem_bytes(n, K, ct) > 100 * 1024) ct >>= 1;
   }

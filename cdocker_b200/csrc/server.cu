@@ -271,6 +271,7 @@ void worker_loop(cdk_server* s) {
   a.phat = s->v.phat;
   a.tw = s->v.tw;
   a.err_count = reinterpret_cast<int*>(s->d_misc);
+  a.fault = reinterpret_cast<int*>(s->d_misc + 1);
   a.work = reinterpret_cast<unsigned long long*>(s->d_misc + 2);
   a.col_tile = s->v.col_tile_opt > 0 ? s->v.col_tile_opt : pick_col_tile(n, K);
   a.kyof = s->v.kyof;
@@ -281,7 +282,7 @@ void worker_loop(cdk_server* s) {
     // build the next wave from the admitted requests
     WaveSlot& w = s->slots[cur];
     if (w.busy) retire(s, w);
-    int nr = 0, lb = 2;
+    int nr = 0, lb = 2, cap = 1;
     {
       std::unique_lock<std::mutex> lk(s->mu);
       admit(s);
@@ -325,11 +326,13 @@ void worker_loop(cdk_server* s) {
         r->next_rot += take;
         nr += (int)take;
         lb = std::max(lb, r->Lb);
+        cap = std::max(cap, r->nAtom);
       }
     }
     cudaMemcpyAsync(w.d_rots, w.h_rots, sizeof(RotDesc) * nr, cudaMemcpyHostToDevice, s->stream);
     a.nrot = nr;
     a.Lb = lb;
+    a.atom_cap = cap;
     a.rots = w.d_rots;
     launch_prep(a, s->stream);
     launch_spread_yz(a, s->stream);

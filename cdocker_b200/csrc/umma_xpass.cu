@@ -1,0 +1,324 @@
+// umma_xpass.cu -- the precision form's x pass on the 5th-generation tensor cores (tcgen05).
+//
+// Same operator as tc_xpass.cu (the x-direction forward DFT, conjugate product with the
+// receptor spectrum and inverse DFT collapse into one circulant matrix per channel and (ky,kz)
+// column, P~_k((x + x') mod n, col)), here issued as tcgen05.mma with the accumulator in tensor
+// memory. For n = 64 the real-ified operator is exactly 128 rows:
+//     rows 0..63   (x'):  [ Tr | Ti ]   -> Br = sum_x Tr ar + Ti ai
+//     rows 64..127 (x'):  [ Ti | -Tr ]  -> Bi = sum_x Ti ar - Tr ai
+// so one MMA is M = 128 (x', re/im), N = 128 rotations, K = 16 of the 2*Lp (re/im, x) inputs.
+// BF16 hi/lo split: D += A_hi B_hi + A_hi B_lo + A_lo B_hi, FP32 accumulation in TMEM across all
+// channels of a rotation chunk.
+//
+// CTA = 2 spectral columns x 128 rotations; 256 threads. Per channel: all threads build the two
+// Toeplitz operators and stage the ligand operand in shared memory (canonical K-major layout,
+// no swizzle: 8-row x 16-byte core matrices), one thread issues 18 MMAs (2 columns x 3 k-steps x
+// 3 split terms) and commits to an mbarrier that every thread waits on (bounded) before the
+// buffers are rebuilt. Epilogue: tcgen05.ld by the 8 warps (warp w reads TMEM lanes
+// 32*(w%4)..+31 of column w/4), staged through shared memory into B.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "cdk_internal.h"
+
+namespace cdk {
+namespace {
+
+constexpr int UM_CT = 2;
+constexpr int UM_R = 128;
+constexpr int UM_THREADS = 256;
+constexpr int UM_M = 128;
+constexpr uint32_t UM_TMEM_COLS = UM_CT * UM_R;  // 256
+// instruction descriptor, kind::f16: D f32, A bf16, B bf16, both K-major, N, M
+constexpr uint32_t UM_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(UM_R >> 3) << 17) |
+                              ((uint32_t)(UM_M >> 4) << 24);
+constexpr long kWaitLimit = 1l << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// shared-memory matrix descriptor: K-major, no swizzle, version 1
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// byte offset of element (row, k) in a rows x K bf16 tile, K-major core-matrix layout
+__device__ __forceinline__ uint32_t kmaj_off(int row, int k) {
+  return (uint32_t)((k >> 3) * (UM_M / 8) * 128 + (row >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __float2bfloat16_rn(v);
+  lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+}
+
+__device__ __forceinline__ uint32_t pack2(__nv_bfloat16 a, __nv_bfloat16 b) {
+  return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (long i = 0; i < kWaitLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (i > 32) __nanosleep(40);
+  }
+  return false;
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      :
+      : "r"(d_tmem), "l"(a), "l"(b), "r"(UM_IDESC), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// n = 64 only: the real-ified operator has exactly 128 rows
+__global__ void __launch_bounds__(UM_THREADS, 2) k_xpass_umma64(WaveArgs a, const float2* __restrict__ pt,
+                                                              int Lp) {
+  constexpr int N = 64;
+  constexpr int NZH = N / 2 + 1;
+  constexpr int NCOL = N * NZH;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ uint32_t s_tmem;
+  __shared__ short s_rng[UM_R][2];
+  __shared__ int s_W[UM_R];
+  __shared__ float2 s_p[UM_CT][N];
+  __shared__ int s_flags[2];  // [1] any MMA issued
+  const int K = a.K;
+  const int KD = 2 * Lp;                        // MMA K extent (re/im x planes)
+  const uint32_t tile = (uint32_t)UM_M * KD * 2; // bytes of one 128 x KD bf16 operand
+  // operand tiles: [c][A_hi, A_lo, B_hi, B_lo]
+  unsigned char* opnd = smem_raw;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int c0 = blockIdx.x * UM_CT;
+  const int r0 = blockIdx.y * UM_R;
+  const int nr = min(UM_R, a.nrot - r0);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(UM_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid < UM_R) {
+    int W = 0;
+    if (tid < nr && a.rec[r0 + tid].valid) W = a.rec[r0 + tid].W[0];
+    s_W[tid] = W;
+  }
+  if (tid < 2) s_flags[tid] = 0;
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = s_tmem;
+  const uint32_t bar = smem_u32(&s_bar);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int k = 0; k < K && ok; ++k) {
+    // channel ranges of the chunk's rotations
+    int mine = 0;
+    if (tid < UM_R) {
+      short lo = 1, hi = 0;
+      if (tid < nr) {
+        const RotRec* rec = a.rec + r0 + tid;
+        if (rec->valid) {
+          lo = rec->xlo[k];
+          hi = rec->xhi[k];
+        }
+      }
+      s_rng[tid][0] = lo;
+      s_rng[tid][1] = hi;
+      mine = lo <= hi;
+    }
+    for (int i = tid; i < UM_CT * N; i += UM_THREADS) {
+      const int c = i / N, m = i - c * N;
+      s_p[c][m] = pt[((size_t)(c0 + c) * K + k) * N + m];
+    }
+    if (!__syncthreads_or(mine)) continue;  // no rotation of the chunk touches channel k
+    // ---- Toeplitz operators: element pairs (k, k+1) = (x, x+1) of one part -> one 32-bit word
+    for (int i = tid; i < UM_CT * UM_M * Lp; i += UM_THREADS) {
+      const int kp = i % Lp;           // pair index over the KD = 2*Lp columns
+      const int row = (i / Lp) % UM_M;
+      const int c = i / (Lp * UM_M);
+      const int kk = 2 * kp;           // first K index of the pair
+      const int part = kk >= Lp;
+      const int x = kk - part * Lp;
+      const int xp = row & (N - 1);
+      const bool imrow = row >= N;
+      const float2 p0 = s_p[c][(x + xp) & (N - 1)], p1 = s_p[c][(x + 1 + xp) & (N - 1)];
+      // rows < 64: [Tr | Ti]; rows >= 64: [Ti | -Tr]
+      float v0, v1;
+      if (!imrow) {
+        v0 = part ? p0.y : p0.x;
+        v1 = part ? p1.y : p1.x;
+      } else {
+        v0 = part ? -p0.x : p0.y;
+        v1 = part ? -p1.x : p1.y;
+      }
+      __nv_bfloat16 h0, l0, h1, l1;
+      split_bf16(v0, h0, l0);
+      split_bf16(v1, h1, l1);
+      unsigned char* base = opnd + (size_t)c * 4 * tile;
+      const uint32_t off = kmaj_off(row, kk);
+      *reinterpret_cast<uint32_t*>(base + 0 * tile + off) = pack2(h0, h1);
+      *reinterpret_cast<uint32_t*>(base + 1 * tile + off) = pack2(l0, l1);
+    }
+    // ---- ligand operand: row = rotation, K = (part, x); two columns per 16-byte load
+    for (int i = tid; i < UM_R * (Lp / 2); i += UM_THREADS) {
+      const int x2 = i % (Lp / 2);
+      const int rr = i / (Lp / 2);
+      const int x = 2 * x2;
+      float4 v[2];
+#pragma unroll
+      for (int d = 0; d < 2; ++d) {
+        const bool in = rr < nr && x + d >= s_rng[rr][0] && x + d <= s_rng[rr][1];
+        v[d] = in ? *reinterpret_cast<const float4*>(
+                        a.A + (((size_t)(r0 + rr) * K + k) * a.Lb + x + d) * NCOL + c0)
+                  : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int c = 0; c < UM_CT; ++c) {
+        const float re0 = c ? v[0].z : v[0].x, im0 = c ? v[0].w : v[0].y;
+        const float re1 = c ? v[1].z : v[1].x, im1 = c ? v[1].w : v[1].y;
+        __nv_bfloat16 rh0, rl0, rh1, rl1, ih0, il0, ih1, il1;
+        split_bf16(re0, rh0, rl0);
+        split_bf16(re1, rh1, rl1);
+        split_bf16(im0, ih0, il0);
+        split_bf16(im1, ih1, il1);
+        unsigned char* base = opnd + (size_t)c * 4 * tile;
+        const uint32_t ore = kmaj_off(rr, x), oim = kmaj_off(rr, Lp + x);
+        *reinterpret_cast<uint32_t*>(base + 2 * tile + ore) = pack2(rh0, rh1);
+        *reinterpret_cast<uint32_t*>(base + 3 * tile + ore) = pack2(rl0, rl1);
+        *reinterpret_cast<uint32_t*>(base + 2 * tile + oim) = pack2(ih0, ih1);
+        *reinterpret_cast<uint32_t*>(base + 3 * tile + oim) = pack2(il0, il1);
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t kstride = (uint32_t)(UM_M / 8) * 128;  // bytes between K groups of 8
+      for (int c = 0; c < UM_CT; ++c) {
+        const uint32_t base = smem_u32(opnd + (size_t)c * 4 * tile);
+        const uint32_t d = tmem + (uint32_t)(c * UM_R);
+        for (int s = 0; s < KD / 16; ++s) {
+          const uint32_t ks = (uint32_t)s * 2 * kstride;
+          const uint64_t ah = make_desc(base + 0 * tile + ks, kstride, 128);
+          const uint64_t al = make_desc(base + 1 * tile + ks, kstride, 128);
+          const uint64_t bh = make_desc(base + 2 * tile + ks, kstride, 128);
+          const uint64_t bl = make_desc(base + 3 * tile + ks, kstride, 128);
+          const uint32_t acc0 = (s_flags[1] || s > 0) ? 1u : 0u;
+          umma_f16(d, ah, bh, acc0);
+          umma_f16(d, ah, bl, 1u);
+          umma_f16(d, al, bh, 1u);
+        }
+      }
+      s_flags[1] = 1;
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                   : "memory");
+    }
+    const bool done = mbar_wait(bar, phase);
+    phase ^= 1u;
+    ok = __syncthreads_and(done ? 1 : 0) != 0;
+  }
+  if (!ok) {
+    if (tid == 0) atomicOr(a.fault, 1);  // an MMA commit never arrived: report, free TMEM
+  } else if (s_flags[1]) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // ---- epilogue: TMEM -> shared staging [c][32 rotations][64 x'] float2 -> B
+    float2* stage = reinterpret_cast<float2*>(smem_raw);
+    const int q = warp & 3, c = warp >> 2;
+    const int row = 32 * q + lane;  // TMEM lane = operator row
+    const int xp = row & (N - 1);
+    const bool imrow = row >= N;
+    for (int j = 0; j < UM_R / 32; ++j) {
+      float v[32];
+      tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(c * UM_R + 32 * j), v);
+#pragma unroll
+      for (int t = 0; t < 32; ++t) {
+        float* dst = reinterpret_cast<float*>(&stage[((size_t)c * 32 + t) * N + xp]);
+        dst[imrow ? 1 : 0] = v[t];
+      }
+      __syncthreads();
+      for (int i = tid; i < UM_CT * 32 * N; i += UM_THREADS) {
+        const int cc = i & 1;
+        const int x = (i >> 1) & (N - 1);
+        const int t = i >> 7;  // rotation within the 32
+        const int rr = 32 * j + t;
+        if (rr < nr && x < s_W[rr])
+          a.B[((size_t)(r0 + rr) * N + x) * NCOL + c0 + cc] = stage[((size_t)cc * 32 + t) * N + x];
+      }
+      __syncthreads();
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(UM_TMEM_COLS));
+  }
+}
+
+}  // namespace
+
+size_t xpass_umma_smem_bytes(int Lb) {
+  const int Lp = (Lb + 7) & ~7;
+  // at least 90 KB so that at most two CTAs (2 x 256 TMEM columns) share an SM
+  const size_t need = (size_t)UM_CT * 4 * UM_M * (2 * Lp) * 2 + 1024;
+  return need < 90 * 1024 ? 90 * 1024 : need;
+}
+
+bool umma_supported(int n, int Lb) {
+  const int Lp = (Lb + 7) & ~7;
+  // epilogue staging (2 x 32 x 64 float2 = 32 KB) reuses the operand tiles
+  return n == 64 && Lp <= 32 && xpass_umma_smem_bytes(Lb) <= 200 * 1024;
+}
+
+cudaError_t launch_xpass_umma(const WaveArgs& a, const float2* pt, cudaStream_t s) {
+  if (!umma_supported(a.n, a.Lb)) return cudaErrorInvalidValue;
+  const int Lp = (a.Lb + 7) & ~7;
+  const size_t sm = xpass_umma_smem_bytes(a.Lb);
+  cudaError_t e = cudaFuncSetAttribute(k_xpass_umma64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  constexpr int NCOL = 64 * 33;
+  dim3 grid(NCOL / UM_CT, (a.nrot + UM_R - 1) / UM_R);
+  k_xpass_umma64<<<grid, UM_THREADS, sm, s>>>(a, pt, Lp);
+  return cudaGetLastError();
+}
+
+}  // namespace cdk

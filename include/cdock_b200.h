@@ -51,7 +51,8 @@ typedef struct cdk_opts {
   int reserved[8];     /* [0] = 1: time every kernel with events (cdk_ctx_stats [8..12]);
                           [1] = 1: spread planes through the radix FFT instead of the direct
                           separable evaluation; [2] = 1: autotune the x pass on the first wave
-                          of each new ligand box */
+                          of each new ligand box; [3] = 1: precision form on mma.sync instead
+                          of tcgen05 */
 } cdk_opts;
 
 /* Library version string. */

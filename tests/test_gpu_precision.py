@@ -52,3 +52,14 @@ def test_fp64_rescore_of_top_poses(c0):
         emap = O.energy_map(w.grids, w.spacing, w.coor[0], w.charge, w.eps, w.slot, qq[r])
         ref = emap[tuple(idx[r])]
         assert abs(e64[0, j] - ref) <= 1e-7 * max(1.0, abs(ref))
+
+
+def test_tcgen05_and_mma_sync_variants_agree(grids_cache):
+    """The tcgen05 (TMEM accumulator) and mma.sync kernels apply the same split-BF16 operator."""
+    w = synth.make_workload("c1_64", seed=8, n_conf=2, n_q=150, grids_cache=grids_cache)
+    with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3) as ru, \
+            Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3, tc_mma_sync=True) as rm:
+        eu, iu = ru.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+        em, im = rm.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+    assert rel_err(eu, em).max() <= 1e-5
+    assert np.mean(np.all(iu == im, axis=1)) >= 0.99
