@@ -118,10 +118,12 @@ __global__ void __launch_bounds__(UM_THREADS, 2) k_xpass_umma64(WaveArgs a, cons
   __shared__ short s_rng[UM_R][2];
   __shared__ int s_W[UM_R];
   __shared__ float2 s_p[UM_CT][N];
+  __shared__ uint32_t s_q[UM_CT * 6 * (N + 32 + 8)];  // pair arrays, QL <= n + Lp_max + 8
   __shared__ int s_flags[2];  // [1] any MMA issued
   const int K = a.K;
   const int KD = 2 * Lp;                        // MMA K extent (re/im x planes)
   const uint32_t tile = (uint32_t)UM_M * KD * 2; // bytes of one 128 x KD bf16 operand
+  const int QL = N + Lp + 8;                     // pair-array length (x + x' + 7 < QL)
   // operand tiles: [c][A_hi, A_lo, B_hi, B_lo]
   unsigned char* opnd = smem_raw;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -171,62 +173,88 @@ __global__ void __launch_bounds__(UM_THREADS, 2) k_xpass_umma64(WaveArgs a, cons
       s_p[c][m] = pt[((size_t)(c0 + c) * K + k) * N + m];
     }
     if (!__syncthreads_or(mine)) continue;  // no rotation of the chunk touches channel k
-    // ---- Toeplitz operators: element pairs (k, k+1) = (x, x+1) of one part -> one 32-bit word
-    for (int i = tid; i < UM_CT * UM_M * Lp; i += UM_THREADS) {
-      const int kp = i % Lp;           // pair index over the KD = 2*Lp columns
-      const int row = (i / Lp) % UM_M;
-      const int c = i / (Lp * UM_M);
-      const int kk = 2 * kp;           // first K index of the pair
-      const int part = kk >= Lp;
-      const int x = kk - part * Lp;
-      const int xp = row & (N - 1);
-      const bool imrow = row >= N;
-      const float2 p0 = s_p[c][(x + xp) & (N - 1)], p1 = s_p[c][(x + 1 + xp) & (N - 1)];
-      // rows < 64: [Tr | Ti]; rows >= 64: [Ti | -Tr]
-      float v0, v1;
-      if (!imrow) {
-        v0 = part ? p0.y : p0.x;
-        v1 = part ? p1.y : p1.x;
-      } else {
-        v0 = part ? -p0.x : p0.y;
-        v1 = part ? -p1.x : p1.y;
-      }
+    // ---- pair arrays of the two columns: word j = (v[j], v[j+1]) of hi / lo parts of Re, Im,
+    // -Re of P~ along x (circular), so any 8 consecutive Toeplitz entries are 4 aligned words
+    for (int i = tid; i < UM_CT * QL; i += UM_THREADS) {
+      const int c = i / QL, j = i - c * QL;
+      const float2 p0 = s_p[c][j & (N - 1)], p1 = s_p[c][(j + 1) & (N - 1)];
       __nv_bfloat16 h0, l0, h1, l1;
-      split_bf16(v0, h0, l0);
-      split_bf16(v1, h1, l1);
-      unsigned char* base = opnd + (size_t)c * 4 * tile;
-      const uint32_t off = kmaj_off(row, kk);
-      *reinterpret_cast<uint32_t*>(base + 0 * tile + off) = pack2(h0, h1);
-      *reinterpret_cast<uint32_t*>(base + 1 * tile + off) = pack2(l0, l1);
+      uint32_t* q = s_q + (size_t)c * 6 * QL + j;
+      split_bf16(p0.x, h0, l0);
+      split_bf16(p1.x, h1, l1);
+      q[0 * QL] = pack2(h0, h1);
+      q[1 * QL] = pack2(l0, l1);
+      split_bf16(p0.y, h0, l0);
+      split_bf16(p1.y, h1, l1);
+      q[2 * QL] = pack2(h0, h1);
+      q[3 * QL] = pack2(l0, l1);
+      split_bf16(-p0.x, h0, l0);
+      split_bf16(-p1.x, h1, l1);
+      q[4 * QL] = pack2(h0, h1);
+      q[5 * QL] = pack2(l0, l1);
     }
-    // ---- ligand operand: row = rotation, K = (part, x); two columns per 16-byte load
-    for (int i = tid; i < UM_R * (Lp / 2); i += UM_THREADS) {
-      const int x2 = i % (Lp / 2);
-      const int rr = i / (Lp / 2);
-      const int x = 2 * x2;
-      float4 v[2];
+    __syncthreads();
+    // ---- Toeplitz operators: one 16-byte core-matrix row (8 consecutive K = x values of one
+    // part) per item; rows < 64: [Tr | Ti], rows >= 64: [Ti | -Tr]
+    {
+      const int ng = KD / 8;  // k-groups
+      for (int i = tid; i < UM_CT * ng * UM_M; i += UM_THREADS) {
+        const int row = i % UM_M;  // lanes take consecutive rows: conflict-free 16-byte stores
+        const int t = i / UM_M;
+        const int g = t % ng, c = t / ng;
+        const int kk = 8 * g;
+        const int part = kk >= Lp;
+        const int x0 = kk - part * Lp;
+        const bool imrow = row >= N;
+        // which pair array: 0/1 Re, 2/3 Im, 4/5 -Re
+        const int sel = imrow ? (part ? 4 : 2) : (part ? 2 : 0);
+        const uint32_t* qh = s_q + ((size_t)c * 6 + sel) * QL + x0 + (row & (N - 1));
+        const uint32_t* ql = qh + QL;
+        const uint4 vh = make_uint4(qh[0], qh[2], qh[4], qh[6]);
+        const uint4 vl = make_uint4(ql[0], ql[2], ql[4], ql[6]);
+        unsigned char* base = opnd + (size_t)c * 4 * tile + kmaj_off(row, kk);
+        *reinterpret_cast<uint4*>(base + 0 * tile) = vh;
+        *reinterpret_cast<uint4*>(base + 1 * tile) = vl;
+      }
+    }
+    // ---- ligand operand: one rotation x 8 consecutive x planes (both columns, re and im) per
+    // item; lanes take consecutive rotations
+    for (int i = tid; i < UM_R * (Lp / 8); i += UM_THREADS) {
+      const int rr = i % UM_R;
+      const int x0 = 8 * (i / UM_R);
+      const int lo = s_rng[rr][0], hi = s_rng[rr][1];
+      float4 v[8];
 #pragma unroll
-      for (int d = 0; d < 2; ++d) {
-        const bool in = rr < nr && x + d >= s_rng[rr][0] && x + d <= s_rng[rr][1];
-        v[d] = in ? *reinterpret_cast<const float4*>(
-                        a.A + (((size_t)(r0 + rr) * K + k) * a.Lb + x + d) * NCOL + c0)
-                  : make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int d = 0; d < 8; ++d) {
+        const int x = x0 + d;
+        v[d] = (rr < nr && x >= lo && x <= hi)
+                   ? *reinterpret_cast<const float4*>(
+                         a.A + (((size_t)(r0 + rr) * K + k) * a.Lb + x) * NCOL + c0)
+                   : make_float4(0.f, 0.f, 0.f, 0.f);
       }
 #pragma unroll
       for (int c = 0; c < UM_CT; ++c) {
-        const float re0 = c ? v[0].z : v[0].x, im0 = c ? v[0].w : v[0].y;
-        const float re1 = c ? v[1].z : v[1].x, im1 = c ? v[1].w : v[1].y;
-        __nv_bfloat16 rh0, rl0, rh1, rl1, ih0, il0, ih1, il1;
-        split_bf16(re0, rh0, rl0);
-        split_bf16(re1, rh1, rl1);
-        split_bf16(im0, ih0, il0);
-        split_bf16(im1, ih1, il1);
+        uint32_t reh[4], rel[4], imh[4], iml[4];
+#pragma unroll
+        for (int d = 0; d < 8; d += 2) {
+          const float r0v = c ? v[d].z : v[d].x, i0v = c ? v[d].w : v[d].y;
+          const float r1v = c ? v[d + 1].z : v[d + 1].x, i1v = c ? v[d + 1].w : v[d + 1].y;
+          __nv_bfloat16 h0, l0, h1, l1;
+          split_bf16(r0v, h0, l0);
+          split_bf16(r1v, h1, l1);
+          reh[d / 2] = pack2(h0, h1);
+          rel[d / 2] = pack2(l0, l1);
+          split_bf16(i0v, h0, l0);
+          split_bf16(i1v, h1, l1);
+          imh[d / 2] = pack2(h0, h1);
+          iml[d / 2] = pack2(l0, l1);
+        }
         unsigned char* base = opnd + (size_t)c * 4 * tile;
-        const uint32_t ore = kmaj_off(rr, x), oim = kmaj_off(rr, Lp + x);
-        *reinterpret_cast<uint32_t*>(base + 2 * tile + ore) = pack2(rh0, rh1);
-        *reinterpret_cast<uint32_t*>(base + 3 * tile + ore) = pack2(rl0, rl1);
-        *reinterpret_cast<uint32_t*>(base + 2 * tile + oim) = pack2(ih0, ih1);
-        *reinterpret_cast<uint32_t*>(base + 3 * tile + oim) = pack2(il0, il1);
+        const uint32_t ore = kmaj_off(rr, x0), oim = kmaj_off(rr, Lp + x0);
+        *reinterpret_cast<uint4*>(base + 2 * tile + ore) = make_uint4(reh[0], reh[1], reh[2], reh[3]);
+        *reinterpret_cast<uint4*>(base + 3 * tile + ore) = make_uint4(rel[0], rel[1], rel[2], rel[3]);
+        *reinterpret_cast<uint4*>(base + 2 * tile + oim) = make_uint4(imh[0], imh[1], imh[2], imh[3]);
+        *reinterpret_cast<uint4*>(base + 3 * tile + oim) = make_uint4(iml[0], iml[1], iml[2], iml[3]);
       }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
