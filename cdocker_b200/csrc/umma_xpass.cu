@@ -107,13 +107,13 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
 }
 
 // n = 64 only: the real-ified operator has exactly 128 rows
-__global__ void __launch_bounds__(UM_THREADS, 2) k_xpass_umma64(WaveArgs a, const float2* __restrict__ pt,
-                                                              int Lp) {
+__global__ void __launch_bounds__(UM_THREADS, 1) k_xpass_umma64(WaveArgs a, const float2* __restrict__ pt,
+                                                              int Lp, int nbuf_sets) {
   constexpr int N = 64;
   constexpr int NZH = N / 2 + 1;
   constexpr int NCOL = N * NZH;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ __align__(8) uint64_t s_bar[2];
   __shared__ uint32_t s_tmem;
   __shared__ short s_rng[UM_R][2];
   __shared__ int s_W[UM_R];
@@ -124,14 +124,15 @@ __global__ void __launch_bounds__(UM_THREADS, 2) k_xpass_umma64(WaveArgs a, cons
   const int KD = 2 * Lp;                        // MMA K extent (re/im x planes)
   const uint32_t tile = (uint32_t)UM_M * KD * 2; // bytes of one 128 x KD bf16 operand
   const int QL = N + Lp + 8;                     // pair-array length (x + x' + 7 < QL)
-  // operand tiles: [c][A_hi, A_lo, B_hi, B_lo]
-  unsigned char* opnd = smem_raw;
+  // operand tiles: [set][c][A_hi, A_lo, B_hi, B_lo]
+  unsigned char* opnd0 = smem_raw;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int c0 = blockIdx.x * UM_CT;
   const int r0 = blockIdx.y * UM_R;
   const int nr = min(UM_R, a.nrot - r0);
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar[0])));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar[1])));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -149,8 +150,14 @@ __global__ void __launch_bounds__(UM_THREADS, 2) k_xpass_umma64(WaveArgs a, cons
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = s_tmem;
-  const uint32_t bar = smem_u32(&s_bar);
-  uint32_t phase = 0;
+  const uint32_t bars[2] = {smem_u32(&s_bar[0]), smem_u32(&s_bar[1])};
+  uint32_t ph[2] = {0u, 0u};
+  // double buffering: channel j is built into operand set j & 1 while the MMAs of channel j-1
+  // run on the other set; before building into a set, the MMAs of channel j-2 (same set)
+  // must have completed
+  const size_t set_bytes = (size_t)UM_CT * 4 * tile;
+  const int nbuf = nbuf_sets;
+  int it = 0;
   bool ok = true;
   for (int k = 0; k < K && ok; ++k) {
     // channel ranges of the chunk's rotations
@@ -173,6 +180,16 @@ __global__ void __launch_bounds__(UM_THREADS, 2) k_xpass_umma64(WaveArgs a, cons
       s_p[c][m] = pt[((size_t)(c0 + c) * K + k) * N + m];
     }
     if (!__syncthreads_or(mine)) continue;  // no rotation of the chunk touches channel k
+    const int b = (nbuf == 2) ? (it & 1) : 0;
+    if (it >= nbuf) {  // the set we are about to overwrite is still read by channel it - nbuf
+      const bool done = mbar_wait(bars[b], ph[b]);
+      ph[b] ^= 1u;
+      if (!__syncthreads_and(done ? 1 : 0)) {
+        ok = false;
+        break;
+      }
+    }
+    unsigned char* opnd = opnd0 + (size_t)b * set_bytes;
     // ---- pair arrays of the two columns: word j = (v[j], v[j+1]) of hi / lo parts of Re, Im,
     // -Re of P~ along x (circular), so any 8 consecutive Toeplitz entries are 4 aligned words
     for (int i = tid; i < UM_CT * QL; i += UM_THREADS) {
@@ -278,11 +295,16 @@ __global__ void __launch_bounds__(UM_THREADS, 2) k_xpass_umma64(WaveArgs a, cons
         }
       }
       s_flags[1] = 1;
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bars[b])
                    : "memory");
     }
-    const bool done = mbar_wait(bar, phase);
-    phase ^= 1u;
+    ++it;
+  }
+  // drain the commits not yet waited for (channels it-2 and it-1), oldest first
+  for (int j = (it >= nbuf ? it - nbuf : 0); j < it && ok; ++j) {
+    const int b = (nbuf == 2) ? (j & 1) : 0;
+    const bool done = mbar_wait(bars[b], ph[b]);
+    ph[b] ^= 1u;
     ok = __syncthreads_and(done ? 1 : 0) != 0;
   }
   if (!ok) {
@@ -290,7 +312,7 @@ __global__ void __launch_bounds__(UM_THREADS, 2) k_xpass_umma64(WaveArgs a, cons
   } else if (s_flags[1]) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     // ---- epilogue: TMEM -> shared staging [c][32 rotations][64 x'] float2 -> B
-    float2* stage = reinterpret_cast<float2*>(smem_raw);
+    float2* stage = reinterpret_cast<float2*>(opnd0);
     const int q = warp & 3, c = warp >> 2;
     const int row = 32 * q + lane;  // TMEM lane = operator row
     const int xp = row & (N - 1);
@@ -324,10 +346,18 @@ __global__ void __launch_bounds__(UM_THREADS, 2) k_xpass_umma64(WaveArgs a, cons
 
 }  // namespace
 
+// operand sets that fit: two (double buffering, one CTA per SM) when they fit in 200 KB
+int umma_sets(int Lb) {
+  const int Lp = (Lb + 7) & ~7;
+  const size_t set = (size_t)UM_CT * 4 * UM_M * (2 * Lp) * 2;
+  return (2 * set + 1024 <= 200 * 1024) ? 2 : 1;
+}
+
 size_t xpass_umma_smem_bytes(int Lb) {
   const int Lp = (Lb + 7) & ~7;
+  const size_t set = (size_t)UM_CT * 4 * UM_M * (2 * Lp) * 2;
+  const size_t need = (size_t)umma_sets(Lb) * set + 1024;
   // at least 90 KB so that at most two CTAs (2 x 256 TMEM columns) share an SM
-  const size_t need = (size_t)UM_CT * 4 * UM_M * (2 * Lp) * 2 + 1024;
   return need < 90 * 1024 ? 90 * 1024 : need;
 }
 
@@ -345,7 +375,7 @@ cudaError_t launch_xpass_umma(const WaveArgs& a, const float2* pt, cudaStream_t 
   if (e != cudaSuccess) return e;
   constexpr int NCOL = 64 * 33;
   dim3 grid(NCOL / UM_CT, (a.nrot + UM_R - 1) / UM_R);
-  k_xpass_umma64<<<grid, UM_THREADS, sm, s>>>(a, pt, Lp);
+  k_xpass_umma64<<<grid, UM_THREADS, sm, s>>>(a, pt, Lp, umma_sets(a.Lb));
   return cudaGetLastError();
 }
 
