@@ -448,6 +448,29 @@ def serving_sample(w, rec_unused, secs: float) -> dict:
     return res
 
 
+def serve_sweep(args):
+    """Config 3: one resident 96^3 receptor (6,000 atoms in a 48 A cube, K = 9), requests with
+    ligands of 10-80 atoms, 10-200 conformers, 500-5,000 rotations, Poisson arrivals at five
+    rates; both forms. Prints one JSON line per (form, rate)."""
+    from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP32, Receptor, synth
+    from cdocker_b200.serving import Server, make_requests, poisson_arrivals, run_load
+    grids, mid, length = synth.make_receptor(96, 6000, 48.0, seed=0)
+    secs = max(2.0, args.serve_secs)
+    for form_name, form in (("fp32", CDK_FORM_FP32), ("bf16x3_tensor_core", CDK_FORM_BF16X3)):
+        with Receptor(grids, 0.5, max_atoms=96, form=form) as rec:
+            for rate in (2.0, 5.0, 10.0, 20.0, 40.0):
+                arr = poisson_arrivals(rate, secs, seed=int(rate * 10))
+                reqs = make_requests(len(arr), int(rate * 100), 0.5, length, synth.PROBE_RADII,
+                                     atoms=(10, 80), confs=(10, 200), rots=(500, 5000))
+                with Server(rec, arena_bytes=1 << 30, wave_rotations=1024, max_atoms=96,
+                            max_box=40) as srv:
+                    res = run_load(srv, reqs, arr)
+                    st = srv.stats()
+                res.update({"config": "serving, 96^3 K=9, 6,000-atom receptor", "form": form_name,
+                            "rate_hz": rate, "waves": st["waves"]})
+                print(json.dumps(res), flush=True)
+
+
 def profile_run(args):
     """One warm-up and one timed search of `--profile-run` rotations (first conformers of the
     config-1 workload), per-kernel device times from events around every launch."""
@@ -495,6 +518,9 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--forms", default="both", choices=["both", "fp32", "bf16x3_tensor_core"])
     ap.add_argument("--serve-secs", type=float, default=3.0)
+    ap.add_argument("--serve-sweep", action="store_true",
+                    help="config 3: 96^3 receptor, Poisson request streams at 5 rates; one JSON "
+                         "line per rate (not the bench line)")
     ap.add_argument("--profile-run", type=int, default=0,
                     help="run one search of this many rotations with per-kernel events and "
                          "print the timings (the small case used for ncu captures)")
@@ -508,6 +534,9 @@ def main():
         return
     if args.profile_run:
         profile_run(args)
+        return
+    if args.serve_sweep:
+        serve_sweep(args)
         return
     import torch
     import torch.distributed as dist

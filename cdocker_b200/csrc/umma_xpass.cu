@@ -58,6 +58,15 @@ __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bflo
   lo = __float2bfloat16_rn(v - __bfloat162float(hi));
 }
 
+// (a, b) -> bf16x2 hi = round(a, b), lo = round(a - hi, b - hi): a in the low half
+__device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
 __device__ __forceinline__ uint32_t pack2(__nv_bfloat16 a, __nv_bfloat16 b) {
   return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
 }
@@ -107,7 +116,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
 }
 
 // n = 64 only: the real-ified operator has exactly 128 rows
-__global__ void __launch_bounds__(UM_THREADS, 1) k_xpass_umma64(WaveArgs a, const float2* __restrict__ pt,
+__global__ void __launch_bounds__(UM_THREADS, 2) k_xpass_umma64(WaveArgs a, const float2* __restrict__ pt,
                                                               int Lp, int nbuf_sets) {
   constexpr int N = 64;
   constexpr int NZH = N / 2 + 1;
@@ -193,85 +202,81 @@ __global__ void __launch_bounds__(UM_THREADS, 1) k_xpass_umma64(WaveArgs a, cons
     // ---- pair arrays of the two columns: word j = (v[j], v[j+1]) of hi / lo parts of Re, Im,
     // -Re of P~ along x (circular), so any 8 consecutive Toeplitz entries are 4 aligned words
     for (int i = tid; i < UM_CT * QL; i += UM_THREADS) {
-      const int c = i / QL, j = i - c * QL;
+      const int c = i >= QL;
+      const int j = i - c * QL;
       const float2 p0 = s_p[c][j & (N - 1)], p1 = s_p[c][(j + 1) & (N - 1)];
-      __nv_bfloat16 h0, l0, h1, l1;
       uint32_t* q = s_q + (size_t)c * 6 * QL + j;
-      split_bf16(p0.x, h0, l0);
-      split_bf16(p1.x, h1, l1);
-      q[0 * QL] = pack2(h0, h1);
-      q[1 * QL] = pack2(l0, l1);
-      split_bf16(p0.y, h0, l0);
-      split_bf16(p1.y, h1, l1);
-      q[2 * QL] = pack2(h0, h1);
-      q[3 * QL] = pack2(l0, l1);
-      split_bf16(-p0.x, h0, l0);
-      split_bf16(-p1.x, h1, l1);
-      q[4 * QL] = pack2(h0, h1);
-      q[5 * QL] = pack2(l0, l1);
+      uint32_t h, l;
+      split2(p0.x, p1.x, h, l);
+      q[0 * QL] = h;
+      q[1 * QL] = l;
+      split2(p0.y, p1.y, h, l);
+      q[2 * QL] = h;
+      q[3 * QL] = l;
+      split2(-p0.x, -p1.x, h, l);
+      q[4 * QL] = h;
+      q[5 * QL] = l;
     }
     __syncthreads();
     // ---- Toeplitz operators: one 16-byte core-matrix row (8 consecutive K = x values of one
-    // part) per item; rows < 64: [Tr | Ti], rows >= 64: [Ti | -Tr]
+    // part) per item; rows < 64: [Tr | Ti], rows >= 64: [Ti | -Tr]. This thread's row is fixed
+    // (tid & 127): lanes take consecutive rows, so the 16-byte stores do not conflict.
     {
       const int ng = KD / 8;  // k-groups
-      for (int i = tid; i < UM_CT * ng * UM_M; i += UM_THREADS) {
-        const int row = i % UM_M;  // lanes take consecutive rows: conflict-free 16-byte stores
-        const int t = i / UM_M;
-        const int g = t % ng, c = t / ng;
+      const int row = tid & (UM_M - 1);
+      const bool imrow = row >= N;
+      const int xr = row & (N - 1);
+      const uint32_t rowoff = (uint32_t)((row >> 3) * 128 + (row & 7) * 16);
+      for (int t = tid >> 7; t < UM_CT * ng; t += UM_THREADS / UM_M) {
+        const int c = t >= ng;
+        const int g = t - c * ng;
         const int kk = 8 * g;
         const int part = kk >= Lp;
         const int x0 = kk - part * Lp;
-        const bool imrow = row >= N;
         // which pair array: 0/1 Re, 2/3 Im, 4/5 -Re
         const int sel = imrow ? (part ? 4 : 2) : (part ? 2 : 0);
-        const uint32_t* qh = s_q + ((size_t)c * 6 + sel) * QL + x0 + (row & (N - 1));
+        const uint32_t* qh = s_q + (c * 6 + sel) * QL + x0 + xr;
         const uint32_t* ql = qh + QL;
-        const uint4 vh = make_uint4(qh[0], qh[2], qh[4], qh[6]);
-        const uint4 vl = make_uint4(ql[0], ql[2], ql[4], ql[6]);
-        unsigned char* base = opnd + (size_t)c * 4 * tile + kmaj_off(row, kk);
-        *reinterpret_cast<uint4*>(base + 0 * tile) = vh;
-        *reinterpret_cast<uint4*>(base + 1 * tile) = vl;
+        unsigned char* base = opnd + c * 4 * tile + g * (UM_M / 8) * 128 + rowoff;
+        *reinterpret_cast<uint4*>(base) = make_uint4(qh[0], qh[2], qh[4], qh[6]);
+        *reinterpret_cast<uint4*>(base + tile) = make_uint4(ql[0], ql[2], ql[4], ql[6]);
       }
     }
     // ---- ligand operand: one rotation x 8 consecutive x planes (both columns, re and im) per
-    // item; lanes take consecutive rotations
-    for (int i = tid; i < UM_R * (Lp / 8); i += UM_THREADS) {
-      const int rr = i % UM_R;
-      const int x0 = 8 * (i / UM_R);
+    // item; this thread's rotation is fixed (tid & 127), lanes take consecutive rotations
+    {
+      const int rr = tid & (UM_R - 1);
       const int lo = s_rng[rr][0], hi = s_rng[rr][1];
-      float4 v[8];
+      const float2* src = a.A + (((size_t)(r0 + rr) * K + k) * a.Lb) * NCOL + c0;
+      const uint32_t rowoff = (uint32_t)((rr >> 3) * 128 + (rr & 7) * 16);
+      const bool live = rr < nr;
+      for (int xg = tid >> 7; xg < Lp / 8; xg += UM_THREADS / UM_R) {
+        const int x0 = 8 * xg;
+        float4 v[8];
 #pragma unroll
-      for (int d = 0; d < 8; ++d) {
-        const int x = x0 + d;
-        v[d] = (rr < nr && x >= lo && x <= hi)
-                   ? *reinterpret_cast<const float4*>(
-                         a.A + (((size_t)(r0 + rr) * K + k) * a.Lb + x) * NCOL + c0)
-                   : make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-#pragma unroll
-      for (int c = 0; c < UM_CT; ++c) {
-        uint32_t reh[4], rel[4], imh[4], iml[4];
-#pragma unroll
-        for (int d = 0; d < 8; d += 2) {
-          const float r0v = c ? v[d].z : v[d].x, i0v = c ? v[d].w : v[d].y;
-          const float r1v = c ? v[d + 1].z : v[d + 1].x, i1v = c ? v[d + 1].w : v[d + 1].y;
-          __nv_bfloat16 h0, l0, h1, l1;
-          split_bf16(r0v, h0, l0);
-          split_bf16(r1v, h1, l1);
-          reh[d / 2] = pack2(h0, h1);
-          rel[d / 2] = pack2(l0, l1);
-          split_bf16(i0v, h0, l0);
-          split_bf16(i1v, h1, l1);
-          imh[d / 2] = pack2(h0, h1);
-          iml[d / 2] = pack2(l0, l1);
+        for (int d = 0; d < 8; ++d) {
+          const int x = x0 + d;
+          v[d] = (live && x >= lo && x <= hi) ? *reinterpret_cast<const float4*>(src + (size_t)x * NCOL)
+                                              : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        unsigned char* base = opnd + (size_t)c * 4 * tile;
-        const uint32_t ore = kmaj_off(rr, x0), oim = kmaj_off(rr, Lp + x0);
-        *reinterpret_cast<uint4*>(base + 2 * tile + ore) = make_uint4(reh[0], reh[1], reh[2], reh[3]);
-        *reinterpret_cast<uint4*>(base + 3 * tile + ore) = make_uint4(rel[0], rel[1], rel[2], rel[3]);
-        *reinterpret_cast<uint4*>(base + 2 * tile + oim) = make_uint4(imh[0], imh[1], imh[2], imh[3]);
-        *reinterpret_cast<uint4*>(base + 3 * tile + oim) = make_uint4(iml[0], iml[1], iml[2], iml[3]);
+        const uint32_t ore = (uint32_t)xg * (UM_M / 8) * 128 + rowoff;               // K = x0
+        const uint32_t oim = (uint32_t)(Lp / 8 + xg) * (UM_M / 8) * 128 + rowoff;    // K = Lp + x0
+#pragma unroll
+        for (int c = 0; c < UM_CT; ++c) {
+          uint32_t reh[4], rel[4], imh[4], iml[4];
+#pragma unroll
+          for (int d = 0; d < 8; d += 2) {
+            const float r0v = c ? v[d].z : v[d].x, i0v = c ? v[d].w : v[d].y;
+            const float r1v = c ? v[d + 1].z : v[d + 1].x, i1v = c ? v[d + 1].w : v[d + 1].y;
+            split2(r0v, r1v, reh[d / 2], rel[d / 2]);
+            split2(i0v, i1v, imh[d / 2], iml[d / 2]);
+          }
+          unsigned char* base = opnd + c * 4 * tile;
+          *reinterpret_cast<uint4*>(base + 2 * tile + ore) = make_uint4(reh[0], reh[1], reh[2], reh[3]);
+          *reinterpret_cast<uint4*>(base + 3 * tile + ore) = make_uint4(rel[0], rel[1], rel[2], rel[3]);
+          *reinterpret_cast<uint4*>(base + 2 * tile + oim) = make_uint4(imh[0], imh[1], imh[2], imh[3]);
+          *reinterpret_cast<uint4*>(base + 3 * tile + oim) = make_uint4(iml[0], iml[1], iml[2], iml[3]);
+        }
       }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -350,7 +355,10 @@ __global__ void __launch_bounds__(UM_THREADS, 1) k_xpass_umma64(WaveArgs a, cons
 int umma_sets(int Lb) {
   const int Lp = (Lb + 7) & ~7;
   const size_t set = (size_t)UM_CT * 4 * UM_M * (2 * Lp) * 2;
-  return (2 * set + 1024 <= 200 * 1024) ? 2 : 1;
+  // Two sets keep the tensor pipe fed within one CTA but halve the CTAs per SM; measured on
+  // B200 at 64^3 (config 1) one set with two CTAs per SM ran 1.5x faster, so one set it is.
+  (void)set;
+  return 1;
 }
 
 size_t xpass_umma_smem_bytes(int Lb) {
