@@ -27,7 +27,8 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas"
 CXX_FLAGS = ["-O2", "-std=c++14", "-fPIC", "-ffp-contract=off", "-Wno-deprecated-declarations",
              "-pthread"]
 
-CU_SOURCES = ["search_kernels.cu", "compat_kernels.cu", "capi.cu", "noalloc.cu", "server.cu", "tc_xpass.cu", "umma_xpass.cu"]
+CU_SOURCES = ["search_kernels.cu", "compat_kernels.cu", "capi.cu", "noalloc.cu", "server.cu", "tc_xpass.cu", "umma_xpass.cu",
+              "cluster.cu"]
 CPP_SOURCES = ["host/reference_api.cpp"]
 
 

@@ -249,6 +249,34 @@ std::vector<size_t> sort_index(const std::vector<float>& v) {
   return id;
 }
 
+std::vector<size_t> sort_index(const std::vector<double>& v) {
+  std::vector<size_t> id(v.size());
+  for (size_t i = 0; i < id.size(); ++i) id[i] = i;
+  std::sort(id.begin(), id.end(), [&v](size_t a, size_t b) { return v[a] < v[b]; });
+  return id;
+}
+
+int SelectDiverseConformations(int nConf, int nAtom, const double* coors,
+                               const std::vector<double>& energy, int maxNumOfConformations,
+                               double*& coorsConformers, double cutOff) {
+  if ((int)energy.size() != nConf) throw Error(CDK_ERR_INVALID, "energy.size() != nConf");
+  std::vector<int> centers((size_t)std::max(nConf, 1));
+  int n = 0;
+  const int rc = cdk_cluster_conformers(nConf, nAtom, coors, energy.data(), nullptr, cutOff,
+                                        maxNumOfConformations, centers.data(), &n);
+  if (rc) {
+    char msg[512];
+    cdk_last_error(msg, sizeof msg);
+    throw Error(rc, msg);
+  }
+  delete[] coorsConformers;
+  coorsConformers = new double[(size_t)n * nAtom * 3];
+  for (int i = 0; i < n; ++i)
+    std::memcpy(coorsConformers + (size_t)i * nAtom * 3, coors + (size_t)centers[i] * nAtom * 3,
+                sizeof(double) * nAtom * 3);
+  return n;
+}
+
 TranRotaSearch::TranRotaSearch(int xdim, int ydim, int zdim, float spacing, int K,
                                const float* grids, const cdk_opts* opts) {
   int rc = cdk_ctx_create(xdim, ydim, zdim, spacing, K, grids, opts, &ctx_);

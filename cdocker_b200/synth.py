@@ -125,3 +125,57 @@ def make_workload(name: str = "c0_32", seed: int = 0, n_conf: int | None = None,
                     grids=np.ascontiguousarray(grids), quats=quats,
                     meta={"seed": seed, "receptor_atoms": n_rec, "box": box,
                           "ligand_atoms": n_lig, "ligand_radius": lig_r})
+
+
+def conformer_ensemble(seed: int, n_atoms: int = 40, n_conf: int = 1000, n_rotors: int = 6,
+                       bond: float = 1.5):
+    """Random-rotor conformers of one chain ligand, like the 1000 random conformers the
+    reference draws before clustering (src/GeneDiverseConformations.cpp:30-47): a chain with
+    tetrahedral bond angles; per conformer every rotor bond is set to a uniform angle in
+    (-pi, pi) (the atoms past the bond turn about it), then the whole conformer gets a random
+    rigid rotation and translation, so that only superposition sees the shape. Energies are a
+    seeded smooth function of the shape (compact conformers lower) plus noise.
+    Returns coords [n_conf][n_atoms][3] float64 and energies [n_conf] float64."""
+    rng = np.random.default_rng(seed)
+    # chain with 109.5 degree bond angles and random dihedrals
+    pts = [np.zeros(3), np.array([bond, 0.0, 0.0])]
+    ang = np.deg2rad(109.5)
+    prev = np.array([0.0, 1.0, 0.0])
+    for _ in range(n_atoms - 2):
+        u = pts[-1] - pts[-2]
+        u /= np.linalg.norm(u)
+        w = np.cross(u, prev)
+        if np.linalg.norm(w) < 1e-6:
+            w = np.cross(u, [0.0, 0.0, 1.0])
+        w /= np.linalg.norm(w)
+        v = np.cross(w, u)
+        phi = rng.uniform(-np.pi, np.pi)
+        d = -np.cos(ang) * u + np.sin(ang) * (np.cos(phi) * v + np.sin(phi) * w)
+        prev = u
+        pts.append(pts[-1] + bond * d)
+    base = np.array(pts)
+    rotors = np.sort(rng.choice(np.arange(1, n_atoms - 2), size=min(n_rotors, n_atoms - 3),
+                                replace=False))
+
+    def axis_rot(axis, t):
+        axis = axis / np.linalg.norm(axis)
+        K = np.array([[0, -axis[2], axis[1]], [axis[2], 0, -axis[0]], [-axis[1], axis[0], 0]])
+        return np.eye(3) + np.sin(t) * K + (1 - np.cos(t)) * (K @ K)
+
+    out = np.empty((n_conf, n_atoms, 3))
+    energy = np.empty(n_conf)
+    for c in range(n_conf):
+        x = base.copy()
+        for r in rotors:
+            R = axis_rot(x[r + 1] - x[r], rng.uniform(-np.pi, np.pi))
+            x[r + 1:] = (x[r + 1:] - x[r + 1]) @ R.T + x[r + 1]
+        rg = np.sqrt(((x - x.mean(0)) ** 2).sum(1).mean())
+        energy[c] = 5.0 * rg + rng.normal(0.0, 1.0)
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        w_, a_, b_, c_ = q
+        Rr = np.array([[1 - 2 * (b_ * b_ + c_ * c_), 2 * (a_ * b_ - c_ * w_), 2 * (a_ * c_ + b_ * w_)],
+                       [2 * (a_ * b_ + c_ * w_), 1 - 2 * (a_ * a_ + c_ * c_), 2 * (b_ * c_ - a_ * w_)],
+                       [2 * (a_ * c_ - b_ * w_), 2 * (b_ * c_ + a_ * w_), 1 - 2 * (a_ * a_ + b_ * b_)]])
+        out[c] = x @ Rr.T + rng.uniform(-10, 10, size=3)
+    return out, energy

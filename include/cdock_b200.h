@@ -156,6 +156,26 @@ int cdk_vdw_slots(int nAtom, const float* radii, int nVdw, const float* gridRadi
 int cdk_pose_coordinates(int nAtom, const float* coor, const float* quat, const double* gridMin,
                          float spacing, const int* idx, double* out);
 
+/* Diverse-conformer selection: the greedy leader clustering of GeneDiverseConformations
+ * (src/GeneDiverseConformations.cpp:84-111), on the GPU. Conformers coor[nConf][nAtom][3]
+ * (double, Angstrom, as OBMol coordinates) are taken in energy order (sort_index<double>,
+ * include/GeneDiverseConformations.h:9-20); the lowest is the first centre; each following one
+ * is a new centre when its superposition RMSD to every centre so far is > cutoff (the reference
+ * uses 1.5). The loop stops when the centre count equals maxCenters, tested after each
+ * candidate from the second on, as the reference does. RMSD: minimum over rotations after
+ * centring, over the atoms with atomMask[a] != 0 (NULL = all atoms), without symmetry
+ * permutations (OBAlign, absent here, also tries automorphisms of symmetric molecules).
+ * centers: capacity nConf; receives conformer indices in selection order, *nCenters their
+ * count. nConf <= 32768. Uses the current CUDA device. */
+int cdk_cluster_conformers(int nConf, int nAtom, const double* coor, const double* energy,
+                           const unsigned char* atomMask, double cutoff, int maxCenters,
+                           int* centers, int* nCenters);
+
+/* The RMSD the clustering compares, for all pairs: out[i*nConf + j] = min RMSD of conformer i
+ * (reference) and j (target) after superposition. nConf <= 16384. */
+int cdk_pair_rmsd(int nConf, int nAtom, const double* coor, const unsigned char* atomMask,
+                  double* out);
+
 /* ReadGrids (src/ReadGrids.cpp:6-68): header ints [numGrids, x, y, z], floats
  * [midx, midy, midz, xlen, ylen, zlen, spacing, restraint_k]; radii (numGrids-1) and values
  * (numGrids*x*y*z) are written when the capacities suffice. Pass NULL buffers to size first. */

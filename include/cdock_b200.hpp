@@ -49,6 +49,17 @@ void ReadGrids(int& numOfGrids, int& xdim, int& ydim, int& zdim, float& midx, fl
 // indices of v sorted by value (std::sort, strict <; include/GeneDiverseConformations.h:9-20)
 std::vector<size_t> sort_index(const std::vector<float>& v);
 
+// indices of v sorted by value, for the conformer energies (the double instantiation)
+std::vector<size_t> sort_index(const std::vector<double>& v);
+
+// The centre selection of GeneDiverseConformations (src/GeneDiverseConformations.cpp:84-122)
+// for conformers already generated and minimised: coors [nConf][nAtom][3] and their energies.
+// Like the reference, coorsConformers is (re)allocated with new[] and receives the centres'
+// coordinates in selection order; the return value is the number of centres.
+int SelectDiverseConformations(int nConf, int nAtom, const double* coors,
+                               const std::vector<double>& energy, int maxNumOfConformations,
+                               double*& coorsConformers, double cutOff = 1.5);
+
 // The search with a resident receptor: construct once per receptor grid set, then Search()
 // per conformer batch. Results as the reference's minEnergyQuaternionsUsed / minEnergyIdx*.
 class TranRotaSearch {

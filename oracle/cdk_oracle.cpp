@@ -355,3 +355,148 @@ void orc_sort_index(int n, const float* v, long* out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Diverse-conformer selection (src/GeneDiverseConformations.cpp:84-111): greedy leader
+// clustering in energy order (sort_index<double>, include/GeneDiverseConformations.h:9-20) with
+// RMSD <= cutOff (1.5) after optimal superposition. OBAlign (OpenBabel, absent here) supplies the
+// reference's RMSD; this restatement computes the minimum RMSD over rotations of the centred
+// atom sets, in double, by Horn's quaternion key matrix and Newton's method on its
+// characteristic polynomial, one operation at a time in a fixed order (no contraction). The
+// same recipe, op for op, is what the library's GPU kernels evaluate.
+namespace {
+
+void center_conf(const double* p, const std::vector<int>& sel, std::vector<double>& X, double& G) {
+  const int n = (int)sel.size();
+  double s[3] = {0.0, 0.0, 0.0};
+  for (int i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) s[d] = s[d] + p[sel[i] * 3 + d];
+  double m[3];
+  for (int d = 0; d < 3; ++d) m[d] = s[d] / (double)n;
+  X.assign((size_t)n * 3, 0.0);
+  double g = 0.0;
+  for (int i = 0; i < n; ++i) {
+    double v[3];
+    for (int d = 0; d < 3; ++d) {
+      v[d] = p[sel[i] * 3 + d] - m[d];
+      X[(size_t)i * 3 + d] = v[d];
+    }
+    g = g + ((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]);
+  }
+  G = g;
+}
+
+double qcp_rmsd(const double* A, double Ga, const double* B, double Gb, int n) {
+  double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int a = 0; a < n; ++a)
+    for (int p = 0; p < 3; ++p)
+      for (int q = 0; q < 3; ++q) S[p * 3 + q] = S[p * 3 + q] + A[a * 3 + p] * B[a * 3 + q];
+  const double Sxx = S[0], Sxy = S[1], Sxz = S[2], Syx = S[3], Syy = S[4], Syz = S[5],
+               Szx = S[6], Szy = S[7], Szz = S[8];
+  double N[4][4];
+  N[0][0] = (Sxx + Syy) + Szz;
+  N[0][1] = Syz - Szy;
+  N[0][2] = Szx - Sxz;
+  N[0][3] = Sxy - Syx;
+  N[1][1] = (Sxx - Syy) - Szz;
+  N[1][2] = Sxy + Syx;
+  N[1][3] = Szx + Sxz;
+  N[2][2] = (Syy - Sxx) - Szz;
+  N[2][3] = Syz + Szy;
+  N[3][3] = (Szz - Sxx) - Syy;
+  N[1][0] = N[0][1];
+  N[2][0] = N[0][2];
+  N[3][0] = N[0][3];
+  N[2][1] = N[1][2];
+  N[3][1] = N[1][3];
+  N[3][2] = N[2][3];
+  double p2 = 0.0;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) p2 = p2 + N[i][j] * N[i][j];
+  double p3 = 0.0;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      const double n2 = ((N[i][0] * N[0][j] + N[i][1] * N[1][j]) + N[i][2] * N[2][j]) + N[i][3] * N[3][j];
+      p3 = p3 + n2 * N[j][i];
+    }
+  auto mA = [&](int j, int k) { return N[0][j] * N[1][k] - N[0][k] * N[1][j]; };
+  auto mB = [&](int j, int k) { return N[2][j] * N[3][k] - N[2][k] * N[3][j]; };
+  double det = mA(0, 1) * mB(2, 3) - mA(0, 2) * mB(1, 3);
+  det = det + mA(0, 3) * mB(1, 2);
+  det = det + mA(1, 2) * mB(0, 3);
+  det = det - mA(1, 3) * mB(0, 2);
+  det = det + mA(2, 3) * mB(0, 1);
+  const double c2 = -(p2 * 0.5), c1 = -(p3 / 3.0), c0 = det;
+  double l = (Ga + Gb) * 0.5;
+  for (int it = 0; it < 50; ++it) {
+    const double l2 = l * l;
+    const double P = ((l2 + c2) * l + c1) * l + c0;
+    const double dP = (4.0 * l2 + 2.0 * c2) * l + c1;
+    if (dP == 0.0) break;
+    const double ln = l - P / dP;
+    if (std::fabs(ln - l) <= 1e-11 * std::fabs(ln)) {
+      l = ln;
+      break;
+    }
+    l = ln;
+  }
+  double e = ((Ga + Gb) - 2.0 * l) / (double)n;
+  if (!(e > 0.0)) e = 0.0;
+  return std::sqrt(e);
+}
+
+std::vector<int> mask_sel(int nAtom, const unsigned char* mask) {
+  std::vector<int> sel;
+  for (int a = 0; a < nAtom; ++a)
+    if (!mask || mask[a]) sel.push_back(a);
+  return sel;
+}
+
+}  // namespace
+
+extern "C" {
+
+// out[i*nConf + j] = rmsd(reference i, target j)
+void orc_pair_rmsd(int nConf, int nAtom, const double* coor, const unsigned char* mask, double* out) {
+  const std::vector<int> sel = mask_sel(nAtom, mask);
+  const int n = (int)sel.size();
+  std::vector<std::vector<double>> X(nConf);
+  std::vector<double> G(nConf);
+  for (int c = 0; c < nConf; ++c) center_conf(coor + (size_t)c * nAtom * 3, sel, X[c], G[c]);
+  for (int i = 0; i < nConf; ++i)
+    for (int j = 0; j < nConf; ++j) out[(size_t)i * nConf + j] = qcp_rmsd(X[i].data(), G[i], X[j].data(), G[j], n);
+}
+
+// the reference's loop (src/GeneDiverseConformations.cpp:84-111), candidate = reference mol
+// (align.SetRefMol, :96), centre = target (:100); returns the centre count
+int orc_cluster_conformers(int nConf, int nAtom, const double* coor, const double* energy,
+                           const unsigned char* mask, double cutOff, int maxNum, int* centers) {
+  const std::vector<int> sel = mask_sel(nAtom, mask);
+  const int n = (int)sel.size();
+  std::vector<double> e(energy, energy + nConf);
+  std::vector<size_t> idx(e.size());
+  for (size_t i = 0; i != idx.size(); ++i) idx[i] = i;
+  std::sort(idx.begin(), idx.end(), [&e](size_t i1, size_t i2) { return e[i1] < e[i2]; });
+  std::vector<std::vector<double>> X(nConf);
+  std::vector<double> G(nConf);
+  for (int c = 0; c < nConf; ++c) center_conf(coor + (size_t)c * nAtom * 3, sel, X[c], G[c]);
+  std::vector<size_t> idxCenter;
+  idxCenter.push_back(idx[0]);
+  for (int i = 1; i < nConf; i++) {
+    const size_t r = idx[i];
+    bool ifNewCenter = true;
+    for (size_t j = 0; j < idxCenter.size(); j++) {
+      const size_t t = idxCenter[j];
+      if (qcp_rmsd(X[r].data(), G[r], X[t].data(), G[t], n) <= cutOff) {
+        ifNewCenter = false;
+        break;
+      }
+    }
+    if (ifNewCenter) idxCenter.push_back(idx[i]);
+    if ((int)idxCenter.size() == maxNum) break;
+  }
+  for (size_t i = 0; i < idxCenter.size(); ++i) centers[i] = (int)idxCenter[i];
+  return (int)idxCenter.size();
+}
+
+}  // extern "C"

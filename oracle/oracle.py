@@ -86,6 +86,11 @@ def orc() -> C.CDLL:
         L.orc_energy_map.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _fp, C.c_int,
                                      _fp, _fp, _fp, _ip, _fp, _ip, _dp, C.c_long]
         L.orc_sort_index.argtypes = [C.c_int, _fp, _lp]
+        L.orc_pair_rmsd.argtypes = [C.c_int, C.c_int, _dp, C.c_void_p, _dp]
+        L.orc_pair_rmsd.restype = None
+        L.orc_cluster_conformers.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_void_p, C.c_double,
+                                             C.c_int, _ip]
+        L.orc_cluster_conformers.restype = C.c_int
         _orc = L
     return _orc
 
@@ -240,3 +245,45 @@ def fft64_search(grids, spacing, coor, charge, eps, slot, quats):
             minE[r] = e.reshape(-1)[flat]
             idx[r] = np.unravel_index(flat, e.shape)
     return minE, idx
+
+
+def _mask_ptr(mask):
+    if mask is None:
+        return None, None
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    return m, m.ctypes.data_as(C.c_void_p)
+
+
+def pair_rmsd(coor, mask=None):
+    """All-pairs superposition RMSD (reference i, target j), the clustering's recipe."""
+    coor = np.ascontiguousarray(coor, dtype=np.float64)
+    nconf, natom = coor.shape[:2]
+    out = np.empty((nconf, nconf), np.float64)
+    m, mp = _mask_ptr(mask)
+    orc().orc_pair_rmsd(nconf, natom, coor.ctypes.data_as(_dp), mp, out.ctypes.data_as(_dp))
+    return out
+
+
+def cluster_conformers(coor, energy, cutoff=1.5, max_num=100, mask=None):
+    """Greedy leader clustering of src/GeneDiverseConformations.cpp:84-111; centre indices."""
+    coor = np.ascontiguousarray(coor, dtype=np.float64)
+    energy = np.ascontiguousarray(energy, dtype=np.float64)
+    nconf, natom = coor.shape[:2]
+    out = np.empty(max(nconf, 1), np.int32)
+    m, mp = _mask_ptr(mask)
+    n = orc().orc_cluster_conformers(nconf, natom, coor.ctypes.data_as(_dp),
+                                     energy.ctypes.data_as(_dp), mp, cutoff, max_num,
+                                     out.ctypes.data_as(_ip))
+    return out[:n].copy()
+
+
+def kabsch_rmsd(a, b):
+    """Independent form of the superposition RMSD (SVD of the correlation, numpy)."""
+    a = a - a.mean(axis=0)
+    b = b - b.mean(axis=0)
+    h = a.T @ b
+    u, s, vt = np.linalg.svd(h)
+    d = np.sign(np.linalg.det(h)) or 1.0
+    lam = s[0] + s[1] + d * s[2]
+    e = ((a * a).sum() + (b * b).sum() - 2.0 * lam) / len(a)
+    return float(np.sqrt(max(e, 0.0)))
