@@ -129,7 +129,7 @@ class Receptor:
     def __init__(self, grids, spacing: float, device: int = 0, wave_rotations: int = 0,
                  max_atoms: int = 256, col_tile: int = 0, form: int = L.CDK_FORM_FP32,
                  use_graphs: int = 0, profile: bool = False, fft_planes: bool = False,
-                 autotune: bool = False, tc_mma_sync: bool = False):
+                 autotune: bool = False, tc_mma_sync: bool = False, tc_build: bool = False):
         g = _f32(grids)
         if g.ndim != 4:
             raise ValueError("grids must be [K, n, n, n]")
@@ -147,7 +147,7 @@ class Receptor:
         opts.reserved[0] = 1 if profile else 0
         opts.reserved[1] = 1 if fft_planes else 0
         opts.reserved[2] = 1 if autotune else 0
-        opts.reserved[3] = 1 if tc_mma_sync else 0
+        opts.reserved[3] = 1 if tc_mma_sync else (2 if tc_build else 0)
         h = C.c_void_p()
         L.check(lib.cdk_ctx_create(g.shape[1], g.shape[2], g.shape[3], self.spacing, self.K,
                                    _pf(g), C.byref(opts), C.byref(h)))
@@ -215,12 +215,14 @@ class Receptor:
         return out
 
     def stats(self) -> dict:
-        out = np.zeros(16, np.float64)
-        L.check(L.lib().cdk_ctx_stats(self._h, out.ctypes.data_as(_dp), 16))
+        out = np.zeros(17, np.float64)
+        L.check(L.lib().cdk_ctx_stats(self._h, out.ctypes.data_as(_dp), 17))
         names = ["prep", "spread_yz", "xpass", "yz_inv_argmin", "finalize"]
         return {"launches": int(out[0]), "waves": int(out[1]), "rotations": int(out[2]),
                 "device_ms": float(out[3]), "box": int(out[4]), "wave_rotations": int(out[5]),
                 "planes_spread": int(out[6]), "planes_window": int(out[7]),
                 "kernel_ms": {k: float(v) for k, v in zip(names, out[8:13])},
                 "col_tile": int(out[13]), "rotations_per_cta": int(out[14]),
-                "graph_state": int(out[15])}
+                "graph_state": int(out[15]),
+                "xpass_kind": ["fp32_radix", "mma_sync", "tcgen05_build",
+                               "tcgen05_streamed"][int(out[16])]}

@@ -107,6 +107,7 @@ struct cdk_ctx {
   float* d_grids = nullptr;   // [K][n^3], kept for the FP64 re-score
   float2* d_phat = nullptr;   // [n][K][ncol]
   float2* d_ptilde = nullptr; // [ncol][K][n] receptor transformed over (y,z) only, x n (BF16X3 form)
+  void* d_top = nullptr;      // operator image of the streamed tensor-core x pass (built on first use)
   float2* d_tw = nullptr;     // [n]
   int* d_kyof = nullptr;      // [n] natural frequency at each digit-reversed position
   Arena wave;                 // per-wave scratch
@@ -165,7 +166,7 @@ int autotune_xpass(cdk_ctx* c, WaveArgs a, const RotDesc* d_rots, long nRot, int
   CDK_CUDA(launch_spread_yz(a, s));
   struct Cand { int ct, chunk; };
   std::vector<Cand> cands;
-  if (tc && c->opts.reserved[3] == 0 && umma_supported(c->n, a.Lb)) {
+  if (tc && c->opts.reserved[3] != 1 && umma_supported(c->n, a.Lb)) {
     cands.push_back({a.col_tile, 0});  // fixed 128-rotation tiles
   } else if (tc) {
     for (int ch : {32, 64, 128, 256}) cands.push_back({a.col_tile, ch});
@@ -189,7 +190,7 @@ int autotune_xpass(cdk_ctx* c, WaveArgs a, const RotDesc* d_rots, long nRot, int
     float ms = 0.f, total = 0.f;
     for (int rep = 0; rep < 2; ++rep) {
       CDK_CUDA(cudaEventRecord(e0, s));
-      if (tc && c->opts.reserved[3] == 0 && umma_supported(c->n, a.Lb))
+      if (tc && c->opts.reserved[3] != 1 && umma_supported(c->n, a.Lb))
         CDK_CUDA(launch_xpass_umma(t, c->d_ptilde, s));
       else if (tc) CDK_CUDA(launch_xpass_tc(t, c->d_ptilde, s));
       else CDK_CUDA(launch_xpass(t, s));
@@ -219,10 +220,27 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
               cudaStream_t s) {
   const int n = c->n, K = c->K;
   const size_t ncol = (size_t)n * (n / 2 + 1);
+  const bool tc = c->opts.form == CDK_FORM_BF16X3;
+  // streamed tensor-core x pass: n = 64, box <= 32 planes, direct planes (<= 96 atoms)
+  WaveArgs probe{};
+  probe.kyof = (c->opts.reserved[1] == 0) ? c->d_kyof : nullptr;
+  probe.max_atoms = maxAtoms;
+  probe.atom_cap = maxAtoms;
+  const bool streamed = tc && c->opts.reserved[3] == 0 && stream_supported(n, Lb) && direct_planes(probe);
+  if (streamed && !c->d_top) {
+    const size_t tb = stream_top_bytes(n, K);
+    if (cudaMalloc(&c->d_top, tb) != cudaSuccess) {
+      c->d_top = nullptr;
+      set_error("cudaMalloc of the tensor-core operator image failed (" + std::to_string(tb >> 20) + " MiB)");
+      return CDK_ERR_NOMEM;
+    }
+    CDK_CUDA(launch_top_build(n, K, c->d_ptilde, c->d_top, s));
+  }
+  const size_t lop_per = streamed ? stream_lop_bytes_per_rotation(n, K) : 0;
   int wave = c->opts.wave_rotations;
   if (wave <= 0) {
     // keep A + B of one wave near 6 GiB: big enough to fill the GPU, small next to HBM
-    const double per = (double)K * Lb * ncol * 8 + (double)n * ncol * 8;
+    const double per = (streamed ? (double)lop_per : (double)K * Lb * ncol * 8) + (double)n * ncol * 8;
     wave = (int)std::min<double>(4096.0, std::max(64.0, 6.0 * (1ull << 30) / per));
   }
   wave = (int)std::min<long>(wave, std::min<long>(nRot, 65535));
@@ -230,7 +248,8 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   const size_t b_rotxyz = align_up((size_t)wave * maxAtoms * sizeof(float4));
   const size_t b_rec = align_up((size_t)wave * sizeof(RotRec));
   const size_t b_keys = align_up((size_t)wave * sizeof(unsigned long long));
-  const size_t b_A = align_up((size_t)wave * K * Lb * ncol * sizeof(float2));
+  const size_t b_A = align_up(streamed ? (size_t)((wave + 7) & ~7) * lop_per
+                                       : (size_t)wave * K * Lb * ncol * sizeof(float2));
   const size_t b_B = align_up((size_t)wave * n * ncol * sizeof(float2));
   if (!grow(c->wave, b_rotxyz + b_rec + b_keys + b_A + b_B)) {
     set_error("cudaMalloc of the wave scratch failed (" +
@@ -251,7 +270,8 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   a.rot_xyz = reinterpret_cast<float4*>(base);
   a.rec = reinterpret_cast<RotRec*>(base + b_rotxyz);
   a.keys = reinterpret_cast<unsigned long long*>(base + b_rotxyz + b_rec);
-  a.A = reinterpret_cast<float2*>(base + b_rotxyz + b_rec + b_keys);
+  a.A = streamed ? nullptr : reinterpret_cast<float2*>(base + b_rotxyz + b_rec + b_keys);
+  a.lop = streamed ? reinterpret_cast<unsigned char*>(base + b_rotxyz + b_rec + b_keys) : nullptr;
   a.B = reinterpret_cast<float2*>(base + b_rotxyz + b_rec + b_keys + b_A);
   a.phat = c->d_phat;
   a.tw = c->d_tw;
@@ -266,8 +286,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     if (c->tuned_col_tile) a.col_tile = c->tuned_col_tile;
     a.chunk = c->tuned_chunk;
   }
-  const bool tc = c->opts.form == CDK_FORM_BF16X3;
-  if (tc && xpass_tc_smem_bytes(n, K, Lb) > 227 * 1024) {
+  if (tc && !streamed && xpass_tc_smem_bytes(n, K, Lb) > 227 * 1024) {
     set_error("ligand box too large for the tensor-core x pass at this grid size and K");
     return CDK_ERR_UNSUPPORTED;
   }
@@ -278,7 +297,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   }
   CDK_CUDA(cudaMemsetAsync(c->d_misc + 2, 0, 2 * sizeof(unsigned int), s));
   CDK_CUDA(cudaMemsetAsync(c->d_work, 0, 2 * sizeof(unsigned long long), s));
-  const bool umma = tc && c->opts.reserved[3] == 0 && umma_supported(n, Lb);
+  const bool umma = tc && !streamed && c->opts.reserved[3] != 1 && umma_supported(n, Lb);
   a.work = c->d_work;
   const bool prof = c->opts.reserved[0] != 0;
   const long nwaves = (nRot + wave - 1) / wave;
@@ -291,7 +310,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     }
   }
   c->kev_used = 0;
-  if (c->opts.reserved[2] && c->tuned_Lb != Lb) {
+  if (c->opts.reserved[2] && c->tuned_Lb != Lb && !streamed) {
     int rc = autotune_xpass(c, a, d_rots, nRot, wave, tc, s);
     if (rc) return rc;
     a.col_tile = c->tuned_col_tile ? c->tuned_col_tile : a.col_tile;
@@ -307,7 +326,8 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     if (prof) CDK_CUDA(cudaEventRecord(ev[1], s));
     CDK_CUDA(launch_spread_yz(a, s));
     if (prof) CDK_CUDA(cudaEventRecord(ev[2], s));
-    if (umma) CDK_CUDA(launch_xpass_umma(a, c->d_ptilde, s));
+    if (streamed) CDK_CUDA(launch_xpass_stream(a, c->d_top, s));
+    else if (umma) CDK_CUDA(launch_xpass_umma(a, c->d_ptilde, s));
     else if (tc) CDK_CUDA(launch_xpass_tc(a, c->d_ptilde, s));
     else CDK_CUDA(launch_xpass(a, s));
     if (prof) CDK_CUDA(cudaEventRecord(ev[3], s));
@@ -324,8 +344,9 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   c->stats[2] = (double)nRot;
   c->stats[4] = (double)Lb;
   c->stats[5] = (double)wave;
-  c->stats[13] = (double)a.col_tile;
-  c->stats[14] = (double)(a.chunk > 0 ? a.chunk : (tc ? 64 : 32));
+  c->stats[13] = streamed ? 4.0 : (double)a.col_tile;
+  c->stats[14] = streamed || umma ? 128.0 : (double)(a.chunk > 0 ? a.chunk : (tc ? 64 : 32));
+  c->stats[16] = streamed ? 3.0 : umma ? 2.0 : tc ? 1.0 : 0.0;
   c->stats[15] = (double)(c->gkey_seen);
   return CDK_OK;
 }
@@ -615,6 +636,7 @@ int cdk_ctx_destroy(cdk_ctx* c) {
   cudaFree(c->d_grids);
   cudaFree(c->d_phat);
   cudaFree(c->d_ptilde);
+  cudaFree(c->d_top);
   cudaFree(c->d_tw);
   cudaFree(c->d_kyof);
   cudaFree(c->d_misc);

@@ -76,6 +76,10 @@ struct WaveArgs {
   int* fault;                // set when a bounded device wait gave up
   const int* kyof;           // [n] natural frequency at each digit-reversed position; when set
                              // (and ligands have <= 96 atoms) planes are evaluated directly
+  unsigned char* lop;        // when set (n = 64, direct planes): the plane kernel writes the
+                             // ligand as split-BF16 x-chunk rows here instead of A:
+                             // [nrot/8][K][hi/lo][chunk j < 4][re/im][ncol/4][nrot%8][ncol%4]
+                             // x 16 B (8 planes; nrot rounded up to a multiple of 8)
 };
 
 // Launchers (stream-ordered, no synchronisation). Return cudaError_t of the launch.
@@ -115,6 +119,15 @@ size_t xpass_tc_smem_bytes(int n, int K, int Lb);
 // tcgen05 variant of the precision x pass (n = 64)
 bool umma_supported(int n, int Lb);
 cudaError_t launch_xpass_umma(const WaveArgs& a, const float2* pt, cudaStream_t s);
+// tcgen05 x pass with streamed operands (n = 64): the operator image is built once per receptor
+// from P~, the ligand rows come from the plane kernel (WaveArgs.lop)
+bool stream_supported(int n, int Lb);
+size_t stream_top_bytes(int n, int K);
+size_t stream_lop_bytes_per_rotation(int n, int K);
+cudaError_t launch_top_build(int n, int K, const float2* pt, void* top, cudaStream_t s);
+cudaError_t launch_xpass_stream(const WaveArgs& a, const void* top, cudaStream_t s);
+// true when launch_spread_yz takes the direct plane path (the only one that can write lop)
+bool direct_planes(const WaveArgs& a);
 
 // Digit-reversed position of natural frequency k for the radix plan of length n.
 int fft_position(int n, int k);

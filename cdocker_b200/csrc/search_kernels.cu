@@ -17,6 +17,7 @@
 // The energy grid never leaves shared memory. Spectra stay in the digit-reversed order the
 // in-place FFT stages produce; the receptor spectra are computed by the same stages, so
 // the pointwise product lines up without any permutation.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -26,6 +27,15 @@
 namespace cdk {
 
 namespace {
+
+// (a, b) -> packed bf16x2 hi = rn(a), rn(b) and lo = rn(a - hi), rn(b - hi); a in the low half
+__device__ __forceinline__ void split_bf16x2(float a, float b, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
+}
 
 // ---------------------------------------------------------------------------------------
 // exact-order float rotation (src/QuaternionMultiply.cpp:3-11, src/Rotate.cpp:4-27)
@@ -275,7 +285,7 @@ __global__ void __launch_bounds__(256) k_spread_yz(WaveArgs a) {
 // Atoms are visited per plane in ascending order: deterministic.
 constexpr int kDirectMaxAtoms = 96;
 
-template <int N>
+template <int N, bool LOP>
 __global__ void __launch_bounds__(256) k_spread_yz_direct(WaveArgs a, const int* __restrict__ kyof,
                                                            int cap) {
   constexpr int NZH = N / 2 + 1;
@@ -366,21 +376,67 @@ __global__ void __launch_bounds__(256) k_spread_yz_direct(WaveArgs a, const int*
     s_start[0] = 0;
   }
   __syncthreads();
-  for (int x = xlo; x <= xhi; ++x) {
-    const int e0 = s_start[x], e1 = s_start[x + 1];
-    float2* dst = a.A + (((size_t)r * a.K + k) * a.Lb + x) * NCOL;
-    for (int c = tid; c < NCOL; c += nthr) {
-      const int kyp = c / NZH, kz = c - kyp * NZH;
-      float accx = 0.f, accy = 0.f;
-      for (int e = e0; e < e1; ++e) {
-        const int j = s_list[e];
-        const float wv = s_w[e];
-        const float2 fy = Fy[(size_t)j * N + kyp];
-        const float2 fz = Fz[(size_t)j * NZH + kz];
-        accx += wv * (fy.x * fz.x - fy.y * fz.y);
-        accy += wv * (fy.x * fz.y + fy.y * fz.x);
+  if constexpr (!LOP) {
+    for (int x = xlo; x <= xhi; ++x) {
+      const int e0 = s_start[x], e1 = s_start[x + 1];
+      float2* dst = a.A + (((size_t)r * a.K + k) * a.Lb + x) * NCOL;
+      for (int c = tid; c < NCOL; c += nthr) {
+        const int kyp = c / NZH, kz = c - kyp * NZH;
+        float accx = 0.f, accy = 0.f;
+        for (int e = e0; e < e1; ++e) {
+          const int j = s_list[e];
+          const float wv = s_w[e];
+          const float2 fy = Fy[(size_t)j * N + kyp];
+          const float2 fz = Fz[(size_t)j * NZH + kz];
+          accx += wv * (fy.x * fz.x - fy.y * fz.y);
+          accy += wv * (fy.x * fz.y + fy.y * fz.x);
+        }
+        dst[c] = make_float2(accx, accy);
       }
-      dst[c] = make_float2(accx, accy);
+    }
+  } else {
+    // split-BF16 rows of 8 planes (chunk j covers planes 8j..8j+7, zero outside [xlo, xhi]):
+    // per (rotation, channel) 16 rows [hi, lo][chunk][re, im] of ncol x 16 B (8 planes each),
+    // the tensor-core x pass's K order; 512 B blocks of (8 rotations x 4 columns) x 16 B
+    for (int jc = xlo >> 3; jc <= (xhi >> 3); ++jc) {
+      for (int c = tid; c < NCOL; c += nthr) {
+        const int kyp = c / NZH, kz = c - kyp * NZH;
+        uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+        for (int d = 0; d < 8; d += 2) {
+          float re[2], im[2];
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const int x = 8 * jc + d + u;
+            float accx = 0.f, accy = 0.f;
+            if (x >= xlo && x <= xhi) {
+              const int e0 = s_start[x], e1 = s_start[x + 1];
+              for (int e = e0; e < e1; ++e) {
+                const int j = s_list[e];
+                const float wv = s_w[e];
+                const float2 fy = Fy[(size_t)j * N + kyp];
+                const float2 fz = Fz[(size_t)j * NZH + kz];
+                accx += wv * (fy.x * fz.x - fy.y * fz.y);
+                accy += wv * (fy.x * fz.y + fy.y * fz.x);
+              }
+            }
+            re[u] = accx;
+            im[u] = accy;
+          }
+          split_bf16x2(re[0], re[1], rh[d / 2], rl[d / 2]);
+          split_bf16x2(im[0], im[1], ih[d / 2], il[d / 2]);
+        }
+        // row (hl, chunk, part) = (hl * 4 + jc) * 2 + part; 16 B unit
+        // (((r/8 * K + k) * 16 + row) * ncol/4 + c/4) * 32 + (r%8) * 4 + c%4: a 512 B block holds
+        // a column quad of 8 rotations (lanes here write 64 B runs, the x pass reads blocks)
+        uint4* dst = reinterpret_cast<uint4*>(a.lop) +
+                     (((size_t)(r >> 3) * a.K + k) * 16 * (NCOL / 4) + (c >> 2)) * 32 + (r & 7) * 4 + (c & 3);
+        constexpr size_t RS = (size_t)(NCOL / 4) * 32;  // one row
+        dst[((0 * 4 + jc) * 2 + 0) * RS] = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+        dst[((0 * 4 + jc) * 2 + 1) * RS] = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+        dst[((1 * 4 + jc) * 2 + 0) * RS] = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+        dst[((1 * 4 + jc) * 2 + 1) * RS] = make_uint4(il[0], il[1], il[2], il[3]);
+      }
     }
   }
 }
@@ -777,11 +833,19 @@ cudaError_t launch_spread_yz_t(const WaveArgs& a, cudaStream_t s) {
   const int cap = a.atom_cap > 0 ? a.atom_cap : a.max_atoms;
   if (a.kyof && cap <= kDirectMaxAtoms) {
     const size_t sm = direct_smem<N>(cap);
-    cudaError_t e = cudaFuncSetAttribute(k_spread_yz_direct<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (a.lop) {
+      if (N != 64) return cudaErrorInvalidValue;
+      cudaError_t e = cudaFuncSetAttribute(k_spread_yz_direct<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      if (e != cudaSuccess) return e;
+      k_spread_yz_direct<N, true><<<dim3(a.K, a.nrot), 256, sm, s>>>(a, a.kyof, cap);
+      return cudaGetLastError();
+    }
+    cudaError_t e = cudaFuncSetAttribute(k_spread_yz_direct<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    k_spread_yz_direct<N><<<dim3(a.K, a.nrot), 256, sm, s>>>(a, a.kyof, cap);
+    k_spread_yz_direct<N, false><<<dim3(a.K, a.nrot), 256, sm, s>>>(a, a.kyof, cap);
     return cudaGetLastError();
   }
+  if (a.lop) return cudaErrorInvalidValue;  // the FFT plane path writes A only
   const size_t sm = plane_smem<N>();
   cudaError_t e = cudaFuncSetAttribute(k_spread_yz<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
@@ -906,6 +970,10 @@ cudaError_t launch_prep(const WaveArgs& a, cudaStream_t s) {
 }
 cudaError_t launch_spread_yz(const WaveArgs& a, cudaStream_t s) {
   CDK_DISPATCH_N(a.n, launch_spread_yz_t, a, s);
+}
+bool direct_planes(const WaveArgs& a) {
+  const int cap = a.atom_cap > 0 ? a.atom_cap : a.max_atoms;
+  return a.kyof != nullptr && cap <= kDirectMaxAtoms;
 }
 cudaError_t launch_xpass(const WaveArgs& a, cudaStream_t s) {
   CDK_DISPATCH_N(a.n, launch_xpass_t, a, s);

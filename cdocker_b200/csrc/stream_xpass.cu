@@ -1,0 +1,407 @@
+// stream_xpass.cu -- the precision form's x pass with streamed operands (n = 64).
+//
+// Same contraction as umma_xpass.cu -- per spectral column and channel, the circulant operator
+// T = [[Tr, Ti], [Ti, -Tr]] (T(x', x) = P~((x + x') mod n)) times the ligand's x planes, BF16
+// hi/lo split, three products, FP32 accumulation in tensor memory over all channels -- but no
+// operand is built inside the kernel:
+//  * the operator tiles are precomputed once per receptor (k_top_build) as the exact shared-
+//    memory image of the K-major, no-swizzle layout and arrive by bulk copies (cp.async.bulk
+//    with an mbarrier transaction count);
+//  * the ligand rows are written split and packed by the plane kernel (k_spread_yz_direct
+//    with a lop buffer: per rotation and channel 16 rows [hi, lo][chunk][re, im] of ncol x 16 B,
+//    in 512 B blocks of 8 rotations x 4 columns, so the plane kernel writes 64 B runs and the
+//    four stages of a column quad read each block whole) and arrive by 16-byte cp.async copies; rows of x chunks that a rotation does not occupy
+//    are zero-filled by the copy itself (source size 0, no read).
+// K order: step j (16 wide) = group 2j (re part of planes 8j..8j+7) and group 2j+1 (im part).
+// Steps outside the chunks any rotation of the CTA occupies are neither loaded nor multiplied.
+//
+// CTA = 4 columns (32 bytes of B per (rotation, x')) x 128 rotations, 256 threads, one per SM
+// (512 TMEM columns). Stages are (channel, column) pairs through a 3-deep ring of 64 KB
+// buffers, warp-specialized: warps 0-3 produce (thread = rotation; thread 0 also issues the
+// operator bulk copies), each stage's "full" mbarrier completing when every producer's copies
+// have landed (cp.async.mbarrier.arrive.noinc) and the operator bytes arrived; one thread of
+// warp 4 waits for it, issues the MMAs and commits them to the stage's "empty" mbarrier, which
+// the producers wait on before refilling the buffer. All 8 warps run the epilogue. Every wait
+// is bounded; a wait that gives up sets the fault flag, lets issued copies land, frees TMEM.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "cdk_internal.h"
+
+namespace cdk {
+namespace {
+
+constexpr int XS_N = 64;
+constexpr int XS_NZH = XS_N / 2 + 1;
+constexpr int XS_NCOL = XS_N * XS_NZH;
+constexpr int XS_COLS = 4;
+constexpr int XS_R = 128;
+constexpr int XS_M = 128;
+constexpr int XS_THREADS = 256;
+constexpr int XS_PRODUCERS = 128;  // warps 0-3: one producer thread per rotation of the tile
+constexpr int XS_STAGES = 3;
+constexpr int XS_JMAX = 4;                          // x chunks of 8 planes (Lb <= 32)
+constexpr uint32_t XS_GROUP = (XS_M / 8) * 128;     // 2048 B: one K group of 8 for 128 rows
+constexpr uint32_t XS_STEP = 2 * XS_GROUP;          // 4096 B: one K step of 16
+constexpr uint32_t XS_TILE = XS_JMAX * XS_STEP;     // 16 KB: 128 rows x 64 K, bf16
+constexpr uint32_t XS_STAGE = 4 * XS_TILE;          // T_hi, T_lo, L_hi, L_lo
+constexpr uint32_t XS_TMEM_COLS = XS_COLS * XS_R;   // 512
+constexpr size_t XS_SMEM = (size_t)XS_STAGES * XS_STAGE + 1024;
+constexpr uint32_t XS_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(XS_R >> 3) << 17) |
+                              ((uint32_t)(XS_M >> 4) << 24);
+constexpr long kWaitLimit = 1l << 22;
+static_assert(XS_NCOL % XS_COLS == 0, "column quads tile the half spectrum");
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (long i = 0; i < kWaitLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (i > 32) __nanosleep(40);
+  }
+  return false;
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      :
+      : "r"(d_tmem), "l"(a), "l"(b), "r"(XS_IDESC), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void bf16_split(float v, uint16_t& hi, uint16_t& lo) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(v);
+  const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+  hi = __bfloat16_as_ushort(h);
+  lo = __bfloat16_as_ushort(l);
+}
+
+// Operator image: top[((c * K + k) * 2 + hl) * XS_TILE + j * XS_STEP + part * XS_GROUP
+//                     + (m >> 3) * 128 + (m & 7) * 16 + d * 2] = hl part of
+//   rows m < 64 (x' = m):        part 0: Re P~(x + x'),  part 1: Im P~(x + x')
+//   rows m >= 64 (x' = m - 64):  part 0: Im P~(x + x'),  part 1: -Re P~(x + x')
+// with x = 8 j + d. One thread per 16-byte row.
+__global__ void __launch_bounds__(256) k_top_build(int K, const float2* __restrict__ pt,
+                                                   uint4* __restrict__ top) {
+  const int c = blockIdx.x, k = blockIdx.y;
+  __shared__ float2 s_p[XS_N];
+  if (threadIdx.x < XS_N) s_p[threadIdx.x] = pt[((size_t)c * K + k) * XS_N + threadIdx.x];
+  __syncthreads();
+  uint4* dst = top + ((size_t)c * K + k) * 2 * (XS_TILE / 16);
+  for (int row = threadIdx.x; row < 2 * (int)(XS_TILE / 16); row += blockDim.x) {
+    const int hl = row / (XS_TILE / 16);
+    const int rem = row - hl * (XS_TILE / 16);
+    const int j = rem / (XS_STEP / 16);
+    const int part = (rem / (XS_GROUP / 16)) & 1;
+    const int m = rem & (XS_M - 1);
+    const int xp = m & (XS_N - 1);
+    const bool imrow = m >= XS_N;
+    uint16_t e[8];
+#pragma unroll
+    for (int d = 0; d < 8; ++d) {
+      const float2 v = s_p[(8 * j + d + xp) & (XS_N - 1)];
+      const float val = imrow ? (part ? -v.x : v.y) : (part ? v.y : v.x);
+      uint16_t h, l;
+      bf16_split(val, h, l);
+      e[d] = hl ? l : h;
+    }
+    dst[row] = make_uint4((uint32_t)e[0] | ((uint32_t)e[1] << 16), (uint32_t)e[2] | ((uint32_t)e[3] << 16),
+                          (uint32_t)e[4] | ((uint32_t)e[5] << 16), (uint32_t)e[6] | ((uint32_t)e[7] << 16));
+  }
+}
+
+__global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, const unsigned char* __restrict__ top) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // keep the ring 1024-aligned whatever the dynamic base
+  unsigned char* ring = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  __shared__ __align__(8) uint64_t s_full[XS_STAGES];
+  __shared__ __align__(8) uint64_t s_empty[XS_STAGES];
+  __shared__ int s_fail;
+  __shared__ int s_issued, s_consumed;
+  __shared__ uint32_t s_tmem;
+  __shared__ unsigned char s_jr[KMAX][XS_R];  // per channel, rotation: jlo | jhi << 4 (empty: 0x0F)
+  __shared__ int s_jlo[KMAX], s_jhi[KMAX];
+  __shared__ int s_act[KMAX], s_nact;
+  __shared__ int s_W[XS_R];
+  const int K = a.K;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int r0 = blockIdx.x * XS_R;
+  const int c0 = blockIdx.y * XS_COLS;
+  const int nr = min(XS_R, a.nrot - r0);
+  if (tid == 0) {
+    for (int b = 0; b < XS_STAGES; ++b) {
+      // full: one cp.async arrival per producer thread + the operator copies' expect_tx arrival
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_full[b])), "r"(XS_PRODUCERS + 1));
+      // empty: the MMA thread's tcgen05.commit
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_empty[b])));
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(XS_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid < KMAX) {
+    s_jlo[tid] = XS_JMAX;
+    s_jhi[tid] = -1;
+  }
+  if (tid == 0) {
+    s_fail = 0;
+    s_issued = 0;
+    s_consumed = 0;
+  }
+  __syncthreads();
+  // per-rotation chunk ranges; block union per channel
+  if (tid < XS_R) {
+    const bool live = tid < nr && a.rec[r0 + tid].valid;
+    s_W[tid] = live ? a.rec[r0 + tid].W[0] : 0;
+    for (int k = 0; k < K; ++k) {
+      int lo = 1, hi = 0;
+      if (live) {
+        lo = a.rec[r0 + tid].xlo[k];
+        hi = a.rec[r0 + tid].xhi[k];
+      }
+      if (lo <= hi) {
+        // valid rotations keep every plane inside the planned box (<= 32 planes); the clamp
+        // only keeps shared-memory offsets in range whatever the record says
+        const int jl = min(lo >> 3, XS_JMAX - 1), jh = min(hi >> 3, XS_JMAX - 1);
+        s_jr[k][tid] = (unsigned char)(jl | (jh << 4));
+        atomicMin(&s_jlo[k], jl);
+        atomicMax(&s_jhi[k], jh);
+      } else {
+        s_jr[k][tid] = 0x0F;  // jlo 15 > jhi 0: no chunk
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (tid == 0) {
+    int n = 0;
+    for (int k = 0; k < K; ++k)
+      if (s_jlo[k] <= s_jhi[k]) s_act[n++] = k;
+    s_nact = n;
+  }
+  __syncthreads();
+  const uint32_t tmem = s_tmem;
+  const int NS = s_nact * XS_COLS;  // stages: (active channel, column), column fastest
+  const unsigned char* lop = a.lop;
+  const uint32_t ring_s = smem_u32(ring);
+
+  if (tid < XS_PRODUCERS) {
+    // ---- producers: thread = rotation rr of the tile; per stage its 4 * nj split rows
+    const int rr = tid;
+    const uint32_t row_s = (uint32_t)(rr >> 3) * 128 + (uint32_t)(rr & 7) * 16;
+    const int rg = r0 + (rr < nr ? rr : 0);
+    // 16 B units: (((r/8 * K + k) * 16 + row) * ncol/4 + c/4) * 32 + (r%8) * 4 + c%4
+    constexpr size_t RS = (size_t)(XS_NCOL / 4) * 32;
+    const size_t rot_rows = (size_t)(rg >> 3) * K * 16 * RS + (size_t)(c0 >> 2) * 32 + (rg & 7) * 4;
+    int s = 0;
+    for (; s < NS; ++s) {
+      const int b = s % XS_STAGES;
+      if (s >= XS_STAGES) {
+        // the MMAs of stage s - 3 must be done with this buffer
+        if (!mbar_wait(smem_u32(&s_empty[b]), (uint32_t)((s / XS_STAGES) - 1) & 1u)) {
+          atomicOr(&s_fail, 1);
+          break;
+        }
+      }
+      const int k = s_act[s / XS_COLS];
+      const int c = s % XS_COLS;
+      const int jlo = s_jlo[k], jhi = s_jhi[k];
+      const int nj = jhi - jlo + 1;
+      const uint32_t st = ring_s + (uint32_t)b * XS_STAGE;
+      const uint32_t full = smem_u32(&s_full[b]);
+      if (tid == 0) {
+        const uint32_t bytes = (uint32_t)nj * XS_STEP;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(2 * bytes), "r"(full)
+                     : "memory");
+#pragma unroll
+        for (int hl = 0; hl < 2; ++hl) {
+          const unsigned char* src = top + (((size_t)(c0 + c) * K + k) * 2 + hl) * XS_TILE + (size_t)jlo * XS_STEP;
+          const uint32_t dst = st + (uint32_t)hl * XS_TILE + (uint32_t)jlo * XS_STEP;
+          asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                       "l"(src), "r"(bytes), "r"(full)
+                       : "memory");
+        }
+        s_issued = s + 1;
+      }
+      const unsigned int jr = s_jr[k][rr];
+      const int jl = (int)(jr & 15), jh = (int)(jr >> 4);
+      const uint4* src0 = reinterpret_cast<const uint4*>(lop) + rot_rows + (size_t)k * 16 * RS + c;
+      for (int j = jlo; j <= jhi; ++j) {
+        const bool have = jl <= j && j <= jh;
+#pragma unroll
+        for (int hl = 0; hl < 2; ++hl)
+#pragma unroll
+          for (int part = 0; part < 2; ++part) {
+            const uint4* src = src0 + (size_t)((hl * 4 + j) * 2 + part) * RS;
+            const uint32_t dst = st + (uint32_t)(2 + hl) * XS_TILE + (uint32_t)j * XS_STEP +
+                                 (uint32_t)part * XS_GROUP + row_s;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(have ? 16 : 0)
+                         : "memory");
+          }
+      }
+      asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(full) : "memory");
+    }
+  } else if (tid == XS_PRODUCERS) {
+    // ---- MMA issuer
+    uint32_t acc_cols = 0;
+    int s = 0;
+    for (; s < NS; ++s) {
+      const int b = s % XS_STAGES;
+      if (!mbar_wait(smem_u32(&s_full[b]), (uint32_t)(s / XS_STAGES) & 1u)) {
+        atomicOr(&s_fail, 1);
+        break;
+      }
+      // the producers' cp.async writes (generic proxy) reach the tensor core (async proxy)
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int k = s_act[s / XS_COLS];
+      const int c = s % XS_COLS;
+      const uint32_t st = ring_s + (uint32_t)b * XS_STAGE;
+      const uint32_t d = tmem + (uint32_t)(c * XS_R);
+      for (int j = s_jlo[k]; j <= s_jhi[k]; ++j) {
+        const uint32_t off = (uint32_t)j * XS_STEP;
+        const uint64_t ah = make_desc(st + 0 * XS_TILE + off, XS_GROUP, 128);
+        const uint64_t al = make_desc(st + 1 * XS_TILE + off, XS_GROUP, 128);
+        const uint64_t bh = make_desc(st + 2 * XS_TILE + off, XS_GROUP, 128);
+        const uint64_t bl = make_desc(st + 3 * XS_TILE + off, XS_GROUP, 128);
+        umma_f16(d, ah, bh, (acc_cols >> c) & 1u);
+        acc_cols |= 1u << c;
+        umma_f16(d, ah, bl, 1u);
+        umma_f16(d, al, bh, 1u);
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&s_empty[b]))
+                   : "memory");
+    }
+    s_consumed = s;
+    // the newest commit completes after every earlier MMA of this thread
+    if (s > 0 && !mbar_wait(smem_u32(&s_empty[(s - 1) % XS_STAGES]), (uint32_t)((s - 1) / XS_STAGES) & 1u))
+      atomicOr(&s_fail, 1);
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncthreads();
+  bool ok = s_fail == 0;
+  if (!ok && tid == 0) {
+    // operator copies issued for stages the MMA thread never consumed: let them land
+    for (int t = s_consumed; t < s_issued; ++t)
+      mbar_wait(smem_u32(&s_full[t % XS_STAGES]), (uint32_t)(t / XS_STAGES) & 1u);
+  }
+  __syncthreads();
+  if (!ok) {
+    if (tid == 0) atomicOr(a.fault, 1);
+  } else if (NS > 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // ---- epilogue: per 32-rotation chunk, TMEM -> planes S[part][t][c][x'] -> B (32 B rows)
+    float* S = reinterpret_cast<float*>(ring);
+    const int q = warp & 3, h = warp >> 2;
+    const int row = 32 * q + lane;
+    const int xp = row & (XS_N - 1);
+    const int part = row >> 6;
+    for (int jr = 0; jr < XS_R / 32; ++jr) {
+#pragma unroll
+      for (int cc = 0; cc < 2; ++cc) {
+        const int c = 2 * h + cc;
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(c * XS_R + 32 * jr), v);
+#pragma unroll
+        for (int t = 0; t < 32; ++t) S[((part * 32 + t) * XS_COLS + c) * XS_N + xp] = v[t];
+      }
+      __syncthreads();
+      for (int i = tid; i < 32 * XS_N; i += XS_THREADS) {
+        const int x = i & (XS_N - 1), t = i >> 6;
+        const int rr = 32 * jr + t;
+        if (rr < nr && x < s_W[rr]) {
+          float re[XS_COLS], im[XS_COLS];
+#pragma unroll
+          for (int c = 0; c < XS_COLS; ++c) {
+            re[c] = S[((0 * 32 + t) * XS_COLS + c) * XS_N + x];
+            im[c] = S[((1 * 32 + t) * XS_COLS + c) * XS_N + x];
+          }
+          float4* dst = reinterpret_cast<float4*>(a.B + ((size_t)(r0 + rr) * XS_N + x) * XS_NCOL + c0);
+          dst[0] = make_float4(re[0], im[0], re[1], im[1]);
+          dst[1] = make_float4(re[2], im[2], re[3], im[3]);
+        }
+      }
+      __syncthreads();
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(XS_TMEM_COLS));
+  }
+}
+
+}  // namespace
+
+bool stream_supported(int n, int Lb) { return n == 64 && Lb >= 1 && Lb <= 8 * XS_JMAX; }
+
+size_t stream_top_bytes(int n, int K) {
+  return n == 64 ? (size_t)XS_NCOL * K * 2 * XS_TILE : 0;
+}
+
+size_t stream_lop_bytes_per_rotation(int n, int K) {
+  return n == 64 ? (size_t)K * XS_NCOL * 256 : 0;
+}
+
+cudaError_t launch_top_build(int n, int K, const float2* pt, void* top, cudaStream_t s) {
+  if (n != 64) return cudaErrorInvalidValue;
+  k_top_build<<<dim3(XS_NCOL, K), 256, 0, s>>>(K, pt, reinterpret_cast<uint4*>(top));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_xpass_stream(const WaveArgs& a, const void* top, cudaStream_t s) {
+  if (!stream_supported(a.n, a.Lb) || !a.lop || !top) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(k_xpass_stream64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XS_SMEM);
+  if (e != cudaSuccess) return e;
+  dim3 grid((a.nrot + XS_R - 1) / XS_R, XS_NCOL / XS_COLS);
+  k_xpass_stream64<<<grid, XS_THREADS, XS_SMEM, s>>>(a, reinterpret_cast<const unsigned char*>(top));
+  return cudaGetLastError();
+}
+
+}  // namespace cdk

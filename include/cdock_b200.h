@@ -51,8 +51,10 @@ typedef struct cdk_opts {
   int reserved[8];     /* [0] = 1: time every kernel with events (cdk_ctx_stats [8..12]);
                           [1] = 1: spread planes through the radix FFT instead of the direct
                           separable evaluation; [2] = 1: autotune the x pass on the first wave
-                          of each new ligand box; [3] = 1: precision form on mma.sync instead
-                          of tcgen05 */
+                          of each new ligand box; [3] precision-form x pass: 0 = tcgen05 with
+                          streamed operands where it applies (n = 64, ligand box <= 32
+                          planes, ligands <= 96 atoms), else the next one; 1 = mma.sync;
+                          2 = tcgen05 with operands built inside the kernel */
 } cdk_opts;
 
 /* Library version string. */
@@ -236,8 +238,10 @@ int cdk_server_destroy(cdk_server* s);
  * spread kernel transformed, [7] window planes the x pass wrote, [8..12] device ms per kernel
  * kind (prep, spread_yz, xpass, yz_inv_argmin, finalize) when the context was created with
  * opts.reserved[0] = 1 (events around every launch), else 0; [13] x-pass column tile,
- * [14] x-pass rotations per CTA, [15] graph state (0 off, 1 shape seen, 2 replaying). */
-#define CDK_NSTATS 16
+ * [14] x-pass rotations per CTA, [15] graph state (0 off, 1 shape seen, 2 replaying),
+ * [16] x-pass kind (0 FP32 radix, 1 mma.sync, 2 tcgen05 with in-kernel operand builds,
+ * 3 tcgen05 with streamed operands). */
+#define CDK_NSTATS 17
 int cdk_ctx_stats(cdk_ctx* ctx, double* out, int n);
 
 #ifdef __cplusplus

@@ -54,12 +54,35 @@ def test_fp64_rescore_of_top_poses(c0):
         assert abs(e64[0, j] - ref) <= 1e-7 * max(1.0, abs(ref))
 
 
-def test_tcgen05_and_mma_sync_variants_agree(grids_cache):
-    """The tcgen05 (TMEM accumulator) and mma.sync kernels apply the same split-BF16 operator."""
+@pytest.mark.parametrize("wave", [0, 200])
+def test_tensor_core_variants_agree(grids_cache, wave):
+    """tcgen05 with streamed operands (default at 64^3), tcgen05 with in-kernel operand builds
+    and mma.sync apply the same split-BF16 operator; ragged waves (200 rotations: a partial
+    128-rotation tile) included."""
     w = synth.make_workload("c1_64", seed=8, n_conf=2, n_q=150, grids_cache=grids_cache)
-    with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3) as ru, \
-            Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3, tc_mma_sync=True) as rm:
-        eu, iu = ru.search(w.coor, w.charge, w.eps, w.slot, w.quats)
-        em, im = rm.search(w.coor, w.charge, w.eps, w.slot, w.quats)
-    assert rel_err(eu, em).max() <= 1e-5
-    assert np.mean(np.all(iu == im, axis=1)) >= 0.99
+    out = {}
+    for name, kw in [("streamed", {}), ("build", {"tc_build": True}),
+                     ("mma_sync", {"tc_mma_sync": True})]:
+        with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3, wave_rotations=wave, **kw) as r:
+            out[name] = r.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+            kind = r.stats()["xpass_kind"]
+        assert kind == {"streamed": "tcgen05_streamed", "build": "tcgen05_build",
+                        "mma_sync": "mma_sync"}[name]
+    es, is_ = out["streamed"]
+    for other in ("build", "mma_sync"):
+        eo, io = out[other]
+        assert rel_err(es, eo).max() <= 1e-5
+        assert np.mean(np.all(is_ == io, axis=1)) >= 0.99
+
+
+def test_streamed_falls_back_for_large_ligands(grids_cache):
+    """Ligands above 96 atoms take the FFT plane path, which writes no split rows: the context
+    picks the in-kernel-build tcgen05 x pass for them and stays correct."""
+    w = synth.make_workload("c1_64", seed=9, n_conf=1, n_q=20, grids_cache=grids_cache,
+                            n_atoms=110)
+    with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3) as rtc, \
+            Receptor(w.grids, w.spacing) as r32:
+        etc, itc = rtc.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+        assert rtc.stats()["xpass_kind"] != "tcgen05_streamed"
+        e32, i32 = r32.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+    assert rel_err(etc, e32).max() <= TOL_TC
