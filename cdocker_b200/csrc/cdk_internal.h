@@ -1,6 +1,7 @@
 // cdk_internal.h -- device data layout and launch interface shared by the .cu files.
 #pragma once
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #include <string>
@@ -46,6 +47,8 @@ struct RotRec {
   short xlo[KMAX];  // per channel: first and last x plane touched (xlo > xhi: empty)
   short xhi[KMAX];
 };
+// the x ranges are read as 16-byte vectors
+static_assert(offsetof(RotRec, xlo) % 16 == 0 && sizeof(RotRec) % 16 == 0, "RotRec x-range alignment");
 
 // Everything one wave of rotations needs on the device.
 struct WaveArgs {

@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(256) k_spread_yz(WaveArgs a) {
 // (the same numbers the spread + radix FFT produce, without the float rounding of the plane).
 // CTA per (rotation, channel): per-atom factor tables in shared memory, then every touched
 // plane's n*(n/2+1) outputs, written in the (ky position, kz) order of the FFT path.
-// Atoms are visited per plane in ascending order: deterministic.
+// Atoms are visited in ascending order for every plane: deterministic.
 constexpr int kDirectMaxAtoms = 96;
 
 template <int N, bool LOP>
@@ -294,10 +294,10 @@ __global__ void __launch_bounds__(256) k_spread_yz_direct(WaveArgs a, const int*
   float2* tw = reinterpret_cast<float2*>(smem_raw);          // [N]
   float2* Fy = tw + N;                                        // [cap][N] by ky position
   float2* Fz = Fy + (size_t)cap * N;                          // [cap][NZH]
-  int* s_list = reinterpret_cast<int*>(Fz + (size_t)cap * NZH);  // [2*cap]
-  float* s_w = reinterpret_cast<float*>(s_list + 2 * cap);       // [2*cap]
-  int* s_start = reinterpret_cast<int*>(s_w + 2 * cap);          // [N+2]
-  int* s_atom = s_start + N + 2;                                 // [cap]
+  int* s_ax = reinterpret_cast<int*>(Fz + (size_t)cap * NZH);  // [cap] x cell of atom j
+  float* s_w0 = reinterpret_cast<float*>(s_ax + cap);          // [cap] weight of plane x cell
+  float* s_w1 = s_w0 + cap;                                    // [cap] weight of plane x cell + 1
+  int* s_atom = reinterpret_cast<int*>(s_w1 + cap);            // [cap]
   __shared__ int s_cnt;
   const int k = blockIdx.x, r = blockIdx.y;
   const RotRec* rec = a.rec + r;
@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(256) k_spread_yz_direct(WaveArgs a, const int*
   }
   __syncthreads();
   const int na = s_cnt;
-  // factor tables; the per-plane lists (thread 0, ascending atom order)
+  // factor tables and per-atom x cell / weights
   for (int i = tid; i < na * (N + NZH); i += nthr) {
     const int j = i / (N + NZH), f = i - j * (N + NZH);
     const int at = s_atom[j];
@@ -345,90 +345,76 @@ __global__ void __launch_bounds__(256) k_spread_yz_direct(WaveArgs a, const int*
       const float2 w0 = tw[(zi * kz) % N], w1 = tw[((zi + 1) * kz) % N];
       Fz[(size_t)j * NZH + kz] = make_float2((1.f - rz) * w0.x + rz * w1.x, (1.f - rz) * w0.y + rz * w1.y);
     }
-  }
-  if (tid == 0) {
-    // counting sort of (plane, atom) entries by plane; atoms stay in ascending order
-    for (int x = 0; x <= N; ++x) s_start[x] = 0;
-    for (int j = 0; j < na; ++j) {
-      const int xi = cell_of(a.rot_xyz[(size_t)r * a.max_atoms + s_atom[j]].x, mn0, h);
-      s_start[xi + 1]++;
-      if (xi + 1 < N) s_start[xi + 2]++;
-    }
-    for (int x = 0; x < N; ++x) s_start[x + 1] += s_start[x];
-    for (int j = 0; j < na; ++j) {
-      const int at = s_atom[j];
-      const float4 p = a.rot_xyz[(size_t)r * a.max_atoms + at];
+    if (f == 0) {
       const int xi = cell_of(p.x, mn0, h);
       const double xr = ratio_of(p.x, mn0, h, xi);
       const double sc = elec ? (double)prm[at].charge : (double)prm[at].w_vdw;
-      // s_start[x] is advanced as entries land; rebuilt below
-      const int e0 = s_start[xi]++;
-      s_list[e0] = j;
-      s_w[e0] = (float)(sc * (1.0 - xr));
-      if (xi + 1 < N) {
-        const int e1 = s_start[xi + 1]++;
-        s_list[e1] = j;
-        s_w[e1] = (float)(sc * xr);
-      }
+      s_ax[j] = xi;
+      s_w0[j] = (float)(sc * (1.0 - xr));
+      s_w1[j] = (xi + 1 < N) ? (float)(sc * xr) : 0.f;
     }
-    // s_start[x] now holds the end of plane x; shift back to starts
-    for (int x = N; x > 0; --x) s_start[x] = s_start[x - 1];
-    s_start[0] = 0;
   }
   __syncthreads();
-  if constexpr (!LOP) {
-    for (int x = xlo; x <= xhi; ++x) {
-      const int e0 = s_start[x], e1 = s_start[x + 1];
-      float2* dst = a.A + (((size_t)r * a.K + k) * a.Lb + x) * NCOL;
-      for (int c = tid; c < NCOL; c += nthr) {
-        const int kyp = c / NZH, kz = c - kyp * NZH;
-        float accx = 0.f, accy = 0.f;
-        for (int e = e0; e < e1; ++e) {
-          const int j = s_list[e];
-          const float wv = s_w[e];
-          const float2 fy = Fy[(size_t)j * N + kyp];
-          const float2 fz = Fz[(size_t)j * NZH + kz];
-          accx += wv * (fy.x * fz.x - fy.y * fz.y);
-          accy += wv * (fy.x * fz.y + fy.y * fz.x);
+  // Chunks of 8 planes: every thread owns columns, accumulates the chunk's planes in registers
+  // and visits the channel's atoms in ascending order; an atom adds to planes xi and xi + 1,
+  // whose offsets in the chunk are the same for the whole CTA (a uniform switch).
+  for (int jc = xlo >> 3; jc <= (xhi >> 3); ++jc) {
+    const int x0 = 8 * jc;
+    for (int c = tid; c < NCOL; c += nthr) {
+      const int kyp = c / NZH, kz = c - kyp * NZH;
+      float ax[8], ay[8];
+#pragma unroll
+      for (int d = 0; d < 8; ++d) ax[d] = ay[d] = 0.f;
+      for (int j = 0; j < na; ++j) {
+        const int o = s_ax[j] - x0;
+        if (o < -1 || o > 7) continue;
+        const float2 fy = Fy[(size_t)j * N + kyp];
+        const float2 fz = Fz[(size_t)j * NZH + kz];
+        const float gx = fy.x * fz.x - fy.y * fz.y;
+        const float gy = fy.x * fz.y + fy.y * fz.x;
+        const float w0 = s_w0[j], w1 = s_w1[j];
+        switch (o) {
+#define CDK_PLANE_PAIR(D)                    \
+  case D:                                    \
+    ax[D] += w0 * gx;                        \
+    ay[D] += w0 * gy;                        \
+    ax[D + 1] += w1 * gx;                    \
+    ay[D + 1] += w1 * gy;                    \
+    break;
+          case -1:
+            ax[0] += w1 * gx;
+            ay[0] += w1 * gy;
+            break;
+          CDK_PLANE_PAIR(0)
+          CDK_PLANE_PAIR(1)
+          CDK_PLANE_PAIR(2)
+          CDK_PLANE_PAIR(3)
+          CDK_PLANE_PAIR(4)
+          CDK_PLANE_PAIR(5)
+          CDK_PLANE_PAIR(6)
+#undef CDK_PLANE_PAIR
+          default:  // o == 7: plane xi + 1 is the next chunk's
+            ax[7] += w0 * gx;
+            ay[7] += w0 * gy;
+            break;
         }
-        dst[c] = make_float2(accx, accy);
       }
-    }
-  } else {
-    // split-BF16 rows of 8 planes (chunk j covers planes 8j..8j+7, zero outside [xlo, xhi]):
-    // per (rotation, channel) 16 rows [hi, lo][chunk][re, im] of ncol x 16 B (8 planes each),
-    // the tensor-core x pass's K order; 512 B blocks of (8 rotations x 4 columns) x 16 B
-    for (int jc = xlo >> 3; jc <= (xhi >> 3); ++jc) {
-      for (int c = tid; c < NCOL; c += nthr) {
-        const int kyp = c / NZH, kz = c - kyp * NZH;
+      if constexpr (!LOP) {
+#pragma unroll
+        for (int d = 0; d < 8; ++d) {
+          const int x = x0 + d;
+          if (x >= xlo && x <= xhi) a.A[(((size_t)r * a.K + k) * a.Lb + x) * NCOL + c] = make_float2(ax[d], ay[d]);
+        }
+      } else {
+        // split-BF16 rows of the 8 planes (zero outside [xlo, xhi] by construction): per
+        // (rotation, channel) 16 rows [hi, lo][chunk][re, im] of ncol x 16 B, the tensor-core x
+        // pass's K order, in 512 B blocks of (8 rotations x 4 columns) x 16 B
         uint32_t rh[4], rl[4], ih[4], il[4];
 #pragma unroll
         for (int d = 0; d < 8; d += 2) {
-          float re[2], im[2];
-#pragma unroll
-          for (int u = 0; u < 2; ++u) {
-            const int x = 8 * jc + d + u;
-            float accx = 0.f, accy = 0.f;
-            if (x >= xlo && x <= xhi) {
-              const int e0 = s_start[x], e1 = s_start[x + 1];
-              for (int e = e0; e < e1; ++e) {
-                const int j = s_list[e];
-                const float wv = s_w[e];
-                const float2 fy = Fy[(size_t)j * N + kyp];
-                const float2 fz = Fz[(size_t)j * NZH + kz];
-                accx += wv * (fy.x * fz.x - fy.y * fz.y);
-                accy += wv * (fy.x * fz.y + fy.y * fz.x);
-              }
-            }
-            re[u] = accx;
-            im[u] = accy;
-          }
-          split_bf16x2(re[0], re[1], rh[d / 2], rl[d / 2]);
-          split_bf16x2(im[0], im[1], ih[d / 2], il[d / 2]);
+          split_bf16x2(ax[d], ax[d + 1], rh[d / 2], rl[d / 2]);
+          split_bf16x2(ay[d], ay[d + 1], ih[d / 2], il[d / 2]);
         }
-        // row (hl, chunk, part) = (hl * 4 + jc) * 2 + part; 16 B unit
-        // (((r/8 * K + k) * 16 + row) * ncol/4 + c/4) * 32 + (r%8) * 4 + c%4: a 512 B block holds
-        // a column quad of 8 rotations (lanes here write 64 B runs, the x pass reads blocks)
         uint4* dst = reinterpret_cast<uint4*>(a.lop) +
                      (((size_t)(r >> 3) * a.K + k) * 16 * (NCOL / 4) + (c >> 2)) * 32 + (r & 7) * 4 + (c & 3);
         constexpr size_t RS = (size_t)(NCOL / 4) * 32;  // one row
@@ -825,7 +811,7 @@ constexpr size_t plane_smem() {
 template <int N>
 size_t direct_smem(int cap) {
   return sizeof(float2) * (N + (size_t)cap * (N + N / 2 + 1)) + sizeof(int) * 2 * cap +
-         sizeof(float) * 2 * cap + sizeof(int) * (N + 2 + cap);
+         sizeof(float) * 2 * cap;
 }
 
 template <int N>

@@ -16,8 +16,8 @@
 // Steps outside the chunks any rotation of the CTA occupies are neither loaded nor multiplied.
 //
 // CTA = 4 columns (32 bytes of B per (rotation, x')) x 128 rotations, 256 threads, one per SM
-// (512 TMEM columns). Stages are (channel, column) pairs through a 3-deep ring of 64 KB
-// buffers, warp-specialized: warps 0-3 produce (thread = rotation; thread 0 also issues the
+// (512 TMEM columns). Stages are (channel, column) pairs through a ring of 192 KB cut into
+// stages of 4 tiles of ceil(Lb/8) K-steps (3 stages at Lb 32, 4 at 24, 6 at 16), warp-specialized: warps 0-3 produce (thread = rotation; thread 0 also issues the
 // operator bulk copies), each stage's "full" mbarrier completing when every producer's copies
 // have landed (cp.async.mbarrier.arrive.noinc) and the operator bytes arrived; one thread of
 // warp 4 waits for it, issues the MMAs and commits them to the stage's "empty" mbarrier, which
@@ -40,14 +40,14 @@ constexpr int XS_R = 128;
 constexpr int XS_M = 128;
 constexpr int XS_THREADS = 256;
 constexpr int XS_PRODUCERS = 128;  // warps 0-3: one producer thread per rotation of the tile
-constexpr int XS_STAGES = 3;
+constexpr int XS_MAXSTAGES = 8;
 constexpr int XS_JMAX = 4;                          // x chunks of 8 planes (Lb <= 32)
 constexpr uint32_t XS_GROUP = (XS_M / 8) * 128;     // 2048 B: one K group of 8 for 128 rows
 constexpr uint32_t XS_STEP = 2 * XS_GROUP;          // 4096 B: one K step of 16
-constexpr uint32_t XS_TILE = XS_JMAX * XS_STEP;     // 16 KB: 128 rows x 64 K, bf16
-constexpr uint32_t XS_STAGE = 4 * XS_TILE;          // T_hi, T_lo, L_hi, L_lo
+constexpr uint32_t XS_TILE = XS_JMAX * XS_STEP;     // 16 KB: 128 rows x 64 K, bf16 (operator image)
+constexpr uint32_t XS_RING = 192 * 1024;            // shared-memory ring (stages of 4 tiles)
 constexpr uint32_t XS_TMEM_COLS = XS_COLS * XS_R;   // 512
-constexpr size_t XS_SMEM = (size_t)XS_STAGES * XS_STAGE + 1024;
+constexpr size_t XS_SMEM = (size_t)XS_RING + 1024;
 constexpr uint32_t XS_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(XS_R >> 3) << 17) |
                               ((uint32_t)(XS_M >> 4) << 24);
 constexpr long kWaitLimit = 1l << 22;
@@ -150,13 +150,14 @@ __global__ void __launch_bounds__(256) k_top_build(int K, const float2* __restri
   }
 }
 
-__global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, const unsigned char* __restrict__ top) {
+__global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, const unsigned char* __restrict__ top,
+                                                                   int jc) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // keep the ring 1024-aligned whatever the dynamic base
   unsigned char* ring = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  __shared__ __align__(8) uint64_t s_full[XS_STAGES];
-  __shared__ __align__(8) uint64_t s_empty[XS_STAGES];
+  __shared__ __align__(8) uint64_t s_full[XS_MAXSTAGES];
+  __shared__ __align__(8) uint64_t s_empty[XS_MAXSTAGES];
   __shared__ int s_fail;
   __shared__ int s_issued, s_consumed;
   __shared__ uint32_t s_tmem;
@@ -165,12 +166,16 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
   __shared__ int s_act[KMAX], s_nact;
   __shared__ int s_W[XS_R];
   const int K = a.K;
+  // ring geometry: tiles of jc K-steps (the planned box's x chunks), as many stages as fit
+  const uint32_t tile = (uint32_t)jc * XS_STEP;
+  const uint32_t stage = 4 * tile;
+  const int nb = min(XS_MAXSTAGES, (int)(XS_RING / stage));
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r0 = blockIdx.x * XS_R;
   const int c0 = blockIdx.y * XS_COLS;
   const int nr = min(XS_R, a.nrot - r0);
   if (tid == 0) {
-    for (int b = 0; b < XS_STAGES; ++b) {
+    for (int b = 0; b < nb; ++b) {
       // full: one cp.async arrival per producer thread + the operator copies' expect_tx arrival
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_full[b])), "r"(XS_PRODUCERS + 1));
       // empty: the MMA thread's tcgen05.commit
@@ -193,25 +198,39 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
     s_consumed = 0;
   }
   __syncthreads();
-  // per-rotation chunk ranges; block union per channel
+  // per-rotation chunk ranges (one vector load of the record's x ranges), block union per
+  // channel by warp reductions
   if (tid < XS_R) {
-    const bool live = tid < nr && a.rec[r0 + tid].valid;
-    s_W[tid] = live ? a.rec[r0 + tid].W[0] : 0;
-    for (int k = 0; k < K; ++k) {
-      int lo = 1, hi = 0;
-      if (live) {
-        lo = a.rec[r0 + tid].xlo[k];
-        hi = a.rec[r0 + tid].xhi[k];
-      }
-      if (lo <= hi) {
-        // valid rotations keep every plane inside the planned box (<= 32 planes); the clamp
-        // only keeps shared-memory offsets in range whatever the record says
-        const int jl = min(lo >> 3, XS_JMAX - 1), jh = min(hi >> 3, XS_JMAX - 1);
-        s_jr[k][tid] = (unsigned char)(jl | (jh << 4));
-        atomicMin(&s_jlo[k], jl);
-        atomicMax(&s_jhi[k], jh);
-      } else {
-        s_jr[k][tid] = 0x0F;  // jlo 15 > jhi 0: no chunk
+    const RotRec* rec = a.rec + r0 + min(tid, nr - 1);
+    const bool live = tid < nr && rec->valid;
+    s_W[tid] = live ? rec->W[0] : 0;
+    static_assert(KMAX == 16, "x ranges are two 32-byte vectors");
+    uint4 v[4];
+    const uint4* xr = reinterpret_cast<const uint4*>(rec->xlo);  // xlo[16] then xhi[16]
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = xr[i];
+    const short* lo16 = reinterpret_cast<const short*>(&v[0]);
+    const short* hi16 = reinterpret_cast<const short*>(&v[2]);
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) {
+      if (k < K) {
+        const int lo = live ? lo16[k] : 1, hi = live ? hi16[k] : 0;
+        int jl = 15, jh = -1;
+        if (lo <= hi) {
+          // valid rotations keep every plane inside the planned box; the clamp only keeps
+          // shared-memory offsets in range whatever the record says
+          jl = min(lo >> 3, jc - 1);
+          jh = min(hi >> 3, jc - 1);
+          s_jr[k][tid] = (unsigned char)(jl | (jh << 4));
+        } else {
+          s_jr[k][tid] = 0x0F;  // jlo 15 > jhi 0: no chunk
+        }
+        const int wl = __reduce_min_sync(0xffffffffu, jl);
+        const int wh = __reduce_max_sync(0xffffffffu, jh);
+        if (lane == 0) {
+          if (wl < 15) atomicMin(&s_jlo[k], wl);
+          if (wh >= 0) atomicMax(&s_jhi[k], wh);
+        }
       }
     }
   }
@@ -240,10 +259,10 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
     const size_t rot_rows = (size_t)(rg >> 3) * K * 16 * RS + (size_t)(c0 >> 2) * 32 + (rg & 7) * 4;
     int s = 0;
     for (; s < NS; ++s) {
-      const int b = s % XS_STAGES;
-      if (s >= XS_STAGES) {
-        // the MMAs of stage s - 3 must be done with this buffer
-        if (!mbar_wait(smem_u32(&s_empty[b]), (uint32_t)((s / XS_STAGES) - 1) & 1u)) {
+      const int b = s % nb;
+      if (s >= nb) {
+        // the MMAs of stage s - nb must be done with this buffer
+        if (!mbar_wait(smem_u32(&s_empty[b]), (uint32_t)((s / nb) - 1) & 1u)) {
           atomicOr(&s_fail, 1);
           break;
         }
@@ -252,7 +271,7 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
       const int c = s % XS_COLS;
       const int jlo = s_jlo[k], jhi = s_jhi[k];
       const int nj = jhi - jlo + 1;
-      const uint32_t st = ring_s + (uint32_t)b * XS_STAGE;
+      const uint32_t st = ring_s + (uint32_t)b * stage;
       const uint32_t full = smem_u32(&s_full[b]);
       if (tid == 0) {
         const uint32_t bytes = (uint32_t)nj * XS_STEP;
@@ -261,7 +280,7 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
 #pragma unroll
         for (int hl = 0; hl < 2; ++hl) {
           const unsigned char* src = top + (((size_t)(c0 + c) * K + k) * 2 + hl) * XS_TILE + (size_t)jlo * XS_STEP;
-          const uint32_t dst = st + (uint32_t)hl * XS_TILE + (uint32_t)jlo * XS_STEP;
+          const uint32_t dst = st + (uint32_t)hl * tile + (uint32_t)jlo * XS_STEP;
           asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                        "l"(src), "r"(bytes), "r"(full)
                        : "memory");
@@ -278,7 +297,7 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
 #pragma unroll
           for (int part = 0; part < 2; ++part) {
             const uint4* src = src0 + (size_t)((hl * 4 + j) * 2 + part) * RS;
-            const uint32_t dst = st + (uint32_t)(2 + hl) * XS_TILE + (uint32_t)j * XS_STEP +
+            const uint32_t dst = st + (uint32_t)(2 + hl) * tile + (uint32_t)j * XS_STEP +
                                  (uint32_t)part * XS_GROUP + row_s;
             asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(have ? 16 : 0)
                          : "memory");
@@ -291,8 +310,8 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
     uint32_t acc_cols = 0;
     int s = 0;
     for (; s < NS; ++s) {
-      const int b = s % XS_STAGES;
-      if (!mbar_wait(smem_u32(&s_full[b]), (uint32_t)(s / XS_STAGES) & 1u)) {
+      const int b = s % nb;
+      if (!mbar_wait(smem_u32(&s_full[b]), (uint32_t)(s / nb) & 1u)) {
         atomicOr(&s_fail, 1);
         break;
       }
@@ -301,14 +320,14 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int k = s_act[s / XS_COLS];
       const int c = s % XS_COLS;
-      const uint32_t st = ring_s + (uint32_t)b * XS_STAGE;
+      const uint32_t st = ring_s + (uint32_t)b * stage;
       const uint32_t d = tmem + (uint32_t)(c * XS_R);
       for (int j = s_jlo[k]; j <= s_jhi[k]; ++j) {
         const uint32_t off = (uint32_t)j * XS_STEP;
-        const uint64_t ah = make_desc(st + 0 * XS_TILE + off, XS_GROUP, 128);
-        const uint64_t al = make_desc(st + 1 * XS_TILE + off, XS_GROUP, 128);
-        const uint64_t bh = make_desc(st + 2 * XS_TILE + off, XS_GROUP, 128);
-        const uint64_t bl = make_desc(st + 3 * XS_TILE + off, XS_GROUP, 128);
+        const uint64_t ah = make_desc(st + 0 * tile + off, XS_GROUP, 128);
+        const uint64_t al = make_desc(st + 1 * tile + off, XS_GROUP, 128);
+        const uint64_t bh = make_desc(st + 2 * tile + off, XS_GROUP, 128);
+        const uint64_t bl = make_desc(st + 3 * tile + off, XS_GROUP, 128);
         umma_f16(d, ah, bh, (acc_cols >> c) & 1u);
         acc_cols |= 1u << c;
         umma_f16(d, ah, bl, 1u);
@@ -320,7 +339,7 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
     }
     s_consumed = s;
     // the newest commit completes after every earlier MMA of this thread
-    if (s > 0 && !mbar_wait(smem_u32(&s_empty[(s - 1) % XS_STAGES]), (uint32_t)((s - 1) / XS_STAGES) & 1u))
+    if (s > 0 && !mbar_wait(smem_u32(&s_empty[(s - 1) % nb]), (uint32_t)((s - 1) / nb) & 1u))
       atomicOr(&s_fail, 1);
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
@@ -329,7 +348,7 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
   if (!ok && tid == 0) {
     // operator copies issued for stages the MMA thread never consumed: let them land
     for (int t = s_consumed; t < s_issued; ++t)
-      mbar_wait(smem_u32(&s_full[t % XS_STAGES]), (uint32_t)(t / XS_STAGES) & 1u);
+      mbar_wait(smem_u32(&s_full[t % nb]), (uint32_t)(t / nb) & 1u);
   }
   __syncthreads();
   if (!ok) {
@@ -400,7 +419,8 @@ cudaError_t launch_xpass_stream(const WaveArgs& a, const void* top, cudaStream_t
   cudaError_t e = cudaFuncSetAttribute(k_xpass_stream64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XS_SMEM);
   if (e != cudaSuccess) return e;
   dim3 grid((a.nrot + XS_R - 1) / XS_R, XS_NCOL / XS_COLS);
-  k_xpass_stream64<<<grid, XS_THREADS, XS_SMEM, s>>>(a, reinterpret_cast<const unsigned char*>(top));
+  const int jc = (a.Lb + 7) / 8;  // K-steps a valid rotation can touch
+  k_xpass_stream64<<<grid, XS_THREADS, XS_SMEM, s>>>(a, reinterpret_cast<const unsigned char*>(top), jc);
   return cudaGetLastError();
 }
 
