@@ -15,9 +15,10 @@
 // K order: step j (16 wide) = group 2j (re part of planes 8j..8j+7) and group 2j+1 (im part).
 // Steps outside the chunks any rotation of the CTA occupies are neither loaded nor multiplied.
 //
-// CTA = 4 columns (32 bytes of B per (rotation, x')) x 128 rotations, 256 threads, one per SM
-// (512 TMEM columns). Stages are (channel, column) pairs through a ring of 192 KB cut into
-// stages of 4 tiles of ceil(Lb/8) K-steps (3 stages at Lb 32, 4 at 24, 6 at 16), warp-specialized: warps 0-3 produce (thread = rotation; thread 0 also issues the
+// CTA = COLS columns x 128 rotations, 256 threads: 2 columns, 96 KB ring, 256 TMEM columns and
+// two CTAs per SM when two stages fit the ring (ligand box <= 24 planes), else 4 columns (32
+// bytes of B per (rotation, x')), 192 KB ring, 512 TMEM columns, one CTA per SM. Stages are
+// (channel, column) pairs; a stage is 4 tiles of ceil(Lb/8) K-steps. Warp-specialized: warps 0-3 produce (thread = rotation; thread 0 also issues the
 // operator bulk copies), each stage's "full" mbarrier completing when every producer's copies
 // have landed (cp.async.mbarrier.arrive.noinc) and the operator bytes arrived; one thread of
 // warp 4 waits for it, issues the MMAs and commits them to the stage's "empty" mbarrier, which
@@ -35,7 +36,6 @@ namespace {
 constexpr int XS_N = 64;
 constexpr int XS_NZH = XS_N / 2 + 1;
 constexpr int XS_NCOL = XS_N * XS_NZH;
-constexpr int XS_COLS = 4;
 constexpr int XS_R = 128;
 constexpr int XS_M = 128;
 constexpr int XS_THREADS = 256;
@@ -45,13 +45,20 @@ constexpr int XS_JMAX = 4;                          // x chunks of 8 planes (Lb 
 constexpr uint32_t XS_GROUP = (XS_M / 8) * 128;     // 2048 B: one K group of 8 for 128 rows
 constexpr uint32_t XS_STEP = 2 * XS_GROUP;          // 4096 B: one K step of 16
 constexpr uint32_t XS_TILE = XS_JMAX * XS_STEP;     // 16 KB: 128 rows x 64 K, bf16 (operator image)
-constexpr uint32_t XS_RING = 192 * 1024;            // shared-memory ring (stages of 4 tiles)
-constexpr uint32_t XS_TMEM_COLS = XS_COLS * XS_R;   // 512
-constexpr size_t XS_SMEM = (size_t)XS_RING + 1024;
+// Two shapes: 2 columns per CTA with a 96 KB ring (two CTAs per SM, so one CTA's epilogue and
+// MMA-issue gaps overlap the other's work) when stages are at most 48 KB (ligand box <= 24
+// planes), else 4 columns with a 192 KB ring (one CTA per SM).
+template <int COLS>
+struct XsShape {
+  static constexpr uint32_t RING = COLS == 2 ? 96 * 1024 : 192 * 1024;
+  static constexpr uint32_t TMEM_COLS = COLS * XS_R;
+  static constexpr size_t SMEM = (size_t)RING + 1024;
+  static constexpr int MIN_BLOCKS = COLS == 2 ? 2 : 1;
+};
 constexpr uint32_t XS_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(XS_R >> 3) << 17) |
                               ((uint32_t)(XS_M >> 4) << 24);
 constexpr long kWaitLimit = 1l << 22;
-static_assert(XS_NCOL % XS_COLS == 0, "column quads tile the half spectrum");
+static_assert(XS_NCOL % 4 == 0, "column quads tile the half spectrum");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -150,8 +157,10 @@ __global__ void __launch_bounds__(256) k_top_build(int K, const float2* __restri
   }
 }
 
-__global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, const unsigned char* __restrict__ top,
-                                                                   int jc) {
+template <int COLS>
+__global__ void __launch_bounds__(XS_THREADS, XsShape<COLS>::MIN_BLOCKS)
+    k_xpass_stream64(WaveArgs a, const unsigned char* __restrict__ top, int jc) {
+  using Shape = XsShape<COLS>;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // keep the ring 1024-aligned whatever the dynamic base
   unsigned char* ring = reinterpret_cast<unsigned char*>(
@@ -169,10 +178,10 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
   // ring geometry: tiles of jc K-steps (the planned box's x chunks), as many stages as fit
   const uint32_t tile = (uint32_t)jc * XS_STEP;
   const uint32_t stage = 4 * tile;
-  const int nb = min(XS_MAXSTAGES, (int)(XS_RING / stage));
+  const int nb = min(XS_MAXSTAGES, (int)(Shape::RING / stage));
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r0 = blockIdx.x * XS_R;
-  const int c0 = blockIdx.y * XS_COLS;
+  const int c0 = blockIdx.y * COLS;
   const int nr = min(XS_R, a.nrot - r0);
   if (tid == 0) {
     for (int b = 0; b < nb; ++b) {
@@ -185,7 +194,7 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                 "r"(XS_TMEM_COLS));
+                 "r"(Shape::TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid < KMAX) {
@@ -245,9 +254,18 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
   }
   __syncthreads();
   const uint32_t tmem = s_tmem;
-  const int NS = s_nact * XS_COLS;  // stages: (active channel, column), column fastest
+  const int NS = s_nact * COLS;  // stages: (active channel, column), column fastest
   const unsigned char* lop = a.lop;
   const uint32_t ring_s = smem_u32(ring);
+  // stage parameters in registers (4 bits per active channel: id, first and last K-step), so
+  // the loops below read no shared memory but the mbarriers
+  uint64_t pk = 0, pl = 0, ph = 0;
+  for (int i = 0; i < s_nact; ++i) {
+    const int k = s_act[i];
+    pk |= (uint64_t)k << (4 * i);
+    pl |= (uint64_t)s_jlo[k] << (4 * i);
+    ph |= (uint64_t)s_jhi[k] << (4 * i);
+  }
 
   if (tid < XS_PRODUCERS) {
     // ---- producers: thread = rotation rr of the tile; per stage its 4 * nj split rows
@@ -256,20 +274,27 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
     const int rg = r0 + (rr < nr ? rr : 0);
     // 16 B units: (((r/8 * K + k) * 16 + row) * ncol/4 + c/4) * 32 + (r%8) * 4 + c%4
     constexpr size_t RS = (size_t)(XS_NCOL / 4) * 32;
-    const size_t rot_rows = (size_t)(rg >> 3) * K * 16 * RS + (size_t)(c0 >> 2) * 32 + (rg & 7) * 4;
-    int s = 0;
+    const size_t rot_rows = (size_t)(rg >> 3) * K * 16 * RS + (size_t)(c0 >> 2) * 32 + (rg & 7) * 4 + (c0 & 3);
+    // this rotation's chunk ranges, 8 bits per channel
+    uint64_t jr_lo = 0, jr_hi = 0;
+    for (int k = 0; k < K; ++k) {
+      const uint64_t v = s_jr[k][rr];
+      if (k < 8) jr_lo |= v << (8 * k);
+      else jr_hi |= v << (8 * (k - 8));
+    }
+    int s = 0, b = 0, ci = 0, ai = 0;
+    uint32_t round = 0;  // s / nb
     for (; s < NS; ++s) {
-      const int b = s % nb;
       if (s >= nb) {
         // the MMAs of stage s - nb must be done with this buffer
-        if (!mbar_wait(smem_u32(&s_empty[b]), (uint32_t)((s / nb) - 1) & 1u)) {
+        if (!mbar_wait(smem_u32(&s_empty[b]), (round - 1) & 1u)) {
           atomicOr(&s_fail, 1);
           break;
         }
       }
-      const int k = s_act[s / XS_COLS];
-      const int c = s % XS_COLS;
-      const int jlo = s_jlo[k], jhi = s_jhi[k];
+      const int k = (int)((pk >> (4 * ai)) & 15);
+      const int c = ci;
+      const int jlo = (int)((pl >> (4 * ai)) & 15), jhi = (int)((ph >> (4 * ai)) & 15);
       const int nj = jhi - jlo + 1;
       const uint32_t st = ring_s + (uint32_t)b * stage;
       const uint32_t full = smem_u32(&s_full[b]);
@@ -287,7 +312,7 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
         }
         s_issued = s + 1;
       }
-      const unsigned int jr = s_jr[k][rr];
+      const unsigned int jr = (unsigned int)(((k < 8 ? jr_lo : jr_hi) >> (8 * (k & 7))) & 255);
       const int jl = (int)(jr & 15), jh = (int)(jr >> 4);
       const uint4* src0 = reinterpret_cast<const uint4*>(lop) + rot_rows + (size_t)k * 16 * RS + c;
       for (int j = jlo; j <= jhi; ++j) {
@@ -304,25 +329,33 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
           }
       }
       asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(full) : "memory");
+      if (++b == nb) {
+        b = 0;
+        ++round;
+      }
+      if (++ci == COLS) {
+        ci = 0;
+        ++ai;
+      }
     }
   } else if (tid == XS_PRODUCERS) {
     // ---- MMA issuer
     uint32_t acc_cols = 0;
-    int s = 0;
+    int s = 0, b = 0, ci = 0, ai = 0;
+    uint32_t round = 0;
     for (; s < NS; ++s) {
-      const int b = s % nb;
-      if (!mbar_wait(smem_u32(&s_full[b]), (uint32_t)(s / nb) & 1u)) {
+      if (!mbar_wait(smem_u32(&s_full[b]), round & 1u)) {
         atomicOr(&s_fail, 1);
         break;
       }
       // the producers' cp.async writes (generic proxy) reach the tensor core (async proxy)
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int k = s_act[s / XS_COLS];
-      const int c = s % XS_COLS;
+      const int c = ci;
+      const int jlo = (int)((pl >> (4 * ai)) & 15), jhi = (int)((ph >> (4 * ai)) & 15);
       const uint32_t st = ring_s + (uint32_t)b * stage;
       const uint32_t d = tmem + (uint32_t)(c * XS_R);
-      for (int j = s_jlo[k]; j <= s_jhi[k]; ++j) {
+      for (int j = jlo; j <= jhi; ++j) {
         const uint32_t off = (uint32_t)j * XS_STEP;
         const uint64_t ah = make_desc(st + 0 * tile + off, XS_GROUP, 128);
         const uint64_t al = make_desc(st + 1 * tile + off, XS_GROUP, 128);
@@ -336,6 +369,14 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                        smem_u32(&s_empty[b]))
                    : "memory");
+      if (++b == nb) {
+        b = 0;
+        ++round;
+      }
+      if (++ci == COLS) {
+        ci = 0;
+        ++ai;
+      }
     }
     s_consumed = s;
     // the newest commit completes after every earlier MMA of this thread
@@ -363,27 +404,27 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
     const int part = row >> 6;
     for (int jr = 0; jr < XS_R / 32; ++jr) {
 #pragma unroll
-      for (int cc = 0; cc < 2; ++cc) {
-        const int c = 2 * h + cc;
+      for (int cc = 0; cc < COLS / 2; ++cc) {
+        const int c = (COLS / 2) * h + cc;
         float v[32];
         tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(c * XS_R + 32 * jr), v);
 #pragma unroll
-        for (int t = 0; t < 32; ++t) S[((part * 32 + t) * XS_COLS + c) * XS_N + xp] = v[t];
+        for (int t = 0; t < 32; ++t) S[((part * 32 + t) * COLS + c) * XS_N + xp] = v[t];
       }
       __syncthreads();
       for (int i = tid; i < 32 * XS_N; i += XS_THREADS) {
         const int x = i & (XS_N - 1), t = i >> 6;
         const int rr = 32 * jr + t;
         if (rr < nr && x < s_W[rr]) {
-          float re[XS_COLS], im[XS_COLS];
+          float re[COLS], im[COLS];
 #pragma unroll
-          for (int c = 0; c < XS_COLS; ++c) {
-            re[c] = S[((0 * 32 + t) * XS_COLS + c) * XS_N + x];
-            im[c] = S[((1 * 32 + t) * XS_COLS + c) * XS_N + x];
+          for (int c = 0; c < COLS; ++c) {
+            re[c] = S[((0 * 32 + t) * COLS + c) * XS_N + x];
+            im[c] = S[((1 * 32 + t) * COLS + c) * XS_N + x];
           }
           float4* dst = reinterpret_cast<float4*>(a.B + ((size_t)(r0 + rr) * XS_N + x) * XS_NCOL + c0);
-          dst[0] = make_float4(re[0], im[0], re[1], im[1]);
-          dst[1] = make_float4(re[2], im[2], re[3], im[3]);
+#pragma unroll
+          for (int c = 0; c < COLS; c += 2) dst[c / 2] = make_float4(re[c], im[c], re[c + 1], im[c + 1]);
         }
       }
       __syncthreads();
@@ -392,7 +433,7 @@ __global__ void __launch_bounds__(XS_THREADS, 1) k_xpass_stream64(WaveArgs a, co
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(XS_TMEM_COLS));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Shape::TMEM_COLS));
   }
 }
 
@@ -414,14 +455,27 @@ cudaError_t launch_top_build(int n, int K, const float2* pt, void* top, cudaStre
   return cudaGetLastError();
 }
 
+template <int COLS>
+cudaError_t launch_stream_cols(const WaveArgs& a, const void* top, int jc, cudaStream_t s) {
+  using Shape = XsShape<COLS>;
+  cudaError_t e = cudaFuncSetAttribute(k_xpass_stream64<COLS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)Shape::SMEM);
+  if (e != cudaSuccess) return e;
+  // all of the unified L1 as shared memory, so two 2-column CTAs fit one SM
+  e = cudaFuncSetAttribute(k_xpass_stream64<COLS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  dim3 grid((a.nrot + XS_R - 1) / XS_R, XS_NCOL / COLS);
+  k_xpass_stream64<COLS><<<grid, XS_THREADS, Shape::SMEM, s>>>(a, reinterpret_cast<const unsigned char*>(top), jc);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_xpass_stream(const WaveArgs& a, const void* top, cudaStream_t s) {
   if (!stream_supported(a.n, a.Lb) || !a.lop || !top) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(k_xpass_stream64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XS_SMEM);
-  if (e != cudaSuccess) return e;
-  dim3 grid((a.nrot + XS_R - 1) / XS_R, XS_NCOL / XS_COLS);
   const int jc = (a.Lb + 7) / 8;  // K-steps a valid rotation can touch
-  k_xpass_stream64<<<grid, XS_THREADS, XS_SMEM, s>>>(a, reinterpret_cast<const unsigned char*>(top), jc);
-  return cudaGetLastError();
+  // two stages of 4 tiles of jc steps must fit the 96 KB ring of the 2-column shape
+  if (2 * 4 * (uint32_t)jc * XS_STEP <= XsShape<2>::RING) return launch_stream_cols<2>(a, top, jc, s);
+  return launch_stream_cols<4>(a, top, jc, s);
 }
 
 }  // namespace cdk
