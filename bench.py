@@ -431,21 +431,26 @@ def run_ours(args, rank, world, local_rank):
 
 def serving_sample(w, rec_unused, secs: float) -> dict:
     """Continuous-batching server on the same 64^3 receptor (all 8 vdW grids + elec): Poisson
-    arrivals of requests with ligands of 10-80 atoms, 10-50 conformers, 500-2,000 rotations."""
-    from cdocker_b200 import Receptor, synth
+    arrivals of requests with ligands of 10-80 atoms, 10-50 conformers, 500-2,000 rotations,
+    served by each form (the precision form runs its waves on the streamed tensor-core x
+    pass; `tc_waves` counts them)."""
+    from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP32, Receptor, synth
     from cdocker_b200.serving import Server, make_requests, poisson_arrivals, run_load
     rate = 40.0
     arr = poisson_arrivals(rate, secs, seed=7)
     reqs = make_requests(len(arr), 21, w.spacing, w.length, synth.PROBE_RADII, atoms=(10, 80),
                          confs=(10, 50), rots=(500, 2000))
-    with Receptor(w.all_grids, w.spacing, max_atoms=128) as r:
-        with Server(r, arena_bytes=512 << 20, wave_rotations=1024, max_atoms=128) as srv:
-            res = run_load(srv, reqs, arr)
-            st = srv.stats()
-    res.update({"rate_hz": rate, "grid": 64, "waves": st["waves"],
-                "request_mix": "ligand U(10,80) atoms, conformers U(10,50), rotations "
-                               "U(500,2000), Poisson arrivals"})
-    return res
+    out = {}
+    for name, form in (("fp32", CDK_FORM_FP32), ("bf16x3_tensor_core", CDK_FORM_BF16X3)):
+        with Receptor(w.all_grids, w.spacing, max_atoms=96, form=form) as r:
+            with Server(r, arena_bytes=512 << 20, wave_rotations=1024, max_atoms=96) as srv:
+                res = run_load(srv, reqs, arr)
+                st = srv.stats()
+        res.update({"rate_hz": rate, "grid": 64, "waves": st["waves"], "tc_waves": st["tc_waves"],
+                    "request_mix": "ligand U(10,80) atoms, conformers U(10,50), rotations "
+                                   "U(500,2000), Poisson arrivals"})
+        out[name] = res
+    return out
 
 
 def serve_sweep(args):
@@ -466,8 +471,10 @@ def serve_sweep(args):
                             max_box=40) as srv:
                     res = run_load(srv, reqs, arr)
                     st = srv.stats()
+                # the streamed tensor-core x pass exists at 64^3 only: at 96^3 both forms
+                # serve on the FP32 x pass (tc_waves = 0)
                 res.update({"config": "serving, 96^3 K=9, 6,000-atom receptor", "form": form_name,
-                            "rate_hz": rate, "waves": st["waves"]})
+                            "rate_hz": rate, "waves": st["waves"], "tc_waves": st["tc_waves"]})
                 print(json.dumps(res), flush=True)
 
 

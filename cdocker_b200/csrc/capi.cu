@@ -234,7 +234,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
       set_error("cudaMalloc of the tensor-core operator image failed (" + std::to_string(tb >> 20) + " MiB)");
       return CDK_ERR_NOMEM;
     }
-    CDK_CUDA(launch_top_build(n, K, c->d_ptilde, c->d_top, s));
+    CDK_CUDA(launch_top_build(n, K, c->d_ptilde, c->d_top, s));  // stream-ordered before the waves
   }
   const size_t lop_per = streamed ? stream_lop_bytes_per_rotation(n, K) : 0;
   int wave = c->opts.wave_rotations;
@@ -511,7 +511,35 @@ bool ctx_view(const cdk_ctx* c, CtxView* v) {
   v->kyof = (c->opts.reserved[1] == 0) ? c->d_kyof : nullptr;
   v->h_misc = c->h_misc;
   v->stream = c->stream;
+  v->form = c->opts.form;
+  v->tc_variant = c->opts.reserved[3];
+  v->top = c->d_top;
   return true;
+}
+
+int ctx_ensure_top(cdk_ctx* c) {
+  if (c->d_top) return CDK_OK;
+  if (c->opts.form != CDK_FORM_BF16X3 || !c->d_ptilde) {
+    set_error("the operator image needs a precision-form context");
+    return CDK_ERR_INVALID;
+  }
+  const size_t tb = stream_top_bytes(c->n, c->K);
+  if (tb == 0) {
+    set_error("no streamed tensor-core x pass at this grid size");
+    return CDK_ERR_UNSUPPORTED;
+  }
+  if (cudaMalloc(&c->d_top, tb) != cudaSuccess) {
+    c->d_top = nullptr;
+    set_error("cudaMalloc of the tensor-core operator image failed (" + std::to_string(tb >> 20) + " MiB)");
+    return CDK_ERR_NOMEM;
+  }
+  cudaError_t e = launch_top_build(c->n, c->K, c->d_ptilde, c->d_top, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    set_error(std::string("operator image: ") + cudaGetErrorString(e));
+    return CDK_ERR_CUDA;
+  }
+  return CDK_OK;
 }
 }  // namespace cdk
 

@@ -150,6 +150,9 @@ struct CtxView {
   const int* kyof;
   unsigned int* h_misc;  // pinned host scratch of the context (4 words)
   cudaStream_t stream;
+  int form;              // CDK_FORM_*
+  int tc_variant;        // opts.reserved[3]
+  const void* top;       // operator image of the streamed tensor-core x pass (or null)
 };
 
 }  // namespace cdk
@@ -158,4 +161,7 @@ struct cdk_ctx;
 namespace cdk {
 // Fills *v from the context; returns false for a null context.
 bool ctx_view(const cdk_ctx* c, CtxView* v);
+// Builds the context's operator image for the streamed tensor-core x pass if it does not exist
+// yet (precision-form contexts at n = 64); synchronises the context stream. CDK_* status.
+int ctx_ensure_top(cdk_ctx* c);
 }  // namespace cdk

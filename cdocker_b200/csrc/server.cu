@@ -120,7 +120,8 @@ struct cdk_server {
   size_t arena_bytes = 0;
   ConfDesc* d_confs = nullptr;    // conformer table, one slot range per request
   int conf_cap = 0;
-  void* scratch = nullptr;        // wave scratch (rot_xyz, rec, keys, A, B)
+  void* scratch = nullptr;        // wave scratch (rot_xyz, rec, keys, A or split rows, B)
+  bool streamed = false;          // precision form: streamed tensor-core x pass where it applies
   unsigned int* d_misc = nullptr;  // [0] overflow count, [2..5] work counters
   WaveSlot slots[2];
   RangeAlloc* alloc = nullptr;
@@ -135,7 +136,7 @@ struct cdk_server {
   bool stop = false;
   std::thread worker;
   // statistics
-  long waves = 0, rotations = 0, launches = 0;
+  long waves = 0, rotations = 0, launches = 0, tc_waves = 0;
   double busy_ms = 0.0;
   std::vector<double> latencies;
   std::string error;
@@ -266,7 +267,9 @@ void worker_loop(cdk_server* s) {
   a.keys = reinterpret_cast<unsigned long long*>(sc);
   sc += up((size_t)W * sizeof(unsigned long long));
   a.A = reinterpret_cast<float2*>(sc);
-  sc += up((size_t)W * K * Lmax * ncol * sizeof(float2));
+  const size_t rows = s->streamed ? (size_t)((W + 7) & ~7) * stream_lop_bytes_per_rotation(n, K) : 0;
+  unsigned char* lop_base = reinterpret_cast<unsigned char*>(sc);
+  sc += up(std::max((size_t)W * K * Lmax * ncol * sizeof(float2), rows));
   a.B = reinterpret_cast<float2*>(sc);
   a.phat = s->v.phat;
   a.tw = s->v.tw;
@@ -334,9 +337,12 @@ void worker_loop(cdk_server* s) {
     a.Lb = lb;
     a.atom_cap = cap;
     a.rots = w.d_rots;
+    const bool tc_wave = s->streamed && stream_supported(n, lb) && direct_planes(a);
+    a.lop = tc_wave ? lop_base : nullptr;
     launch_prep(a, s->stream);
     launch_spread_yz(a, s->stream);
-    launch_xpass(a, s->stream);
+    if (tc_wave) launch_xpass_stream(a, s->v.top, s->stream);
+    else launch_xpass(a, s->stream);
     launch_yz_inv_argmin(a, s->stream);
     launch_finalize_server(a, reinterpret_cast<float*>(s->arena),
                            reinterpret_cast<int*>(s->arena), s->stream);
@@ -345,6 +351,7 @@ void worker_loop(cdk_server* s) {
     {
       std::lock_guard<std::mutex> lk(s->mu);
       s->waves++;
+      s->tc_waves += tc_wave ? 1 : 0;
       s->rotations += nr;
       s->launches += kLaunchesPerWave;
     }
@@ -388,10 +395,24 @@ int cdk_server_create(cdk_ctx* ctx, const cdk_server_opts* opts, cdk_server** ou
   const int n = s->v.n, K = s->v.K, W = s->opts.wave_rotations;
   const size_t ncol = (size_t)n * (n / 2 + 1);
   auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+  // precision-form contexts run the streamed tensor-core x pass on waves it applies to (ligand
+  // box <= 32 planes at n = 64, ligands <= 96 atoms on the direct plane path); other waves and
+  // FP32 contexts run the FP32 radix x pass
+  s->streamed = s->v.form == CDK_FORM_BF16X3 && s->v.tc_variant == 0 && s->v.kyof != nullptr &&
+                stream_supported(n, std::min(s->opts.max_box, 32));
+  if (s->streamed) {
+    const int rc = ctx_ensure_top(ctx);
+    if (rc != CDK_OK) {
+      delete s;
+      return rc;
+    }
+    ctx_view(ctx, &s->v);
+  }
+  const size_t planes = (size_t)W * K * s->opts.max_box * ncol * sizeof(float2);
+  const size_t rows = s->streamed ? (size_t)((W + 7) & ~7) * stream_lop_bytes_per_rotation(n, K) : 0;
   const size_t scratch = up((size_t)W * s->opts.max_atoms * sizeof(float4)) +
                          up((size_t)W * sizeof(RotRec)) + up((size_t)W * 8) +
-                         up((size_t)W * K * s->opts.max_box * ncol * sizeof(float2)) +
-                         up((size_t)W * n * ncol * sizeof(float2));
+                         up(std::max(planes, rows)) + up((size_t)W * n * ncol * sizeof(float2));
   auto fail = [&](const std::string& m, int code) {
     set_error(m);
     cdk_server_destroy(s);
@@ -519,10 +540,11 @@ int cdk_server_stats(cdk_server* s, double* out, int n) {
     size_t k = (size_t)std::ceil(p * lat.size()) - 1;
     return lat[std::min(k, lat.size() - 1)];
   };
-  const double vals[8] = {(double)s->waves, (double)s->rotations, (double)s->launches,
+  const double vals[9] = {(double)s->waves, (double)s->rotations, (double)s->launches,
                           (double)lat.size(), pct(0.50), pct(0.99),
-                          (double)s->waiting.size(), (double)s->active.size()};
-  for (int i = 0; i < n && i < 8; ++i) out[i] = vals[i];
+                          (double)s->waiting.size(), (double)s->active.size(),
+                          (double)s->tc_waves};
+  for (int i = 0; i < n && i < 9; ++i) out[i] = vals[i];
   return CDK_OK;
 }
 

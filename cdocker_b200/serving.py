@@ -76,11 +76,11 @@ class Server:
         return e, i, tm
 
     def stats(self) -> dict:
-        out = np.zeros(8, np.float64)
-        L.check(L.lib().cdk_server_stats(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), 8))
+        out = np.zeros(9, np.float64)
+        L.check(L.lib().cdk_server_stats(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), 9))
         return {"waves": int(out[0]), "rotations": int(out[1]), "launches": int(out[2]),
                 "completed": int(out[3]), "p50_ms": float(out[4]), "p99_ms": float(out[5]),
-                "waiting": int(out[6]), "in_flight": int(out[7])}
+                "waiting": int(out[6]), "in_flight": int(out[7]), "tc_waves": int(out[8])}
 
 
 def poisson_arrivals(rate_hz: float, duration_s: float, seed: int) -> np.ndarray:

@@ -228,7 +228,9 @@ int cdk_server_submit(cdk_server* s, int nAtom, int nConf, const float* coor,
 int cdk_server_poll(cdk_server* s, uint64_t ticket, int wait_ms, float* minE, int* idx,
                     double* timing);
 /* [0] waves, [1] rotations, [2] kernel launches, [3] completed requests, [4] p50 latency ms,
- * [5] p99 latency ms, [6] waiting requests, [7] admitted requests in flight. */
+ * [5] p99 latency ms, [6] waiting requests, [7] admitted requests in flight, [8] waves run on
+ * the streamed tensor-core x pass (precision-form contexts: waves whose ligand box is <= 32
+ * planes at n = 64 and whose ligands have <= 96 atoms; the others run the FP32 x pass). */
 int cdk_server_stats(cdk_server* s, double* out, int n);
 int cdk_server_destroy(cdk_server* s);
 

@@ -3,7 +3,7 @@ request searched alone, admission waits for arena space, and latency stats are r
 import numpy as np
 import pytest
 
-from cdocker_b200 import Receptor, synth
+from cdocker_b200 import CDK_FORM_BF16X3, Receptor, synth
 from cdocker_b200.serving import Server, make_requests, poisson_arrivals, run_load
 
 pytestmark = pytest.mark.gpu
@@ -63,6 +63,25 @@ def test_poisson_load_reports_latency(receptor_c1):
     with Server(rec, arena_bytes=256 << 20, wave_rotations=1024, max_atoms=128) as srv:
         res = run_load(srv, reqs[: len(arr)], arr)
     assert res["requests"] == len(arr) and res["p99_ms"] >= res["p50_ms"] > 0
+
+
+def test_precision_form_server_runs_tensor_core_waves(grids_cache):
+    """A precision-form receptor serves its waves on the streamed tensor-core x pass; each
+    rotation's column of the contraction is independent of the other rotations in its tile, so
+    shared waves reproduce each request searched alone."""
+    w = synth.make_workload("c1_64", seed=4, n_conf=1, n_q=1, grids_cache=grids_cache)
+    with Receptor(w.all_grids, w.spacing, max_atoms=96, form=CDK_FORM_BF16X3) as rec:
+        reqs = _reqs(w, 4, seed=21, atoms=(10, 60), confs=(2, 6), rots=(100, 400))
+        alone = [rec.search(r["coor"], r["charge"], r["eps"], _full_slot(r), r["quats"])
+                 for r in reqs]
+        with Server(rec, arena_bytes=64 << 20, wave_rotations=256, max_atoms=96) as srv:
+            tickets = [srv.submit(r["coor"], r["charge"], r["eps"], _full_slot(r), r["quats"])
+                       for r in reqs]
+            outs = [srv.poll(t, -1) for t in tickets]
+            st = srv.stats()
+    assert st["tc_waves"] == st["waves"] > 0
+    for (e, i, _), (ae, ai) in zip(outs, alone):
+        assert np.array_equal(e, ae) and np.array_equal(i, ai)
 
 
 def _full_slot(req):
