@@ -241,6 +241,53 @@ __device__ __forceinline__ void fft_stage(float2* buf, int nlines, int ls, int e
   }
 }
 
+// fft_stage with a compile-time line count bound SLOTS >= nlines: work item w is line w % SLOTS
+// of butterfly block w / SLOTS (no division by a run-time count), lines >= nlines idle.
+template <int N, int R, int M, bool INV, int SLOTS>
+__device__ __forceinline__ void fft_stage_slots(float2* buf, int nlines, int ls, int es,
+                                                const float2* __restrict__ tw, int tid, int nthr) {
+  constexpr int NB = N / R;
+  constexpr int TWM = N / (R * M);
+  for (int w = tid; w < SLOTS * NB; w += nthr) {
+    const int l = w % SLOTS;
+    if (l >= nlines) continue;
+    const int b = w / SLOTS;
+    const int blk = b / M;
+    const int np = b - blk * M;
+    float2* p = buf + l * ls + (blk * R * M + np) * es;
+    float2 v[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) v[j] = p[j * M * es];
+    if (!INV) {
+      Radix<R, -1>::run(v);
+      if (M > 1) {
+#pragma unroll
+        for (int k = 1; k < R; ++k) v[k] = c_mul(v[k], tw[np * k * TWM]);
+      }
+    } else {
+      if (M > 1) {
+#pragma unroll
+        for (int k = 1; k < R; ++k) v[k] = c_mulc(v[k], tw[np * k * TWM]);
+      }
+      Radix<R, +1>::run(v);
+    }
+#pragma unroll
+    for (int j = 0; j < R; ++j) p[j * M * es] = v[j];
+  }
+}
+
+// Inverse transform of at most SLOTS lines (two-stage plans), without run-time divisions.
+template <int N, int SLOTS>
+__device__ __forceinline__ void ifft_lines_slots(float2* buf, int nlines, int ls, int es,
+                                                 const float2* __restrict__ tw, int tid, int nthr) {
+  using P = FFTPlan<N>;
+  static_assert(P::NS == 2, "two-stage plans only");
+  fft_stage_slots<N, P::R1, StageM<N, 2>::value, true, SLOTS>(buf, nlines, ls, es, tw, tid, nthr);
+  __syncthreads();
+  fft_stage_slots<N, P::R0, StageM<N, 1>::value, true, SLOTS>(buf, nlines, ls, es, tw, tid, nthr);
+  __syncthreads();
+}
+
 // Full forward (DIF, natural -> digit-reversed) or inverse (DIT, digit-reversed -> natural)
 // transform of `nlines` lines. Contains the __syncthreads() between stages and one at the end.
 template <int N, bool INV>

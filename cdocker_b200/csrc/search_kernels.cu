@@ -682,16 +682,23 @@ __global__ void __launch_bounds__(256) k_yz_inv_argmin(WaveArgs a) {
     P[p * (N + 1) + fft_pos<N>(k)] = z;
   }
   __syncthreads();
-  fft_lines<N, true>(P, npairs, N + 1, 1, tw, tid, nthr);
+  if constexpr (FFTPlan<N>::NS == 2) {
+    ifft_lines_slots<N, N / 2>(P, npairs, N + 1, 1, tw, tid, nthr);
+  } else {
+    fft_lines<N, true>(P, npairs, N + 1, 1, tw, tid, nthr);
+  }
   const float inv = 1.0f / (float)((double)N * N * N);
   unsigned long long best = ~0ull;
-  for (int i = tid; i < Wy * Wz; i += nthr) {
-    const int y = i / Wz, z = i - y * Wz;
-    const float2 v = P[(y >> 1) * (N + 1) + z];
-    const float e = ((y & 1) ? v.y : v.x) * inv;
-    const unsigned int lin = (unsigned int)((x * N + y) * N + z);
-    const unsigned long long key = ((unsigned long long)order_key(e) << 32) | lin;
-    best = key < best ? key : best;
+  // window rows by warp, columns by lane (the key carries the index: order does not matter)
+  for (int y = tid >> 5; y < Wy; y += nthr >> 5) {
+    const float2* row = P + (y >> 1) * (N + 1);
+    for (int z = tid & 31; z < Wz; z += 32) {
+      const float2 v = row[z];
+      const float e = ((y & 1) ? v.y : v.x) * inv;
+      const unsigned int lin = (unsigned int)((x * N + y) * N + z);
+      const unsigned long long key = ((unsigned long long)order_key(e) << 32) | lin;
+      best = key < best ? key : best;
+    }
   }
   for (int o = 16; o > 0; o >>= 1) {
     unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
