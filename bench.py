@@ -54,6 +54,17 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def _tensor_peak():
+    """Dense BF16 TFLOP/s: the sustained measured figure (the x pass runs inside a long
+    step), else the fallback."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("bf16_tflops_sustained", d["bf16_tflops"])), "measured (sustained)"
+    return 1400.0, "fallback (sustained)"
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
 
@@ -208,18 +219,30 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+TENSOR_STEP_FLOP = 3 * 2 * 128 * 128 * 16  # one K-step of the streamed x pass: 3 BF16 MMAs
+
+
 def _kernel_roofline(stats: dict, n: int, K: int, hbm: float, peak_kind: str, traffic: dict):
-    """Roofline of the dominant kernel of the last search: algorithmic bytes per launch (from
-    the library's exact work counters) over its average launch time (events in the timed
-    region)."""
+    """Roofline of the dominant kernel of the last search, from the library's exact work
+    counters over its average launch time (events in the timed region).
+
+    HBM view: algorithmic bytes = the ligand planes it reads (x planes spread), the window
+    planes it writes, and per wave the receptor data it needs (FP32 x pass: the K receptor
+    spectra; streamed tensor-core x pass: the operator tiles of the ligand box's K-steps).
+    Tensor view (streamed tensor-core x pass): the BF16 MMA flops it issued (K-steps x 3
+    MMAs of 128 x 128 x 16) over the measured dense BF16 peak; the x pass is then bound by the
+    tensor cores and the shared memory that feeds them, so this is the headline bound."""
     ncol = n * (n // 2 + 1)
     waves = max(1, stats["waves"])
     km = stats["kernel_ms"]
     dom = max(km, key=km.get)
     plane = ncol * 8
     rot = stats["rotations"]
+    streamed = stats.get("xpass_kind") == "tcgen05_streamed"
+    jc = (stats["box"] + 7) // 8
+    receptor = K * ncol * 2 * jc * 4096 if streamed else K * n * plane
     alg = {
-        "xpass": (stats["planes_spread"] + stats["planes_window"]) * plane + waves * K * n * plane,
+        "xpass": (stats["planes_spread"] + stats["planes_window"]) * plane + waves * receptor,
         "spread_yz": stats["planes_spread"] * plane,
         "yz_inv_argmin": stats["planes_window"] * plane,
         "prep": rot * 1024,
@@ -229,12 +252,19 @@ def _kernel_roofline(stats: dict, n: int, K: int, hbm: float, peak_kind: str, tr
     t = km[dom] / waves / 1e3
     achieved = per_launch / t / 1e9
     tr = traffic.get(dom)
-    out = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-           "frac": achieved / hbm, "peak_kind": peak_kind,
-           "traffic": (tr * rot / waves) if tr is not None else None,
-           "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": t * 1e3,
-           "share_of_device_time": km[dom] / max(1e-9, sum(km.values())),
-           "kernel_ms": km}
+    hbm_view = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_kind": peak_kind,
+                "traffic": (tr * rot / waves) if tr is not None else None,
+                "algorithmic_bytes_per_launch": per_launch}
+    out = {"kernel": dom, **hbm_view, "avg_launch_ms": t * 1e3,
+           "share_of_device_time": km[dom] / max(1e-9, sum(km.values())), "kernel_ms": km}
+    if dom == "xpass" and streamed and stats.get("tensor_steps"):
+        tp, tkind = _tensor_peak()
+        flop = stats["tensor_steps"] * TENSOR_STEP_FLOP / waves
+        tach = flop / t / 1e12
+        out.update({"bound": "tensor", "achieved": tach, "peak": tp, "unit": "TFLOP/s",
+                    "frac": tach / tp, "peak_kind": tkind, "flop_per_launch": flop,
+                    "hbm_view": hbm_view})
     return out
 
 

@@ -215,8 +215,8 @@ class Receptor:
         return out
 
     def stats(self) -> dict:
-        out = np.zeros(17, np.float64)
-        L.check(L.lib().cdk_ctx_stats(self._h, out.ctypes.data_as(_dp), 17))
+        out = np.zeros(18, np.float64)
+        L.check(L.lib().cdk_ctx_stats(self._h, out.ctypes.data_as(_dp), 18))
         names = ["prep", "spread_yz", "xpass", "yz_inv_argmin", "finalize"]
         return {"launches": int(out[0]), "waves": int(out[1]), "rotations": int(out[2]),
                 "device_ms": float(out[3]), "box": int(out[4]), "wave_rotations": int(out[5]),
@@ -225,4 +225,5 @@ class Receptor:
                 "col_tile": int(out[13]), "rotations_per_cta": int(out[14]),
                 "graph_state": int(out[15]),
                 "xpass_kind": ["fp32_radix", "mma_sync", "tcgen05_build",
-                               "tcgen05_streamed"][int(out[16])]}
+                               "tcgen05_streamed"][int(out[16])],
+                "tensor_steps": int(out[17])}

@@ -114,7 +114,8 @@ struct cdk_ctx {
   Arena tables;               // per-search tables
   Arena io;                   // staging of host-buffer searches
   unsigned int* d_misc = nullptr;  // [0] diameter bits, [1] flags, [2] error count
-  unsigned long long* d_work = nullptr;  // [0] x planes spread (A), [1] window planes (B)
+  unsigned long long* d_work = nullptr;  // [0] x planes spread (A), [1] window planes (B),
+                                          // [2] tensor-core K-steps of the streamed x pass
   unsigned long long* h_work = nullptr;
   unsigned int* h_misc = nullptr;  // pinned mirror
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -296,7 +297,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     return CDK_ERR_INVALID;
   }
   CDK_CUDA(cudaMemsetAsync(c->d_misc + 2, 0, 2 * sizeof(unsigned int), s));
-  CDK_CUDA(cudaMemsetAsync(c->d_work, 0, 2 * sizeof(unsigned long long), s));
+  CDK_CUDA(cudaMemsetAsync(c->d_work, 0, 4 * sizeof(unsigned long long), s));
   const bool umma = tc && !streamed && c->opts.reserved[3] != 1 && umma_supported(n, Lb);
   a.work = c->d_work;
   const bool prof = c->opts.reserved[0] != 0;
@@ -476,9 +477,10 @@ int check_errors_after(cdk_ctx* c, cudaStream_t s) {
   }
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, c->ev0, c->ev1) == cudaSuccess) c->stats[3] = ms;
-  CDK_CUDA(cudaMemcpy(c->h_work, c->d_work, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  CDK_CUDA(cudaMemcpy(c->h_work, c->d_work, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   c->stats[6] = (double)c->h_work[0];
   c->stats[7] = (double)c->h_work[1];
+  c->stats[17] = (double)c->h_work[2];
   for (int k = 0; k < kLaunchesPerWave; ++k) c->stats[8 + k] = 0.0;
   for (int w = 0; w < c->kev_used; ++w) {
     cudaEvent_t* ev = &c->kev[(size_t)w * (kLaunchesPerWave + 1)];
@@ -623,8 +625,8 @@ int cdk_ctx_create(int nx, int ny, int nz, float spacing, int K, const float* gr
   CTX_CUDA(cudaMalloc(&c->d_tw, sizeof(float2) * n));
   CTX_CUDA(cudaMalloc(&c->d_misc, 4 * sizeof(unsigned int)));
   CTX_CUDA(cudaMallocHost(&c->h_misc, 4 * sizeof(unsigned int)));
-  CTX_CUDA(cudaMalloc(&c->d_work, 2 * sizeof(unsigned long long)));
-  CTX_CUDA(cudaMallocHost(&c->h_work, 2 * sizeof(unsigned long long)));
+  CTX_CUDA(cudaMalloc(&c->d_work, 4 * sizeof(unsigned long long)));
+  CTX_CUDA(cudaMallocHost(&c->h_work, 4 * sizeof(unsigned long long)));
   std::vector<float2> tw(n);
   for (int j = 0; j < n; ++j) {
     const double ang = -2.0 * M_PI * j / n;

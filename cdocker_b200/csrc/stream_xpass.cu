@@ -379,6 +379,14 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS>::MIN_BLOCKS)
       }
     }
     s_consumed = s;
+    {
+      unsigned long long steps = 0;  // K-steps issued by this CTA (work counter)
+      for (int t = 0; t < s; ++t) {
+        const int at = t / COLS;
+        steps += (unsigned long long)(((ph >> (4 * at)) & 15) - ((pl >> (4 * at)) & 15) + 1);
+      }
+      if (steps && a.work) atomicAdd(a.work + 2, steps);
+    }
     // the newest commit completes after every earlier MMA of this thread
     if (s > 0 && !mbar_wait(smem_u32(&s_empty[(s - 1) % nb]), (uint32_t)((s - 1) / nb) & 1u))
       atomicOr(&s_fail, 1);

@@ -242,8 +242,9 @@ int cdk_server_destroy(cdk_server* s);
  * opts.reserved[0] = 1 (events around every launch), else 0; [13] x-pass column tile,
  * [14] x-pass rotations per CTA, [15] graph state (0 off, 1 shape seen, 2 replaying),
  * [16] x-pass kind (0 FP32 radix, 1 mma.sync, 2 tcgen05 with in-kernel operand builds,
- * 3 tcgen05 with streamed operands). */
-#define CDK_NSTATS 17
+ * 3 tcgen05 with streamed operands), [17] tensor-core K-steps the streamed x pass issued (one
+ * step = three 128 x 128 x 16 BF16 MMAs, 1,572,864 flops). */
+#define CDK_NSTATS 18
 int cdk_ctx_stats(cdk_ctx* ctx, double* out, int n);
 
 #ifdef __cplusplus
