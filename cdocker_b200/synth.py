@@ -98,9 +98,10 @@ def make_conformers(base: np.ndarray, n_conf: int, seed: int) -> np.ndarray:
 
 def make_workload(name: str = "c0_32", seed: int = 0, n_conf: int | None = None,
                   n_q: int | None = None, grids_cache: dict | None = None,
-                  n_atoms: int | None = None) -> Workload:
+                  n_atoms: int | None = None, ligand_radius: float | None = None) -> Workload:
     n, n_rec, box, n_lig, lig_r, conf_default, q_default = CONFIGS[name]
     n_lig = n_lig if n_atoms is None else n_atoms
+    lig_r = lig_r if ligand_radius is None else ligand_radius
     n_conf = conf_default if n_conf is None else n_conf
     n_q = q_default if n_q is None else n_q
     spacing = 0.5

@@ -86,3 +86,23 @@ def test_streamed_falls_back_for_large_ligands(grids_cache):
         assert rtc.stats()["xpass_kind"] != "tcgen05_streamed"
         e32, i32 = r32.search(w.coor, w.charge, w.eps, w.slot, w.quats)
     assert rel_err(etc, e32).max() <= TOL_TC
+
+
+@pytest.mark.parametrize("n_atoms,radius,n_q,wave", [(6, 1.2, 40, 0),    # box 7 planes: one K-step, 6-stage ring
+                                                     (60, 6.8, 12, 0),   # box 30 planes: 4-column shape
+                                                     (40, 4.7, 37, 29)])  # ragged waves (not multiples of 8)
+def test_streamed_shapes_vs_fp64(grids_cache, n_atoms, radius, n_q, wave):
+    """The streamed tensor-core x pass across ligand boxes (1 to 4 K-steps, both CTA shapes)
+    and ragged waves, against the FP64 oracle."""
+    w = synth.make_workload("c1_64", seed=31, n_conf=1, n_q=n_q, grids_cache=grids_cache,
+                            n_atoms=n_atoms, ligand_radius=radius)
+    with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3, wave_rotations=wave) as rec:
+        minE, idx = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+        assert rec.stats()["xpass_kind"] == "tcgen05_streamed"
+    _, ridx, r64 = O.search_direct(w.grids, w.spacing, w.coor, w.charge, w.eps, w.slot, w.quats,
+                                   prec=1)
+    qq = w.quats.reshape(-1, 4)
+    st = check_search(minE, idx, r64, ridx,
+                      lambda r: O.energy_map(w.grids, w.spacing, w.coor[0], w.charge, w.eps,
+                                             w.slot, qq[r]), rel_tol=TOL_TC)
+    assert st["max_rel"] <= TOL_TC
