@@ -129,7 +129,8 @@ class Receptor:
     def __init__(self, grids, spacing: float, device: int = 0, wave_rotations: int = 0,
                  max_atoms: int = 256, col_tile: int = 0, form: int = L.CDK_FORM_FP32,
                  use_graphs: int = 0, profile: bool = False, fft_planes: bool = False,
-                 autotune: bool = False, tc_mma_sync: bool = False, tc_build: bool = False):
+                 autotune: bool = False, tc_mma_sync: bool = False, tc_build: bool = False,
+                 tc_tmem_ligand: bool = False):
         g = _f32(grids)
         if g.ndim != 4:
             raise ValueError("grids must be [K, n, n, n]")
@@ -147,7 +148,7 @@ class Receptor:
         opts.reserved[0] = 1 if profile else 0
         opts.reserved[1] = 1 if fft_planes else 0
         opts.reserved[2] = 1 if autotune else 0
-        opts.reserved[3] = 1 if tc_mma_sync else (2 if tc_build else 0)
+        opts.reserved[3] = 1 if tc_mma_sync else (2 if tc_build else (3 if tc_tmem_ligand else 0))
         h = C.c_void_p()
         L.check(lib.cdk_ctx_create(g.shape[1], g.shape[2], g.shape[3], self.spacing, self.K,
                                    _pf(g), C.byref(opts), C.byref(h)))
@@ -225,5 +226,5 @@ class Receptor:
                 "col_tile": int(out[13]), "rotations_per_cta": int(out[14]),
                 "graph_state": int(out[15]),
                 "xpass_kind": ["fp32_radix", "mma_sync", "tcgen05_build",
-                               "tcgen05_streamed"][int(out[16])],
+                               "tcgen05_streamed", "tcgen05_streamed_tmem"][int(out[16])],
                 "tensor_steps": int(out[17])}

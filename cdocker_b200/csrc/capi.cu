@@ -227,7 +227,9 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   probe.kyof = (c->opts.reserved[1] == 0) ? c->d_kyof : nullptr;
   probe.max_atoms = maxAtoms;
   probe.atom_cap = maxAtoms;
-  const bool streamed = tc && c->opts.reserved[3] == 0 && stream_supported(n, Lb) && direct_planes(probe);
+  const int variant = c->opts.reserved[3];
+  const bool streamed = tc && (variant == 0 || variant == 3) && stream_supported(n, Lb) && direct_planes(probe);
+  const bool tmem_ligand = variant == 3;
   if (streamed && !c->d_top) {
     const size_t tb = stream_top_bytes(n, K);
     if (cudaMalloc(&c->d_top, tb) != cudaSuccess) {
@@ -327,7 +329,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     if (prof) CDK_CUDA(cudaEventRecord(ev[1], s));
     CDK_CUDA(launch_spread_yz(a, s));
     if (prof) CDK_CUDA(cudaEventRecord(ev[2], s));
-    if (streamed) CDK_CUDA(launch_xpass_stream(a, c->d_top, s));
+    if (streamed) CDK_CUDA(launch_xpass_stream(a, c->d_top, tmem_ligand, s));
     else if (umma) CDK_CUDA(launch_xpass_umma(a, c->d_ptilde, s));
     else if (tc) CDK_CUDA(launch_xpass_tc(a, c->d_ptilde, s));
     else CDK_CUDA(launch_xpass(a, s));
@@ -347,7 +349,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   c->stats[5] = (double)wave;
   c->stats[13] = streamed ? 4.0 : (double)a.col_tile;
   c->stats[14] = streamed || umma ? 128.0 : (double)(a.chunk > 0 ? a.chunk : (tc ? 64 : 32));
-  c->stats[16] = streamed ? 3.0 : umma ? 2.0 : tc ? 1.0 : 0.0;
+  c->stats[16] = streamed ? (tmem_ligand ? 4.0 : 3.0) : umma ? 2.0 : tc ? 1.0 : 0.0;  // 3: default
   c->stats[15] = (double)(c->gkey_seen);
   return CDK_OK;
 }

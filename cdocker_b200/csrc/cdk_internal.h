@@ -128,7 +128,8 @@ bool stream_supported(int n, int Lb);
 size_t stream_top_bytes(int n, int K);
 size_t stream_lop_bytes_per_rotation(int n, int K);
 cudaError_t launch_top_build(int n, int K, const float2* pt, void* top, cudaStream_t s);
-cudaError_t launch_xpass_stream(const WaveArgs& a, const void* top, cudaStream_t s);
+// tmem_ligand: the ligand operand in tensor memory (k_xpass_tmema64), else in shared memory
+cudaError_t launch_xpass_stream(const WaveArgs& a, const void* top, bool tmem_ligand, cudaStream_t s);
 // true when launch_spread_yz takes the direct plane path (the only one that can write lop)
 bool direct_planes(const WaveArgs& a);
 

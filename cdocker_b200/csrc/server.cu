@@ -341,7 +341,7 @@ void worker_loop(cdk_server* s) {
     a.lop = tc_wave ? lop_base : nullptr;
     launch_prep(a, s->stream);
     launch_spread_yz(a, s->stream);
-    if (tc_wave) launch_xpass_stream(a, s->v.top, s->stream);
+    if (tc_wave) launch_xpass_stream(a, s->v.top, s->v.tc_variant == 3, s->stream);
     else launch_xpass(a, s->stream);
     launch_yz_inv_argmin(a, s->stream);
     launch_finalize_server(a, reinterpret_cast<float*>(s->arena),
@@ -398,7 +398,8 @@ int cdk_server_create(cdk_ctx* ctx, const cdk_server_opts* opts, cdk_server** ou
   // precision-form contexts run the streamed tensor-core x pass on waves it applies to (ligand
   // box <= 32 planes at n = 64, ligands <= 96 atoms on the direct plane path); other waves and
   // FP32 contexts run the FP32 radix x pass
-  s->streamed = s->v.form == CDK_FORM_BF16X3 && s->v.tc_variant == 0 && s->v.kyof != nullptr &&
+  s->streamed = s->v.form == CDK_FORM_BF16X3 && (s->v.tc_variant == 0 || s->v.tc_variant == 3) &&
+                s->v.kyof != nullptr &&
                 stream_supported(n, std::min(s->opts.max_box, 32));
   if (s->streamed) {
     const int rc = ctx_ensure_top(ctx);

@@ -52,9 +52,10 @@ typedef struct cdk_opts {
                           [1] = 1: spread planes through the radix FFT instead of the direct
                           separable evaluation; [2] = 1: autotune the x pass on the first wave
                           of each new ligand box; [3] precision-form x pass: 0 = tcgen05 with
-                          streamed operands where it applies (n = 64, ligand box <= 32
-                          planes, ligands <= 96 atoms), else the next one; 1 = mma.sync;
-                          2 = tcgen05 with operands built inside the kernel */
+                          streamed operands in shared memory where it applies (n = 64, ligand
+                          box <= 32 planes, ligands <= 96 atoms), else the next one;
+                          1 = mma.sync; 2 = tcgen05 with operands built inside the kernel;
+                          3 = tcgen05 with streamed operands, the ligand in tensor memory */
 } cdk_opts;
 
 /* Library version string. */
@@ -242,7 +243,8 @@ int cdk_server_destroy(cdk_server* s);
  * opts.reserved[0] = 1 (events around every launch), else 0; [13] x-pass column tile,
  * [14] x-pass rotations per CTA, [15] graph state (0 off, 1 shape seen, 2 replaying),
  * [16] x-pass kind (0 FP32 radix, 1 mma.sync, 2 tcgen05 with in-kernel operand builds,
- * 3 tcgen05 with streamed operands), [17] tensor-core K-steps the streamed x pass issued (one
+ * 3 tcgen05 with streamed operands in shared memory, 4 tcgen05 with streamed operands, the
+ * ligand in tensor memory), [17] tensor-core K-steps the streamed x pass issued (one
  * step = three 128 x 128 x 16 BF16 MMAs, 1,572,864 flops). */
 #define CDK_NSTATS 18
 int cdk_ctx_stats(cdk_ctx* ctx, double* out, int n);

@@ -56,19 +56,22 @@ def test_fp64_rescore_of_top_poses(c0):
 
 @pytest.mark.parametrize("wave", [0, 200])
 def test_tensor_core_variants_agree(grids_cache, wave):
-    """tcgen05 with streamed operands (default at 64^3), tcgen05 with in-kernel operand builds
-    and mma.sync apply the same split-BF16 operator; ragged waves (200 rotations: a partial
-    128-rotation tile) included."""
+    """tcgen05 with streamed operands (default at 64^3: both operands in shared memory; or the
+    ligand in tensor memory), tcgen05 with in-kernel operand builds and mma.sync apply the
+    same split-BF16 operator; ragged waves (200 rotations: a partial 128-rotation tile)
+    included."""
     w = synth.make_workload("c1_64", seed=8, n_conf=2, n_q=150, grids_cache=grids_cache)
     out = {}
-    for name, kw in [("streamed", {}), ("build", {"tc_build": True}),
-                     ("mma_sync", {"tc_mma_sync": True})]:
+    for name, kw in [("streamed", {}), ("streamed_tmem", {"tc_tmem_ligand": True}),
+                     ("build", {"tc_build": True}), ("mma_sync", {"tc_mma_sync": True})]:
         with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3, wave_rotations=wave, **kw) as r:
             out[name] = r.search(w.coor, w.charge, w.eps, w.slot, w.quats)
             kind = r.stats()["xpass_kind"]
-        assert kind == {"streamed": "tcgen05_streamed", "build": "tcgen05_build",
-                        "mma_sync": "mma_sync"}[name]
+        assert kind == {"streamed": "tcgen05_streamed", "streamed_tmem": "tcgen05_streamed_tmem",
+                        "build": "tcgen05_build", "mma_sync": "mma_sync"}[name]
     es, is_ = out["streamed"]
+    # the two streamed kernels run the same MMAs in the same order: bit-identical
+    assert np.array_equal(es, out["streamed_tmem"][0]) and np.array_equal(is_, out["streamed_tmem"][1])
     for other in ("build", "mma_sync"):
         eo, io = out[other]
         assert rel_err(es, eo).max() <= 1e-5
