@@ -97,8 +97,7 @@ cudaError_t launch_finalize_server(const WaveArgs& a, float* ebase, int* ibase, 
 // Dense forward transform of K receptor grids [K][n][n][n] -> phat [n][K][ncol].
 cudaError_t launch_receptor_fft(int n, int K, const float* grids, float2* scratch,
                                 float2* phat, const float2* tw, int col_tile, cudaStream_t s);
-// Shared memory per CTA of the x pass for given n, K, column tile.
-size_t xpass_smem_bytes(int n, int K, int col_tile);
+// Shared memory per CTA of the FP32 x pass for given n, K, column tile.
 size_t xpass2_smem_bytes(int n, int K, int col_tile);
 int pick_col_tile(int n, int K);
 // Dense FillLigandGrid on the GPU.

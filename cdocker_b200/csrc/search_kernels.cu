@@ -428,78 +428,6 @@ __global__ void __launch_bounds__(256) k_spread_yz_direct(WaveArgs a, const int*
 }
 
 // ---------------------------------------------------------------------------------------
-// x pass: forward along x, conj-multiply-sum with the receptor spectra, inverse along x.
-// CTA = one tile of `ct` spectral columns x a contiguous chunk of rotations.
-template <int N>
-__global__ void __launch_bounds__(256) k_xpass(WaveArgs a, int rot_per_cta) {
-  constexpr int NZH = N / 2 + 1;
-  constexpr int NCOL = N * NZH;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* tw = reinterpret_cast<float2*>(smem_raw);
-  int* s_ch = reinterpret_cast<int*>(tw + N);
-  float2* Wb = reinterpret_cast<float2*>(s_ch + 2 * KMAX);
-  const int ct = a.col_tile;
-  const int c0 = blockIdx.x * ct;
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  for (int i = tid; i < N; i += nthr) tw[i] = a.tw[i];
-  const int r_begin = blockIdx.y * rot_per_cta;
-  const int r_end = min(a.nrot, r_begin + rot_per_cta);
-  const int K = a.K;
-  for (int r = r_begin; r < r_end; ++r) {
-    const RotRec* rec = a.rec + r;
-    if (!rec->valid) continue;
-    __syncthreads();  // previous rotation done with s_ch / Wb
-    if (tid == 0) {
-      int nk = 0;
-      for (int k = 0; k < K; ++k)
-        if (rec->xlo[k] <= rec->xhi[k]) s_ch[nk++] = k;
-      s_ch[KMAX] = nk;
-    }
-    __syncthreads();
-    const int nk = s_ch[KMAX];
-    const int nl = nk * ct;  // lines
-    // load A (zero outside each channel's x range)
-    for (int i = tid; i < N * nl; i += nthr) {
-      const int c = i % ct;
-      const int t = i / ct;
-      const int kk = t % nk;
-      const int x = t / nk;
-      const int k = s_ch[kk];
-      float2 v = make_float2(0.f, 0.f);
-      if (x >= rec->xlo[k] && x <= rec->xhi[k] && c0 + c < NCOL)
-        v = a.A[(((size_t)r * K + k) * a.Lb + x) * NCOL + c0 + c];
-      Wb[i] = v;
-    }
-    __syncthreads();
-    fft_lines<N, false>(Wb, nl, 1, nl, tw, tid, nthr);
-    // S = sum_k conj(L_k) * P_k, into the kk = 0 lines
-    for (int i = tid; i < N * ct; i += nthr) {
-      const int c = i % ct;
-      const int xp = i / ct;
-      float2 s = make_float2(0.f, 0.f);
-      if (c0 + c < NCOL) {
-        for (int kk = 0; kk < nk; ++kk) {
-          const float2 l = Wb[xp * nl + kk * ct + c];
-          const float2 p = a.phat[((size_t)xp * K + s_ch[kk]) * NCOL + c0 + c];
-          const float2 t = c_conjmul(l, p);
-          s.x += t.x;
-          s.y += t.y;
-        }
-      }
-      Wb[xp * nl + c] = s;
-    }
-    __syncthreads();
-    fft_lines<N, true>(Wb, ct, 1, nl, tw, tid, nthr);
-    const int Wx = rec->W[0];
-    for (int i = tid; i < Wx * ct; i += nthr) {
-      const int c = i % ct;
-      const int x = i / ct;
-      if (c0 + c < NCOL) a.B[((size_t)r * N + x) * NCOL + c0 + c] = Wb[x * nl + c];
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------------------
 // x pass for two-stage plans (N = R0*R1), fused stage by stage; CT spectral columns per CTA:
 //   phase A  first forward stage straight from A in global memory (only the x planes a
 //            channel touches are read; the rest are known zeros), two channels per round;
@@ -860,41 +788,25 @@ cudaError_t launch_yz_inv_t(const WaveArgs& a, cudaStream_t s) {
 template <int N>
 cudaError_t launch_xpass_t(const WaveArgs& a, cudaStream_t s) {
   constexpr int NCOL = N * (N / 2 + 1);
-  const int tiles = (NCOL + a.col_tile - 1) / a.col_tile;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if constexpr (FFTPlan<N>::NS == 2) {
-    // fixed 16-column tiles; chunks of up to 32 rotations per CTA keep the receptor tile
-    // reused while giving the scheduler many CTAs per SM slot
-    constexpr int CT = 16;
-    if (a.col_tile != CT && a.col_tile != 8) return cudaErrorInvalidValue;
-    if (N > 64 && a.col_tile != 8) return cudaErrorInvalidValue;
-    const size_t sm = xpass2_smem_bytes(N, a.K, a.col_tile);
-    const int per = a.chunk > 0 ? a.chunk : 32;
-    const int chunks = (a.nrot + per - 1) / per;
-    if (N <= 64 && a.col_tile == CT) {
-      cudaError_t e = cudaFuncSetAttribute(k_xpass2<N, (N <= 64 ? 16 : 8)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      if (e != cudaSuccess) return e;
-      k_xpass2<N, (N <= 64 ? 16 : 8)><<<dim3(NCOL / (N <= 64 ? 16 : 8), chunks), 256, sm, s>>>(a, per);
-    } else {
-      cudaError_t e = cudaFuncSetAttribute(k_xpass2<N, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      if (e != cudaSuccess) return e;
-      k_xpass2<N, 8><<<dim3(NCOL / 8, chunks), 256, sm, s>>>(a, per);
-    }
-    return cudaGetLastError();
-  } else {
-    const size_t sm = xpass_smem_bytes(N, a.K, a.col_tile);
-    cudaError_t e = cudaFuncSetAttribute(k_xpass<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  static_assert(FFTPlan<N>::NS == 2, "the x pass runs two-stage radix plans");
+  // fixed 16-column tiles; chunks of up to 32 rotations per CTA keep the receptor tile
+  // reused while giving the scheduler many CTAs per SM slot
+  constexpr int CT = 16;
+  if (a.col_tile != CT && a.col_tile != 8) return cudaErrorInvalidValue;
+  if (N > 64 && a.col_tile != 8) return cudaErrorInvalidValue;
+  const size_t sm = xpass2_smem_bytes(N, a.K, a.col_tile);
+  const int per = a.chunk > 0 ? a.chunk : 32;
+  const int chunks = (a.nrot + per - 1) / per;
+  if (N <= 64 && a.col_tile == CT) {
+    cudaError_t e = cudaFuncSetAttribute(k_xpass2<N, (N <= 64 ? 16 : 8)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    int chunks = (sms * 8 + tiles - 1) / tiles;
-    if (chunks > a.nrot) chunks = a.nrot;
-    if (chunks < 1) chunks = 1;
-    const int per = (a.nrot + chunks - 1) / chunks;
-    chunks = (a.nrot + per - 1) / per;
-    k_xpass<N><<<dim3(tiles, chunks), 256, sm, s>>>(a, per);
-    return cudaGetLastError();
+    k_xpass2<N, (N <= 64 ? 16 : 8)><<<dim3(NCOL / (N <= 64 ? 16 : 8), chunks), 256, sm, s>>>(a, per);
+  } else {
+    cudaError_t e = cudaFuncSetAttribute(k_xpass2<N, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_xpass2<N, 8><<<dim3(NCOL / 8, chunks), 256, sm, s>>>(a, per);
   }
+  return cudaGetLastError();
 }
 
 template <int N>
@@ -930,22 +842,10 @@ size_t xpass2_smem_bytes(int n, int K, int col_tile) {
          sizeof(float2) * (size_t)n * col_tile * (K + 2 + 1);
 }
 
-size_t xpass_smem_bytes(int n, int K, int col_tile) {
-  return sizeof(float2) * n + sizeof(int) * 2 * KMAX + sizeof(float2) * (size_t)n * K * col_tile;
-}
-
 int pick_col_tile(int n, int K) {
-  // largest tile (<= 16 columns) whose buffers stay within ~110 KB of shared memory, so that
-  // two CTAs share an SM
-  int ct = 16;
-  if (n == 32 || n == 64) {
-    if (xpass2_smem_bytes(n, K, 16) > 110 * 1024) ct = 8;
-  } else if (n == 96 || n == 128) {
-    ct = 8;
-  } else {
-    while (ct > 2 && xpass_smem_bytes(n, K, ct) > 100 * 1024) ct >>= 1;
-  }
-  return ct;
+  // 16 columns when the buffers stay within ~110 KB of shared memory (two CTAs per SM), else 8
+  if ((n == 32 || n == 64) && xpass2_smem_bytes(n, K, 16) <= 110 * 1024) return 16;
+  return 8;
 }
 
 #define CDK_DISPATCH_N(n, fn, ...)                 \
