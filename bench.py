@@ -156,6 +156,46 @@ def cpu_baseline(w, budget_s: float = 15.0, threads: int = 0) -> dict:
                       f"{t_total:.1f} s"}
 
 
+def cpu_leg(w, args, outputs: dict, centers) -> tuple:
+    """The CPU leg of the bench line: the timed CPU baseline and, as the checker of the GPU
+    results, the oracle's FP64 energies of a sample of the timed rotations (per form) and the
+    oracle's conformer selection (same centres required)."""
+    from oracle import oracle as O
+    base = None if args.no_cpu_baseline else cpu_baseline(w, budget_s=args.cpu_budget)
+    acc = {}
+    if not args.no_check:
+        for name, (e, i) in outputs.items():
+            acc[name] = _accuracy_sample(w, e, i)
+    clus = None
+    if centers is not None:
+        x, en, cutoff, max_centers = centers["inputs"]
+        t0 = time.perf_counter()
+        want = O.cluster_conformers(x, en, cutoff, max_centers)
+        clus = {"cpu_oracle_ms": round(1e3 * (time.perf_counter() - t0), 1),
+                "identical_to_oracle": bool(np.array_equal(centers["got"], want)),
+                "cpu_threads": 1}
+    return base, acc, clus
+
+
+def clustering_sample(n_conf: int = 1000, n_atoms: int = 40, max_centers: int = 100) -> dict:
+    """Conformer selection (the greedy leader clustering of GeneDiverseConformations) on the
+    GPU for n_conf random-rotor conformers; the CPU leg checks the centres."""
+    import torch
+    from cdocker_b200 import conformers, synth
+    x, e = synth.conformer_ensemble(17, n_atoms=n_atoms, n_conf=n_conf, n_rotors=6)
+    conformers.cluster_conformers(x, e, 1.5, max_centers)  # first call: module load, launch
+    torch.cuda.synchronize()
+    reps = 5
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        got = conformers.cluster_conformers(x, e, 1.5, max_centers)
+    t_gpu = (time.perf_counter() - t0) / reps
+    return {"conformers": n_conf, "atoms": n_atoms, "centers": int(len(got)),
+            "gpu_ms": round(t_gpu * 1e3, 3),
+            "note": "host call: H2D of coordinates, pair-RMSD and greedy kernels, D2H of centres",
+            "_check": {"inputs": (x, e, 1.5, max_centers), "got": got}}
+
+
 def reference_cufft_sample(w, n_rot: int = 1000) -> dict:
     """The reference's own cuFFT path (oracle/_ref, batch 50, host fill, PCIe copies)."""
     from oracle import oracle as O
@@ -216,6 +256,12 @@ def run_reference(args, rank, world):
         "e2e": {"value": value, "unit": "rotations/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if args.ref_cufft:
+        # beside it, the reference's own GPU path (cuFFT, host fill and argmin, PCIe copies)
+        try:
+            line["reference_cufft"] = reference_cufft_sample(w)
+        except Exception as ex:  # no GPU or harness not built: say so, keep the CPU line
+            line["reference_cufft"] = {"unavailable": str(ex)[:200]}
     print(json.dumps(line), flush=True)
 
 
@@ -356,9 +402,16 @@ def run_ours(args, rank, world, local_rank):
         if args.forms != "both" and args.forms != name:
             continue
         rec, ms, stats, clocks, e, i = timed_form(form)
-        acc = _accuracy_sample(w, e, i) if (rank == 0 and not args.no_check) else None
-        forms[name] = {"rec": rec, "ms": ms, "stats": stats, "clocks": clocks, "acc": acc,
-                       "value": world * n_rot * args.steps / (ms / 1e3)}
+        forms[name] = {"rec": rec, "ms": ms, "stats": stats, "clocks": clocks, "acc": None,
+                       "e": e, "i": i, "value": world * n_rot * args.steps / (ms / 1e3)}
+    clustering = clustering_sample() if rank == 0 else None
+    cpu_base, clus_check = None, None
+    if rank == 0:
+        base, acc, clus_check = cpu_leg(w, args, {k: (v["e"], v["i"]) for k, v in forms.items()},
+                                        clustering.pop("_check") if clustering else None)
+        cpu_base = base
+        for k, v in acc.items():
+            forms[k]["acc"] = v
     # headline: the fastest form that meets its error bar on the checked sample
     bars = {"fp32": 1e-4, "bf16x3_tensor_core": 1e-3}
     ok = [k for k, v in forms.items()
@@ -450,10 +503,12 @@ def run_ours(args, rank, world, local_rank):
         }
         if serving is not None:
             line["serving"] = serving
-        if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(w, budget_s=args.cpu_budget)
-        if args.ref_cufft:
-            line["reference_cufft"] = reference_cufft_sample(w)
+        if clustering is not None:
+            if clus_check:
+                clustering.update(clus_check)
+            line["clustering"] = clustering
+        if cpu_base is not None:
+            line["cpu_baseline"] = cpu_base
         print(json.dumps(line), flush=True)
     for v in forms.values():
         v["rec"].close()
