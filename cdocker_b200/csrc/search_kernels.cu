@@ -291,14 +291,13 @@ __global__ void __launch_bounds__(256) k_spread_yz_direct(WaveArgs a, const int*
   constexpr int NZH = N / 2 + 1;
   constexpr int NCOL = N * NZH;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* tw = reinterpret_cast<float2*>(smem_raw);          // [N]
-  float2* Fy = tw + N;                                        // [cap][N] by ky position
-  float2* Fz = Fy + (size_t)cap * N;                          // [cap][NZH]
-  int* s_ax = reinterpret_cast<int*>(Fz + (size_t)cap * NZH);  // [cap] x cell of atom j
-  float* s_w0 = reinterpret_cast<float*>(s_ax + cap);          // [cap] weight of plane x cell
-  float* s_w1 = s_w0 + cap;                                    // [cap] weight of plane x cell + 1
-  int* s_atom = reinterpret_cast<int*>(s_w1 + cap);            // [cap]
+  float2* tw = reinterpret_cast<float2*>(smem_raw);            // [N]
+  int4* s_apk = reinterpret_cast<int4*>(tw + N);                // [cap] (x cell, w(xi), w(xi+1), -)
+  float2* Fy = reinterpret_cast<float2*>(s_apk + cap);          // [cap][N] by ky position
+  float2* Fz = Fy + (size_t)cap * N;                            // [cap][NZH]
+  int* s_atom = reinterpret_cast<int*>(Fz + (size_t)cap * NZH);  // [cap]
   __shared__ int s_cnt;
+  __shared__ uint32_t s_cm[N / 8][3];  // per 8-plane chunk: the channel atoms touching it (bit j)
   const int k = blockIdx.x, r = blockIdx.y;
   const RotRec* rec = a.rec + r;
   if (!rec->valid) return;
@@ -349,31 +348,48 @@ __global__ void __launch_bounds__(256) k_spread_yz_direct(WaveArgs a, const int*
       const int xi = cell_of(p.x, mn0, h);
       const double xr = ratio_of(p.x, mn0, h, xi);
       const double sc = elec ? (double)prm[at].charge : (double)prm[at].w_vdw;
-      s_ax[j] = xi;
-      s_w0[j] = (float)(sc * (1.0 - xr));
-      s_w1[j] = (xi + 1 < N) ? (float)(sc * xr) : 0.f;
+      s_apk[j] = make_int4(xi, __float_as_int((float)(sc * (1.0 - xr))),
+                           __float_as_int((xi + 1 < N) ? (float)(sc * xr) : 0.f), 0);
     }
   }
   __syncthreads();
-  // Chunks of 8 planes: every thread owns columns, accumulates the chunk's planes in registers
-  // and visits the channel's atoms in ascending order; an atom adds to planes xi and xi + 1,
-  // whose offsets in the chunk are the same for the whole CTA (a uniform switch).
-  for (int jc = xlo >> 3; jc <= (xhi >> 3); ++jc) {
-    const int x0 = 8 * jc;
-    for (int c = tid; c < NCOL; c += nthr) {
-      const int kyp = c / NZH, kz = c - kyp * NZH;
+  // per chunk, the atoms whose planes xi, xi + 1 meet it (warp 0, ballots in atom order)
+  const int jc0 = xlo >> 3, njc = (xhi >> 3) - jc0 + 1;  // planes < n: njc <= n / 8
+  if (tid < 32) {
+    for (int q = 0; q < njc; ++q) {
+      const int x0 = 8 * (jc0 + q);
+      for (int base = 0; base < 96; base += 32) {
+        const int j = base + tid;
+        const int o = j < na ? s_apk[j].x - x0 : -2;
+        const unsigned int m = __ballot_sync(0xffffffffu, o >= -1 && o <= 7);
+        if (tid == 0) s_cm[q][base >> 5] = m;
+      }
+    }
+  }
+  __syncthreads();
+  // Chunks of 8 planes: every thread owns columns, accumulates a chunk's planes in registers
+  // and visits the atoms touching the chunk in ascending order; an atom adds to planes xi and
+  // xi + 1, whose offsets in the chunk are the same for the whole CTA (a uniform switch).
+  for (int c = tid; c < NCOL; c += nthr) {
+    const int kyp = c / NZH, kz = c - kyp * NZH;
+    for (int q = 0; q < njc; ++q) {
+      const int jc = jc0 + q;
+      const int x0 = 8 * jc;
       float ax[8], ay[8];
 #pragma unroll
       for (int d = 0; d < 8; ++d) ax[d] = ay[d] = 0.f;
-      for (int j = 0; j < na; ++j) {
-        const int o = s_ax[j] - x0;
-        if (o < -1 || o > 7) continue;
-        const float2 fy = Fy[(size_t)j * N + kyp];
-        const float2 fz = Fz[(size_t)j * NZH + kz];
-        const float gx = fy.x * fz.x - fy.y * fz.y;
-        const float gy = fy.x * fz.y + fy.y * fz.x;
-        const float w0 = s_w0[j], w1 = s_w1[j];
-        switch (o) {
+      // only the atoms touching this chunk, in ascending order (the same for the whole CTA)
+      for (int wd = 0; wd < 3; ++wd) {
+        for (unsigned int mask = s_cm[q][wd]; mask; mask &= mask - 1) {
+          const int j = 32 * wd + __ffs(mask) - 1;
+          const int4 pk = s_apk[j];
+          const int o = pk.x - x0;
+          const float2 fy = Fy[(size_t)j * N + kyp];
+          const float2 fz = Fz[(size_t)j * NZH + kz];
+          const float gx = fy.x * fz.x - fy.y * fz.y;
+          const float gy = fy.x * fz.y + fy.y * fz.x;
+          const float w0 = __int_as_float(pk.y), w1 = __int_as_float(pk.z);
+          switch (o) {
 #define CDK_PLANE_PAIR(D)                    \
   case D:                                    \
     ax[D] += w0 * gx;                        \
@@ -381,22 +397,23 @@ __global__ void __launch_bounds__(256) k_spread_yz_direct(WaveArgs a, const int*
     ax[D + 1] += w1 * gx;                    \
     ay[D + 1] += w1 * gy;                    \
     break;
-          case -1:
-            ax[0] += w1 * gx;
-            ay[0] += w1 * gy;
-            break;
-          CDK_PLANE_PAIR(0)
-          CDK_PLANE_PAIR(1)
-          CDK_PLANE_PAIR(2)
-          CDK_PLANE_PAIR(3)
-          CDK_PLANE_PAIR(4)
-          CDK_PLANE_PAIR(5)
-          CDK_PLANE_PAIR(6)
+            case -1:
+              ax[0] += w1 * gx;
+              ay[0] += w1 * gy;
+              break;
+            CDK_PLANE_PAIR(0)
+            CDK_PLANE_PAIR(1)
+            CDK_PLANE_PAIR(2)
+            CDK_PLANE_PAIR(3)
+            CDK_PLANE_PAIR(4)
+            CDK_PLANE_PAIR(5)
+            CDK_PLANE_PAIR(6)
 #undef CDK_PLANE_PAIR
-          default:  // o == 7: plane xi + 1 is the next chunk's
-            ax[7] += w0 * gx;
-            ay[7] += w0 * gy;
-            break;
+            default:  // o == 7: plane xi + 1 is the next chunk's
+              ax[7] += w0 * gx;
+              ay[7] += w0 * gy;
+              break;
+          }
         }
       }
       if constexpr (!LOP) {
@@ -745,8 +762,8 @@ constexpr size_t plane_smem() {
 
 template <int N>
 size_t direct_smem(int cap) {
-  return sizeof(float2) * (N + (size_t)cap * (N + N / 2 + 1)) + sizeof(int) * 2 * cap +
-         sizeof(float) * 2 * cap;
+  return sizeof(float2) * (N + (size_t)cap * (N + N / 2 + 1)) + sizeof(int4) * cap +
+         sizeof(int) * cap;
 }
 
 template <int N>
