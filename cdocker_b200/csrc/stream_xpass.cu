@@ -137,9 +137,10 @@ __device__ __forceinline__ void bf16_split(float v, uint16_t& hi, uint16_t& lo) 
 
 // Operator image: top[((c * K + k) * 2 + hl) * XS_TILE + j * XS_STEP + part * XS_GROUP
 //                     + (m >> 3) * 128 + (m & 7) * 16 + d * 2] = hl part of
-//   rows m < 64 (x' = m):        part 0: Re P~(x + x'),  part 1: Im P~(x + x')
-//   rows m >= 64 (x' = m - 64):  part 0: Im P~(x + x'),  part 1: -Re P~(x + x')
-// with x = 8 j + d. One thread per 16-byte row.
+//   even rows m = 2x':      part 0: Re P~(x + x'),  part 1: Im P~(x + x')   (real output)
+//   odd rows m = 2x' + 1:   part 0: Im P~(x + x'),  part 1: -Re P~(x + x')  (imaginary output)
+// with x = 8 j + d; real and imaginary outputs of x' land in adjacent TMEM lanes. One thread
+// per 16-byte row.
 __global__ void __launch_bounds__(256) k_top_build(int K, const float2* __restrict__ pt,
                                                    uint4* __restrict__ top) {
   const int c = blockIdx.x, k = blockIdx.y;
@@ -153,8 +154,8 @@ __global__ void __launch_bounds__(256) k_top_build(int K, const float2* __restri
     const int j = rem / (XS_STEP / 16);
     const int part = (rem / (XS_GROUP / 16)) & 1;
     const int m = rem & (XS_M - 1);
-    const int xp = m & (XS_N - 1);
-    const bool imrow = m >= XS_N;
+    const int xp = m >> 1;            // rows interleaved: 2x' real output, 2x' + 1 imaginary
+    const bool imrow = (m & 1) != 0;
     uint16_t e[8];
 #pragma unroll
     for (int d = 0; d < 8; ++d) {
@@ -422,38 +423,30 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS>::MIN_BLOCKS)
     if (tid == 0) atomicOr(a.fault, 1);
   } else if (NS > 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // ---- epilogue: per 32-rotation chunk, TMEM -> planes S[part][t][c][x'] -> B (32 B rows)
-    float* S = reinterpret_cast<float*>(ring);
-    const int q = warp & 3, h = warp >> 2;
-    const int row = 32 * q + lane;
-    const int xp = row & (XS_N - 1);
-    const int part = row >> 6;
-    for (int jr = 0; jr < XS_R / 32; ++jr) {
+    // ---- epilogue, TMEM -> B without a shared-memory round trip: warp w reads lanes
+    // 32 (w % 4) .. + 31 (x' = 16 (w % 4) .. + 15, real and imaginary in adjacent lanes) for
+    // the rotation chunks of its half; an even lane takes its odd neighbour's imaginary part
+    // and writes (re, im) of all the CTA's columns for one (rotation, x'): 16 or 32 B
+    const int q = warp & 3;
+    const int xp = 16 * q + (lane >> 1);
+    const bool writer = (lane & 1) == 0;
+    for (int jr = 2 * (warp >> 2); jr < 2 * (warp >> 2) + 2; ++jr) {
+      float v[COLS][32];
 #pragma unroll
-      for (int cc = 0; cc < COLS / 2; ++cc) {
-        const int c = (COLS / 2) * h + cc;
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(c * XS_R + 32 * jr), v);
+      for (int c = 0; c < COLS; ++c)
+        tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(c * XS_R + 32 * jr), v[c]);
 #pragma unroll
-        for (int t = 0; t < 32; ++t) S[((part * 32 + t) * COLS + c) * XS_N + xp] = v[t];
-      }
-      __syncthreads();
-      for (int i = tid; i < 32 * XS_N; i += XS_THREADS) {
-        const int x = i & (XS_N - 1), t = i >> 6;
+      for (int t = 0; t < 32; ++t) {
+        float im[COLS];
+#pragma unroll
+        for (int c = 0; c < COLS; ++c) im[c] = __shfl_down_sync(0xffffffffu, v[c][t], 1);
         const int rr = 32 * jr + t;
-        if (rr < nr && x < s_W[rr]) {
-          float re[COLS], im[COLS];
+        if (writer && rr < nr && xp < s_W[rr]) {
+          float4* dst = reinterpret_cast<float4*>(a.B + ((size_t)(r0 + rr) * XS_N + xp) * XS_NCOL + c0);
 #pragma unroll
-          for (int c = 0; c < COLS; ++c) {
-            re[c] = S[((0 * 32 + t) * COLS + c) * XS_N + x];
-            im[c] = S[((1 * 32 + t) * COLS + c) * XS_N + x];
-          }
-          float4* dst = reinterpret_cast<float4*>(a.B + ((size_t)(r0 + rr) * XS_N + x) * XS_NCOL + c0);
-#pragma unroll
-          for (int c = 0; c < COLS; c += 2) dst[c / 2] = make_float4(re[c], im[c], re[c + 1], im[c + 1]);
+          for (int c = 0; c < COLS; c += 2) dst[c / 2] = make_float4(v[c][t], im[c], v[c + 1][t], im[c + 1]);
         }
       }
-      __syncthreads();
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -771,13 +764,12 @@ __global__ void __launch_bounds__(TA_THREADS, 1) k_xpass_tmema64(WaveArgs a, con
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       if (__any_sync(0xffffffffu, s_fail != 0)) break;
       float2* dst = a.B + (size_t)(r0 + rr) * XS_N * XS_NCOL + c0 + c;
-      for (int x0 = 0; x0 < XS_N; x0 += 16) {
-        float re[16], im[16];
-        tmem_ld16(tmem + lane_base + (uint32_t)(c * TA_R + x0), re);
-        tmem_ld16(tmem + lane_base + (uint32_t)(c * TA_R + XS_N + x0), im);
+      for (int x0 = 0; x0 < XS_N; x0 += 8) {
+        float v[16];  // operator columns 2x' (real), 2x' + 1 (imaginary) for x' = x0 .. x0 + 7
+        tmem_ld16(tmem + lane_base + (uint32_t)(c * TA_R + 2 * x0), v);
 #pragma unroll
-        for (int t = 0; t < 16; ++t)
-          if (x0 + t < Wr) dst[(size_t)(x0 + t) * XS_NCOL] = make_float2(re[t], im[t]);
+        for (int t = 0; t < 8; ++t)
+          if (x0 + t < Wr) dst[(size_t)(x0 + t) * XS_NCOL] = make_float2(v[2 * t], v[2 * t + 1]);
       }
     }
   }
