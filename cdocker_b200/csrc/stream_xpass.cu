@@ -15,11 +15,13 @@
 // K order: step j (16 wide) = group 2j (re part of planes 8j..8j+7) and group 2j+1 (im part).
 // Steps outside the chunks any rotation of the CTA occupies are neither loaded nor multiplied.
 //
-// CTA = COLS columns x 128 rotations, 256 threads: 2 columns, 96 KB ring, 256 TMEM columns and
-// two CTAs per SM when two stages fit the ring (ligand box <= 24 planes), else 4 columns (32
-// bytes of B per (rotation, x')), 192 KB ring, 512 TMEM columns, one CTA per SM. Stages are
-// (channel, column) pairs; a stage is 4 tiles of ceil(Lb/8) K-steps. Warp-specialized: warps 0-3 produce (thread = rotation; thread 0 also issues the
-// operator bulk copies), each stage's "full" mbarrier completing when every producer's copies
+// CTA = COLS columns x 128 rotations, 256 threads: 2 columns, a 96 KB ring (6 stages), 256
+// TMEM columns and two CTAs per SM for ligand boxes <= 24 planes, else 4 columns (32 bytes of B
+// per (rotation, x')), a 192 KB ring (12 stages), 512 TMEM columns, one CTA per SM. A stage is
+// one K-step of one (channel, column): operator hi, lo and ligand hi, lo tiles of 4 KB, three
+// MMAs; small stages keep many in flight. Warp-specialized: warps 0-3 produce (thread =
+// rotation; thread 0 also issues the operator bulk copies), each stage's "full" mbarrier
+// completing when every producer's copies
 // have landed (cp.async.mbarrier.arrive.noinc) and the operator bytes arrived; one thread of
 // warp 4 waits for it, issues the MMAs and commits them to the stage's "empty" mbarrier, which
 // the producers wait on before refilling the buffer. All 8 warps run the epilogue. Every wait
@@ -40,11 +42,12 @@ constexpr int XS_R = 128;
 constexpr int XS_M = 128;
 constexpr int XS_THREADS = 256;
 constexpr int XS_PRODUCERS = 128;  // warps 0-3: one producer thread per rotation of the tile
-constexpr int XS_MAXSTAGES = 8;
+constexpr int XS_MAXSTAGES = 12;
 constexpr int XS_JMAX = 4;                          // x chunks of 8 planes (Lb <= 32)
 constexpr uint32_t XS_GROUP = (XS_M / 8) * 128;     // 2048 B: one K group of 8 for 128 rows
 constexpr uint32_t XS_STEP = 2 * XS_GROUP;          // 4096 B: one K step of 16
 constexpr uint32_t XS_TILE = XS_JMAX * XS_STEP;     // 16 KB: 128 rows x 64 K, bf16 (operator image)
+constexpr uint32_t XS_SSTAGE = 4 * XS_STEP;         // 16 KB ring stage: T hi, T lo, L hi, L lo
 // Two shapes: 2 columns per CTA with a 96 KB ring (two CTAs per SM, so one CTA's epilogue and
 // MMA-issue gaps overlap the other's work) when stages are at most 48 KB (ligand box <= 24
 // planes), else 4 columns with a 192 KB ring (one CTA per SM).
@@ -188,10 +191,8 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS>::MIN_BLOCKS)
   __shared__ int s_act[KMAX], s_nact;
   __shared__ int s_W[XS_R];
   const int K = a.K;
-  // ring geometry: tiles of jc K-steps (the planned box's x chunks), as many stages as fit
-  const uint32_t tile = (uint32_t)jc * XS_STEP;
-  const uint32_t stage = 4 * tile;
-  const int nb = min(XS_MAXSTAGES, (int)(Shape::RING / stage));
+  // ring: stages of one K-step (operator hi, lo and ligand hi, lo tiles of 4 KB), as many as fit
+  const int nb = min(XS_MAXSTAGES, (int)(Shape::RING / XS_SSTAGE));
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r0 = blockIdx.x * XS_R;
   const int c0 = blockIdx.y * COLS;
@@ -267,21 +268,23 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS>::MIN_BLOCKS)
   }
   __syncthreads();
   const uint32_t tmem = s_tmem;
-  const int NS = s_nact * COLS;  // stages: (active channel, column), column fastest
   const unsigned char* lop = a.lop;
   const uint32_t ring_s = smem_u32(ring);
   // stage parameters in registers (4 bits per active channel: id, first and last K-step), so
   // the loops below read no shared memory but the mbarriers
   uint64_t pk = 0, pl = 0, ph = 0;
+  int NS = 0;  // stages: one K-step of one (channel, column); order channel, column, step
   for (int i = 0; i < s_nact; ++i) {
     const int k = s_act[i];
     pk |= (uint64_t)k << (4 * i);
     pl |= (uint64_t)s_jlo[k] << (4 * i);
     ph |= (uint64_t)s_jhi[k] << (4 * i);
+    NS += COLS * (s_jhi[k] - s_jlo[k] + 1);
   }
+  const int nact = s_nact;
 
   if (tid < XS_PRODUCERS) {
-    // ---- producers: thread = rotation rr of the tile; per stage its 4 * nj split rows
+    // ---- producers: thread = rotation rr of the tile; per stage its 4 split rows
     const int rr = tid;
     const uint32_t row_s = (uint32_t)(rr >> 3) * 128 + (uint32_t)(rr & 7) * 16;
     const int rg = r0 + (rr < nr ? rr : 0);
@@ -295,116 +298,96 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS>::MIN_BLOCKS)
       if (k < 8) jr_lo |= v << (8 * k);
       else jr_hi |= v << (8 * (k - 8));
     }
-    int s = 0, b = 0, ci = 0, ai = 0;
+    int s = 0, b = 0;
     uint32_t round = 0;  // s / nb
-    for (; s < NS; ++s) {
-      if (s >= nb) {
-        // the MMAs of stage s - nb must be done with this buffer
-        if (!mbar_wait(smem_u32(&s_empty[b]), (round - 1) & 1u)) {
-          atomicOr(&s_fail, 1);
-          break;
-        }
-      }
+    for (int ai = 0; ai < nact && s >= 0; ++ai) {
       const int k = (int)((pk >> (4 * ai)) & 15);
-      const int c = ci;
       const int jlo = (int)((pl >> (4 * ai)) & 15), jhi = (int)((ph >> (4 * ai)) & 15);
-      const int nj = jhi - jlo + 1;
-      const uint32_t st = ring_s + (uint32_t)b * stage;
-      const uint32_t full = smem_u32(&s_full[b]);
-      if (tid == 0) {
-        const uint32_t bytes = (uint32_t)nj * XS_STEP;
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(2 * bytes), "r"(full)
-                     : "memory");
-#pragma unroll
-        for (int hl = 0; hl < 2; ++hl) {
-          const unsigned char* src = top + (((size_t)(c0 + c) * K + k) * 2 + hl) * XS_TILE + (size_t)jlo * XS_STEP;
-          const uint32_t dst = st + (uint32_t)hl * tile + (uint32_t)jlo * XS_STEP;
-          asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                       "l"(src), "r"(bytes), "r"(full)
-                       : "memory");
-        }
-        s_issued = s + 1;
-      }
       const unsigned int jr = (unsigned int)(((k < 8 ? jr_lo : jr_hi) >> (8 * (k & 7))) & 255);
       const int jl = (int)(jr & 15), jh = (int)(jr >> 4);
-      const uint4* src0 = reinterpret_cast<const uint4*>(lop) + rot_rows + (size_t)k * 16 * RS + c;
-      for (int j = jlo; j <= jhi; ++j) {
-        const bool have = jl <= j && j <= jh;
-#pragma unroll
-        for (int hl = 0; hl < 2; ++hl)
-#pragma unroll
-          for (int part = 0; part < 2; ++part) {
-            const uint4* src = src0 + (size_t)((hl * 4 + j) * 2 + part) * RS;
-            const uint32_t dst = st + (uint32_t)(2 + hl) * tile + (uint32_t)j * XS_STEP +
-                                 (uint32_t)part * XS_GROUP + row_s;
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(have ? 16 : 0)
-                         : "memory");
+      for (int c = 0; c < COLS && s >= 0; ++c) {
+        const uint4* src0 = reinterpret_cast<const uint4*>(lop) + rot_rows + (size_t)k * 16 * RS + c;
+        const unsigned char* tsrc = top + ((size_t)(c0 + c) * K + k) * 2 * XS_TILE;
+        for (int j = jlo; j <= jhi; ++j, ++s) {
+          if (s >= nb) {
+            // the MMAs of stage s - nb must be done with this buffer
+            if (!mbar_wait(smem_u32(&s_empty[b]), (round - 1) & 1u)) {
+              atomicOr(&s_fail, 1);
+              s = -1;
+              break;
+            }
           }
-      }
-      asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(full) : "memory");
-      if (++b == nb) {
-        b = 0;
-        ++round;
-      }
-      if (++ci == COLS) {
-        ci = 0;
-        ++ai;
+          const uint32_t st = ring_s + (uint32_t)b * XS_SSTAGE;
+          const uint32_t full = smem_u32(&s_full[b]);
+          if (tid == 0) {
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(2 * XS_STEP), "r"(full)
+                         : "memory");
+#pragma unroll
+            for (int hl = 0; hl < 2; ++hl)
+              asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                               st + (uint32_t)hl * XS_STEP),
+                           "l"(tsrc + (size_t)hl * XS_TILE + (size_t)j * XS_STEP), "r"(XS_STEP), "r"(full)
+                           : "memory");
+            s_issued = s + 1;
+          }
+          const bool have = jl <= j && j <= jh;
+#pragma unroll
+          for (int hl = 0; hl < 2; ++hl)
+#pragma unroll
+            for (int part = 0; part < 2; ++part) {
+              const uint4* src = src0 + (size_t)((hl * 4 + j) * 2 + part) * RS;
+              const uint32_t dst = st + (uint32_t)(2 + hl) * XS_STEP + (uint32_t)part * XS_GROUP + row_s;
+              asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(have ? 16 : 0)
+                           : "memory");
+            }
+          asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(full) : "memory");
+          if (++b == nb) {
+            b = 0;
+            ++round;
+          }
+        }
       }
     }
   } else if (warp == XS_PRODUCERS / 32) {
     // ---- MMA issuer: the whole warp runs the loop, one elected lane issues
-    uint32_t acc_cols = 0;
     const uint64_t desc0 = make_desc(ring_s, XS_GROUP, 128);
-    int s = 0, b = 0, ci = 0, ai = 0;
+    constexpr uint64_t TU = XS_STEP >> 4;  // one 4 KB tile in descriptor address units
+    int s = 0, b = 0;
     uint32_t round = 0;
-    for (; s < NS; ++s) {
-      if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_full[b]), round & 1u))) {
-        if (lane == 0) atomicOr(&s_fail, 1);
-        break;
-      }
-      // the producers' cp.async writes (generic proxy) reach the tensor core (async proxy)
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int c = ci;
+    bool good = true;
+    for (int ai = 0; ai < nact && good; ++ai) {
       const int jlo = (int)((pl >> (4 * ai)) & 15), jhi = (int)((ph >> (4 * ai)) & 15);
-      const uint32_t d = tmem + (uint32_t)(c * XS_R);
-      // descriptors: one per stage, the others by adding start-address units (16 B) -- a
-      // single thread issues every MMA, so its instruction count per MMA is the issue rate
-      const uint64_t d0 = desc0 + (uint64_t)((uint32_t)b * (stage >> 4) + (uint32_t)jlo * (XS_STEP >> 4));
-      const uint64_t tu = tile >> 4;
-#pragma unroll
-      for (int jj = 0; jj < XS_JMAX; ++jj) {
-        if (jlo + jj > jhi) break;
-        const uint64_t ah = d0 + (uint64_t)jj * (XS_STEP >> 4);
-        const uint64_t al = ah + tu, bh = ah + 2 * tu, bl = ah + 3 * tu;
-        const uint32_t acc = (acc_cols >> c) & 1u;
-        acc_cols |= 1u << c;
-        if (elect_one()) umma_f16(d, ah, bh, acc);
-        if (elect_one()) umma_f16(d, ah, bl, 1u);
-        if (elect_one()) umma_f16(d, al, bh, 1u);
-      }
-      if (elect_one())
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                         smem_u32(&s_empty[b]))
-                     : "memory");
-      __syncwarp();
-      if (++b == nb) {
-        b = 0;
-        ++round;
-      }
-      if (++ci == COLS) {
-        ci = 0;
-        ++ai;
+      for (int c = 0; c < COLS && good; ++c) {
+        const uint32_t d = tmem + (uint32_t)(c * XS_R);
+        for (int j = jlo; j <= jhi; ++j, ++s) {
+          if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_full[b]), round & 1u))) {
+            if (lane == 0) atomicOr(&s_fail, 1);
+            good = false;
+            break;
+          }
+          // the producers' cp.async writes (generic proxy) reach the tensor core (async proxy)
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint64_t ah = desc0 + (uint64_t)b * (XS_SSTAGE >> 4);
+          const uint32_t acc = (ai > 0 || j > jlo) ? 1u : 0u;  // first product of column c
+          if (elect_one()) umma_f16(d, ah, ah + 2 * TU, acc);
+          if (elect_one()) umma_f16(d, ah, ah + 3 * TU, 1u);
+          if (elect_one()) umma_f16(d, ah + TU, ah + 2 * TU, 1u);
+          if (elect_one())
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&s_empty[b]))
+                         : "memory");
+          __syncwarp();
+          if (++b == nb) {
+            b = 0;
+            ++round;
+          }
+        }
       }
     }
     if (lane == 0) {
       s_consumed = s;
-      unsigned long long steps = 0;  // K-steps issued by this CTA (work counter)
-      for (int t = 0; t < s; ++t) {
-        const int at = t / COLS;
-        steps += (unsigned long long)(((ph >> (4 * at)) & 15) - ((pl >> (4 * at)) & 15) + 1);
-      }
-      if (steps && a.work) atomicAdd(a.work + 2, steps);
+      if (s && a.work) atomicAdd(a.work + 2, (unsigned long long)s);  // K-steps issued
       // the newest commit completes after every earlier MMA of this warp
       if (s > 0 && !mbar_wait(smem_u32(&s_empty[(s - 1) % nb]), (uint32_t)((s - 1) / nb) & 1u))
         atomicOr(&s_fail, 1);
