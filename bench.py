@@ -196,6 +196,35 @@ def clustering_sample(n_conf: int = 1000, n_atoms: int = 40, max_centers: int = 
             "_check": {"inputs": (x, e, 1.5, max_centers), "got": got}}
 
 
+def receptor_grids_sample(n: int = 64, n_atoms: int = 2500, box: float = 32.0) -> dict:
+    """Receptor grid generation for the benchmark receptor's size (8 probe radii + elec): the
+    GPU call against the multithreaded host generator it must match bit for bit."""
+    import os as _os
+
+    from cdocker_b200 import api, synth
+    rng = np.random.default_rng(11)
+    xyz = rng.uniform(0.0, box, size=(n_atoms, 3)).astype(np.float32)
+    rad = rng.uniform(1.5, 2.0, n_atoms).astype(np.float32)
+    se = np.sqrt(rng.uniform(0.05, 0.2, n_atoms)).astype(np.float32)
+    q = rng.normal(0.0, 0.3, n_atoms).astype(np.float32)
+    origin = np.full(3, box / 2 - (n - 1) * 0.25, np.float32)
+    args = (n, 0.5, origin, xyz, rad, se, q, synth.PROBE_RADII)
+    api.synth_receptor_grids(*args, device=0)  # first call: module load
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        dev = api.synth_receptor_grids(*args, device=0)
+    t_gpu = (time.perf_counter() - t0) / reps
+    t0 = time.perf_counter()
+    host = api.synth_receptor_grids(*args)
+    t_host = time.perf_counter() - t0
+    return {"n": n, "receptor_atoms": n_atoms, "grids": int(dev.shape[0]),
+            "gpu_ms": round(t_gpu * 1e3, 3), "host_ms": round(t_host * 1e3, 3),
+            "host_threads": _os.cpu_count(),
+            "bit_identical": bool(np.array_equal(dev.view(np.uint32), host.view(np.uint32))),
+            "note": "host call each: H2D of atoms, one kernel, D2H of the grids"}
+
+
 def reference_cufft_sample(w, n_rot: int = 1000) -> dict:
     """The reference's own cuFFT path (oracle/_ref, batch 50, host fill, PCIe copies)."""
     from oracle import oracle as O
@@ -405,6 +434,7 @@ def run_ours(args, rank, world, local_rank):
         forms[name] = {"rec": rec, "ms": ms, "stats": stats, "clocks": clocks, "acc": None,
                        "e": e, "i": i, "value": world * n_rot * args.steps / (ms / 1e3)}
     clustering = clustering_sample() if rank == 0 else None
+    grids_gen = receptor_grids_sample() if rank == 0 else None
     cpu_base, clus_check = None, None
     if rank == 0:
         base, acc, clus_check = cpu_leg(w, args, {k: (v["e"], v["i"]) for k, v in forms.items()},
@@ -507,6 +537,8 @@ def run_ours(args, rank, world, local_rank):
             if clus_check:
                 clustering.update(clus_check)
             line["clustering"] = clustering
+        if grids_gen is not None:
+            line["receptor_grids"] = grids_gen
         if cpu_base is not None:
             line["cpu_baseline"] = cpu_base
         print(json.dumps(line), flush=True)

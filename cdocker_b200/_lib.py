@@ -89,6 +89,8 @@ SIGNATURES = {
                                   C.c_float, C.c_float, _fp, _fp]),
     "cdk_synth_receptor_grids": (C.c_int, [C.c_int, C.c_float, _fp, C.c_int, _fp, _fp, _fp, _fp,
                                            C.c_int, _fp, C.c_float, C.c_float, C.c_float, _fp]),
+    "cdk_receptor_grids_gpu": (C.c_int, [C.c_int, C.c_int, C.c_float, _fp, C.c_int, _fp, _fp, _fp,
+                                         _fp, C.c_int, _fp, C.c_float, C.c_float, C.c_float, _fp]),
     "cdk_ctx_stats": (C.c_int, [_vp, _dp, C.c_int]),
     "cdk_server_opts_default": (None, [C.POINTER(CdkServerOpts)]),
     "cdk_server_create": (C.c_int, [_vp, C.POINTER(CdkServerOpts), C.POINTER(_vp)]),

@@ -107,13 +107,17 @@ def write_grids(path: str, values, radii, mid, length, spacing: float, restraint
 
 
 def synth_receptor_grids(n, spacing, origin, xyz, radius, sqrt_eps, charge, probe_radii,
-                         vdw_cap=3.0, elec_cap=40.0, cutoff=12.0) -> np.ndarray:
-    """Seeded synthetic receptor grids [len(probe_radii)+1, n, n, n] (host, multithreaded)."""
+                         vdw_cap=3.0, elec_cap=40.0, cutoff=12.0, device=None) -> np.ndarray:
+    """Receptor potential grids [len(probe_radii)+1, n, n, n]: soft-core capped LJ per probe
+    radius, then the eps(r)=4r Coulomb grid. device=None computes on the host (multithreaded);
+    an int computes on that CUDA device, bit-identical to the host result."""
     p = _f32(probe_radii)
     xyz = _f32(xyz).reshape(-1, 3)
     out = np.empty((p.shape[0] + 1, n, n, n), np.float32)
-    L.check(L.lib().cdk_synth_receptor_grids(
-        n, float(spacing), _pf(_f32(origin)), xyz.shape[0], _pf(xyz), _pf(_f32(radius)),
+    head = () if device is None else (int(device),)
+    fn = L.lib().cdk_synth_receptor_grids if device is None else L.lib().cdk_receptor_grids_gpu
+    L.check(fn(
+        *head, n, float(spacing), _pf(_f32(origin)), xyz.shape[0], _pf(xyz), _pf(_f32(radius)),
         _pf(_f32(sqrt_eps)), _pf(_f32(charge)), p.shape[0], _pf(p), float(vdw_cap),
         float(elec_cap), float(cutoff), _pf(out)))
     return out

@@ -479,7 +479,10 @@ int cdk_synth_receptor_grids(int n, float spacing, const float* origin, int nAto
                                origin[2] + (double)k * spacing};
           std::fill(acc.begin(), acc.end(), 0.0);
           int c[3];
-          for (int d = 0; d < 3; ++d) c[d] = (int)std::floor((p[d] - lo[d]) / cutoff);
+          // cells beyond [-2, nc+1] have no occupied neighbours; clamping keeps the
+          // conversion to int defined for points far from every atom
+          for (int d = 0; d < 3; ++d)
+            c[d] = (int)std::floor(std::min(std::max((p[d] - lo[d]) / cutoff, -2.0), nc[d] + 1.0));
           for (int cx = c[0] - 1; cx <= c[0] + 1; ++cx)
             for (int cy = c[1] - 1; cy <= c[1] + 1; ++cy)
               for (int cz = c[2] - 1; cz <= c[2] + 1; ++cz) {

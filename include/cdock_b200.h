@@ -200,6 +200,16 @@ int cdk_synth_receptor_grids(int n, float spacing, const float* origin, int nAto
                              const float* charge, int nVdw, const float* probeRadii,
                              float vdwCap, float elecCap, float cutoff, float* out);
 
+/* The same grids computed on CUDA device `device` (one thread per grid point, double
+ * accumulation with round-to-nearest operations in the host function's order, so the output
+ * is bit-identical to cdk_synth_receptor_grids). Host inputs and output; nVdw <= 15. The
+ * reference reads these grids from CHARMM-written files (src/ReadGrids.cpp:6-68); this
+ * replaces the CHARMM grid-generation step upstream of cdk_read_grids. */
+int cdk_receptor_grids_gpu(int device, int n, float spacing, const float* origin, int nAtom,
+                           const float* xyz, const float* radius, const float* sqrtEps,
+                           const float* charge, int nVdw, const float* probeRadii,
+                           float vdwCap, float elecCap, float cutoff, float* out);
+
 /* ---- serving: continuous batching over one resident receptor ----
  * A server owns a worker thread and a stream on the context's device. Requests (a ligand
  * with its conformers and rotations) are admitted when their inputs and outputs fit the
