@@ -295,6 +295,13 @@ def run_reference(args, rank, world):
 
 
 TENSOR_STEP_FLOP = 3 * 2 * 128 * 128 * 16  # one K-step of the streamed x pass: 3 BF16 MMAs
+# split-FP16 form: 2 FP16 MMAs per K-step and FP16 ligand rows (half the bytes of split BF16)
+TENSOR_STEP_FLOP_FP16 = 2 * 2 * 128 * 128 * 16
+
+
+def FORMS(fp32, bf16x3, fp16x2):
+    """(name, form) of the three search forms, in bench order."""
+    return (("fp32", fp32), ("bf16x3_tensor_core", bf16x3), ("fp16x2_tensor_core", fp16x2))
 
 
 def _kernel_roofline(stats: dict, n: int, K: int, hbm: float, peak_kind: str, traffic: dict):
@@ -313,12 +320,15 @@ def _kernel_roofline(stats: dict, n: int, K: int, hbm: float, peak_kind: str, tr
     dom = max(km, key=km.get)
     plane = ncol * 8
     rot = stats["rotations"]
-    streamed = stats.get("xpass_kind") == "tcgen05_streamed"
+    kind = stats.get("xpass_kind")
+    fp16 = kind == "tcgen05_streamed_fp16"
+    streamed = kind == "tcgen05_streamed" or fp16
+    lig = plane // 2 if fp16 else plane  # ligand bytes per plane: FP16 rows, split BF16 or FP32
     jc = (stats["box"] + 7) // 8
     receptor = K * ncol * 2 * jc * 4096 if streamed else K * n * plane
     alg = {
-        "xpass": (stats["planes_spread"] + stats["planes_window"]) * plane + waves * receptor,
-        "spread_yz": stats["planes_spread"] * plane,
+        "xpass": stats["planes_spread"] * lig + stats["planes_window"] * plane + waves * receptor,
+        "spread_yz": stats["planes_spread"] * lig,
         "yz_inv_argmin": stats["planes_window"] * plane,
         "prep": rot * 1024,
         "finalize": rot * 32,
@@ -335,7 +345,7 @@ def _kernel_roofline(stats: dict, n: int, K: int, hbm: float, peak_kind: str, tr
            "share_of_device_time": km[dom] / max(1e-9, sum(km.values())), "kernel_ms": km}
     if dom == "xpass" and streamed and stats.get("tensor_steps"):
         tp, tkind = _tensor_peak()
-        flop = stats["tensor_steps"] * TENSOR_STEP_FLOP / waves
+        flop = stats["tensor_steps"] * (TENSOR_STEP_FLOP_FP16 if fp16 else TENSOR_STEP_FLOP) / waves
         tach = flop / t / 1e12
         out.update({"bound": "tensor", "achieved": tach, "peak": tp, "unit": "TFLOP/s",
                     "frac": tach / tp, "peak_kind": tkind, "flop_per_launch": flop,
@@ -365,7 +375,7 @@ def _accuracy_sample(w, e, i, n_sample=24):
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
-    from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP32, Receptor
+    from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP16X2, CDK_FORM_FP32, Receptor
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -427,8 +437,8 @@ def run_ours(args, rank, world, local_rank):
         return rec, ms, stats, clocks, e, i
 
     forms = {}
-    for name, form in (("fp32", CDK_FORM_FP32), ("bf16x3_tensor_core", CDK_FORM_BF16X3)):
-        if args.forms != "both" and args.forms != name:
+    for name, form in FORMS(CDK_FORM_FP32, CDK_FORM_BF16X3, CDK_FORM_FP16X2):
+        if args.forms not in ("both", "all") and args.forms != name:
             continue
         rec, ms, stats, clocks, e, i = timed_form(form)
         forms[name] = {"rec": rec, "ms": ms, "stats": stats, "clocks": clocks, "acc": None,
@@ -443,7 +453,7 @@ def run_ours(args, rank, world, local_rank):
         for k, v in acc.items():
             forms[k]["acc"] = v
     # headline: the fastest form that meets its error bar on the checked sample
-    bars = {"fp32": 1e-4, "bf16x3_tensor_core": 1e-3}
+    bars = {"fp32": 1e-4, "bf16x3_tensor_core": 1e-3, "fp16x2_tensor_core": 1e-3}
     ok = [k for k, v in forms.items()
           if v["acc"] is None or v["acc"]["max_rel_err_vs_fp64"] <= bars[k]]
     head = max(ok or list(forms), key=lambda k: forms[k]["value"])
@@ -551,14 +561,14 @@ def serving_sample(w, rec_unused, secs: float) -> dict:
     arrivals of requests with ligands of 10-80 atoms, 10-50 conformers, 500-2,000 rotations,
     served by each form (the precision form runs its waves on the streamed tensor-core x
     pass; `tc_waves` counts them)."""
-    from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP32, Receptor, synth
+    from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP16X2, CDK_FORM_FP32, Receptor, synth
     from cdocker_b200.serving import Server, make_requests, poisson_arrivals, run_load
     rate = 40.0
     arr = poisson_arrivals(rate, secs, seed=7)
     reqs = make_requests(len(arr), 21, w.spacing, w.length, synth.PROBE_RADII, atoms=(10, 80),
                          confs=(10, 50), rots=(500, 2000))
     out = {}
-    for name, form in (("fp32", CDK_FORM_FP32), ("bf16x3_tensor_core", CDK_FORM_BF16X3)):
+    for name, form in FORMS(CDK_FORM_FP32, CDK_FORM_BF16X3, CDK_FORM_FP16X2):
         with Receptor(w.all_grids, w.spacing, max_atoms=96, form=form) as r:
             with Server(r, arena_bytes=512 << 20, wave_rotations=1024, max_atoms=96) as srv:
                 res = run_load(srv, reqs, arr)
@@ -574,11 +584,11 @@ def serve_sweep(args):
     """Config 3: one resident 96^3 receptor (6,000 atoms in a 48 A cube, K = 9), requests with
     ligands of 10-80 atoms, 10-200 conformers, 500-5,000 rotations, Poisson arrivals at five
     rates; both forms. Prints one JSON line per (form, rate)."""
-    from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP32, Receptor, synth
+    from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP16X2, CDK_FORM_FP32, Receptor, synth
     from cdocker_b200.serving import Server, make_requests, poisson_arrivals, run_load
     grids, mid, length = synth.make_receptor(96, 6000, 48.0, seed=0)
     secs = max(2.0, args.serve_secs)
-    for form_name, form in (("fp32", CDK_FORM_FP32), ("bf16x3_tensor_core", CDK_FORM_BF16X3)):
+    for form_name, form in FORMS(CDK_FORM_FP32, CDK_FORM_BF16X3, CDK_FORM_FP16X2):
         with Receptor(grids, 0.5, max_atoms=96, form=form) as rec:
             for rate in (2.0, 5.0, 10.0, 20.0, 40.0):
                 arr = poisson_arrivals(rate, secs, seed=int(rate * 10))
@@ -599,7 +609,7 @@ def profile_run(args):
     """One warm-up and one timed search of `--profile-run` rotations (first conformers of the
     config-1 workload), per-kernel device times from events around every launch."""
     import torch
-    from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP32, Receptor
+    from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP16X2, CDK_FORM_FP32, Receptor
     w = make_rank_workload(0, 1)
     n_q = N_Q
     n_conf = max(1, min(N_CONF, (args.profile_run + n_q - 1) // n_q))
@@ -615,7 +625,8 @@ def profile_run(args):
     e = torch.empty(n_rot, device=dev)
     i = torch.empty(n_rot, 3, dtype=torch.int32, device=dev)
     out = {}
-    form = CDK_FORM_BF16X3 if args.forms == "bf16x3_tensor_core" else CDK_FORM_FP32
+    form = {"bf16x3_tensor_core": CDK_FORM_BF16X3,
+            "fp16x2_tensor_core": CDK_FORM_FP16X2}.get(args.forms, CDK_FORM_FP32)
     with Receptor(w.grids, w.spacing, wave_rotations=args.wave, col_tile=args.col_tile,
                   profile=True, form=form) as rec:
         for it in range(2):
@@ -640,7 +651,8 @@ def main():
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--ref-cufft", type=int, default=1)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
-    ap.add_argument("--forms", default="both", choices=["both", "fp32", "bf16x3_tensor_core"])
+    ap.add_argument("--forms", default="all",
+                    choices=["all", "both", "fp32", "bf16x3_tensor_core", "fp16x2_tensor_core"])
     ap.add_argument("--serve-secs", type=float, default=3.0)
     ap.add_argument("--serve-sweep", action="store_true",
                     help="config 3: 96^3 receptor, Poisson request streams at 5 rates; one JSON "

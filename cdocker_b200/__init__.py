@@ -9,7 +9,7 @@ behind the C-ABI (include/cdock_b200.h); this package only marshals arrays:
 Host helpers keep the reference's semantics bit for bit (quaternion sampling and filtering,
 vdW slot assignment, grid file I/O).
 """
-from ._lib import CdkError, CDK_FORM_FP32, CDK_FORM_BF16X3, lib, last_error  # noqa: F401
+from ._lib import CdkError, CDK_FORM_FP32, CDK_FORM_BF16X3, CDK_FORM_FP16X2, lib, last_error  # noqa: F401
 from .api import (  # noqa: F401
     Receptor,
     fill_ligand_grid,

@@ -23,6 +23,7 @@ CDK_ERR_BUSY = 7
 
 CDK_FORM_FP32 = 0
 CDK_FORM_BF16X3 = 1
+CDK_FORM_FP16X2 = 2
 
 
 class CdkOpts(C.Structure):

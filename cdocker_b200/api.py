@@ -230,5 +230,6 @@ class Receptor:
                 "col_tile": int(out[13]), "rotations_per_cta": int(out[14]),
                 "graph_state": int(out[15]),
                 "xpass_kind": ["fp32_radix", "mma_sync", "tcgen05_build",
-                               "tcgen05_streamed", "tcgen05_streamed_tmem"][int(out[16])],
+                               "tcgen05_streamed", "tcgen05_streamed_tmem",
+                               "tcgen05_streamed_fp16"][int(out[16])],
                 "tensor_steps": int(out[17])}

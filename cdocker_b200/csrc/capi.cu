@@ -108,12 +108,14 @@ struct cdk_ctx {
   float2* d_phat = nullptr;   // [n][K][ncol]
   float2* d_ptilde = nullptr; // [ncol][K][n] receptor transformed over (y,z) only, x n (BF16X3 form)
   void* d_top = nullptr;      // operator image of the streamed tensor-core x pass (built on first use)
+  float lscale[KMAX] = {};    // split-FP16 form: ligand scale 2^sigma_k (the operator carries 2^-sigma_k)
   float2* d_tw = nullptr;     // [n]
   int* d_kyof = nullptr;      // [n] natural frequency at each digit-reversed position
   Arena wave;                 // per-wave scratch
   Arena tables;               // per-search tables
   Arena io;                   // staging of host-buffer searches
-  unsigned int* d_misc = nullptr;  // [0] diameter bits, [1] flags, [2] error count
+  unsigned int* d_misc = nullptr;  // [0] diameter bits, [1] flags, [2] error count, [3] fault,
+                                   // [4] FP16 range flag
   unsigned long long* d_work = nullptr;  // [0] x planes spread (A), [1] window planes (B),
                                           // [2] tensor-core K-steps of the streamed x pass
   unsigned long long* h_work = nullptr;
@@ -221,13 +223,16 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
               cudaStream_t s) {
   const int n = c->n, K = c->K;
   const size_t ncol = (size_t)n * (n / 2 + 1);
-  const bool tc = c->opts.form == CDK_FORM_BF16X3;
+  const bool tc = c->opts.form != CDK_FORM_FP32;
+  const bool f16form = c->opts.form == CDK_FORM_FP16X2;
   // streamed tensor-core x pass: n = 64, box <= 32 planes, direct planes (<= 96 atoms)
   WaveArgs probe{};
   probe.kyof = (c->opts.reserved[1] == 0) ? c->d_kyof : nullptr;
   probe.max_atoms = maxAtoms;
   probe.atom_cap = maxAtoms;
-  const int variant = c->opts.reserved[3];
+  // the split-FP16 form has the streamed kernel only; where that does not apply, the split-BF16
+  // kernels run (more accurate)
+  const int variant = f16form ? 0 : c->opts.reserved[3];
   const bool streamed = tc && (variant == 0 || variant == 3) && stream_supported(n, Lb) && direct_planes(probe);
   const bool tmem_ligand = variant == 3;
   if (streamed && !c->d_top) {
@@ -237,9 +242,13 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
       set_error("cudaMalloc of the tensor-core operator image failed (" + std::to_string(tb >> 20) + " MiB)");
       return CDK_ERR_NOMEM;
     }
-    CDK_CUDA(launch_top_build(n, K, c->d_ptilde, c->d_top, s));  // stream-ordered before the waves
+    std::vector<float> osc(K);
+    for (int k = 0; k < K; ++k) osc[k] = 1.f / c->lscale[k];
+    // stream-ordered before the waves
+    CDK_CUDA(launch_top_build(n, K, c->d_ptilde, c->d_top, f16form ? osc.data() : nullptr, s));
   }
-  const size_t lop_per = streamed ? stream_lop_bytes_per_rotation(n, K) : 0;
+  const bool f16 = f16form && streamed;
+  const size_t lop_per = streamed ? stream_lop_bytes_per_rotation(n, K, f16) : 0;
   int wave = c->opts.wave_rotations;
   if (wave <= 0) {
     // keep A + B of one wave near 6 GiB: big enough to fill the GPU, small next to HBM
@@ -282,6 +291,9 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   a.idx = d_idx;
   a.err_count = reinterpret_cast<int*>(c->d_misc + 2);
   a.fault = reinterpret_cast<int*>(c->d_misc + 3);
+  a.f16 = f16 ? 1 : 0;
+  for (int k = 0; k < KMAX; ++k) a.lscale[k] = c->lscale[k];
+  a.range_err = reinterpret_cast<int*>(c->d_misc + 4);
   a.col_tile = c->opts.col_tile > 0 ? c->opts.col_tile : pick_col_tile(n, K);
   a.kyof = (c->opts.reserved[1] == 0) ? c->d_kyof : nullptr;  // reserved[1] = 1: FFT planes
   a.chunk = 0;
@@ -298,7 +310,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     set_error("column tile must be 8 or 16 (n <= 64) or 8 (n > 64) and fit shared memory");
     return CDK_ERR_INVALID;
   }
-  CDK_CUDA(cudaMemsetAsync(c->d_misc + 2, 0, 2 * sizeof(unsigned int), s));
+  CDK_CUDA(cudaMemsetAsync(c->d_misc + 2, 0, 3 * sizeof(unsigned int), s));
   CDK_CUDA(cudaMemsetAsync(c->d_work, 0, 4 * sizeof(unsigned long long), s));
   const bool umma = tc && !streamed && c->opts.reserved[3] != 1 && umma_supported(n, Lb);
   a.work = c->d_work;
@@ -349,7 +361,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   c->stats[5] = (double)wave;
   c->stats[13] = streamed ? 4.0 : (double)a.col_tile;
   c->stats[14] = streamed || umma ? 128.0 : (double)(a.chunk > 0 ? a.chunk : (tc ? 64 : 32));
-  c->stats[16] = streamed ? (tmem_ligand ? 4.0 : 3.0) : umma ? 2.0 : tc ? 1.0 : 0.0;  // 3: default
+  c->stats[16] = f16 ? 5.0 : streamed ? (tmem_ligand ? 4.0 : 3.0) : umma ? 2.0 : tc ? 1.0 : 0.0;
   c->stats[15] = (double)(c->gkey_seen);
   return CDK_OK;
 }
@@ -470,7 +482,7 @@ int search_device_impl(cdk_ctx* c, int nAtom, int nConf, const float* d_coor,
 }
 
 int check_errors_after(cdk_ctx* c, cudaStream_t s) {
-  CDK_CUDA(cudaMemcpyAsync(c->h_misc + 2, c->d_misc + 2, 2 * sizeof(unsigned int),
+  CDK_CUDA(cudaMemcpyAsync(c->h_misc + 2, c->d_misc + 2, 3 * sizeof(unsigned int),
                            cudaMemcpyDeviceToHost, s));
   CDK_CUDA(cudaStreamSynchronize(s));
   if (c->h_misc[3] != 0) {
@@ -496,6 +508,11 @@ int check_errors_after(cdk_ctx* c, cudaStream_t s) {
               " rotation(s) overflowed the planned ligand box; results for them are invalid");
     return CDK_ERR_OVERFLOW;
   }
+  if (c->h_misc[4] != 0) {
+    set_error("a scaled ligand spectrum value left the FP16 range of the split-FP16 form "
+              "(charges or sqrt-epsilon sums too large for this receptor); use CDK_FORM_BF16X3");
+    return CDK_ERR_UNSUPPORTED;
+  }
   return CDK_OK;
 }
 
@@ -518,12 +535,13 @@ bool ctx_view(const cdk_ctx* c, CtxView* v) {
   v->form = c->opts.form;
   v->tc_variant = c->opts.reserved[3];
   v->top = c->d_top;
+  for (int k = 0; k < KMAX; ++k) v->lscale[k] = c->lscale[k];
   return true;
 }
 
 int ctx_ensure_top(cdk_ctx* c) {
   if (c->d_top) return CDK_OK;
-  if (c->opts.form != CDK_FORM_BF16X3 || !c->d_ptilde) {
+  if (c->opts.form == CDK_FORM_FP32 || !c->d_ptilde) {
     set_error("the operator image needs a precision-form context");
     return CDK_ERR_INVALID;
   }
@@ -537,7 +555,10 @@ int ctx_ensure_top(cdk_ctx* c) {
     set_error("cudaMalloc of the tensor-core operator image failed (" + std::to_string(tb >> 20) + " MiB)");
     return CDK_ERR_NOMEM;
   }
-  cudaError_t e = launch_top_build(c->n, c->K, c->d_ptilde, c->d_top, c->stream);
+  std::vector<float> osc(c->K);
+  for (int k = 0; k < c->K; ++k) osc[k] = 1.f / c->lscale[k];
+  cudaError_t e = launch_top_build(c->n, c->K, c->d_ptilde, c->d_top,
+                                   c->opts.form == CDK_FORM_FP16X2 ? osc.data() : nullptr, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) {
     set_error(std::string("operator image: ") + cudaGetErrorString(e));
@@ -595,7 +616,7 @@ int cdk_ctx_create(int nx, int ny, int nz, float spacing, int K, const float* gr
   if (opts) c->opts = *opts;
   else cdk_opts_default(&c->opts);
   if (c->opts.max_atoms <= 0) c->opts.max_atoms = 256;
-  if (c->opts.form != CDK_FORM_FP32 && c->opts.form != CDK_FORM_BF16X3) {
+  if (c->opts.form != CDK_FORM_FP32 && c->opts.form != CDK_FORM_BF16X3 && c->opts.form != CDK_FORM_FP16X2) {
     delete c;
     set_error("unknown form");
     return CDK_ERR_UNSUPPORTED;
@@ -625,8 +646,8 @@ int cdk_ctx_create(int nx, int ny, int nz, float spacing, int K, const float* gr
   CTX_CUDA(cudaMalloc(&c->d_grids, sizeof(float) * K * N));
   CTX_CUDA(cudaMalloc(&c->d_phat, sizeof(float2) * K * n * ncol));
   CTX_CUDA(cudaMalloc(&c->d_tw, sizeof(float2) * n));
-  CTX_CUDA(cudaMalloc(&c->d_misc, 4 * sizeof(unsigned int)));
-  CTX_CUDA(cudaMallocHost(&c->h_misc, 4 * sizeof(unsigned int)));
+  CTX_CUDA(cudaMalloc(&c->d_misc, 8 * sizeof(unsigned int)));
+  CTX_CUDA(cudaMallocHost(&c->h_misc, 8 * sizeof(unsigned int)));
   CTX_CUDA(cudaMalloc(&c->d_work, 4 * sizeof(unsigned long long)));
   CTX_CUDA(cudaMallocHost(&c->h_work, 4 * sizeof(unsigned long long)));
   std::vector<float2> tw(n);
@@ -648,7 +669,7 @@ int cdk_ctx_create(int nx, int ny, int nz, float spacing, int K, const float* gr
   CTX_CUDA(cudaMalloc(&scratch, sizeof(float2) * K * n * ncol));
   cudaError_t e = launch_receptor_fft(n, K, c->d_grids, scratch, c->d_phat, c->d_tw,
                                       pick_col_tile(n, 1), c->stream);
-  if (e == cudaSuccess && c->opts.form == CDK_FORM_BF16X3) {
+  if (e == cudaSuccess && c->opts.form != CDK_FORM_FP32) {
     e = cudaMalloc(&c->d_ptilde, sizeof(float2) * K * n * ncol);
     if (e == cudaSuccess) e = launch_ptilde(n, K, scratch, c->d_ptilde, c->stream);
   }
@@ -656,6 +677,24 @@ int cdk_ctx_create(int nx, int ny, int nz, float spacing, int K, const float* gr
   cudaFree(scratch);
   CTX_CUDA(e);
   CTX_CUDA(e2);
+  for (int k = 0; k < KMAX; ++k) c->lscale[k] = 1.f;
+  if (c->opts.form == CDK_FORM_FP16X2) {
+    // per channel the power of two that brings max |P~| into [2^14, 2^15): the operator image
+    // holds P~ 2^-sigma and the ligand rows carry 2^sigma (FP16 ends at 65504)
+    std::vector<float2> pt((size_t)K * n * ncol);
+    CTX_CUDA(cudaMemcpy(pt.data(), c->d_ptilde, sizeof(float2) * pt.size(), cudaMemcpyDeviceToHost));
+    std::vector<float> mx(K, 0.f);
+    for (size_t i = 0; i < pt.size(); ++i) {
+      const int k = (int)((i / n) % K);  // [ncol][K][n]
+      mx[k] = std::max(mx[k], std::max(std::fabs(pt[i].x), std::fabs(pt[i].y)));
+    }
+    for (int k = 0; k < K; ++k) {
+      int sigma = 0;
+      if (mx[k] > 0.f && std::isfinite(mx[k]))
+        sigma = std::min(30, std::max(-30, (int)std::floor(std::log2(mx[k])) - 14));
+      c->lscale[k] = std::ldexp(1.0f, sigma);
+    }
+  }
 #undef CTX_CUDA
   *out = c;
   return CDK_OK;

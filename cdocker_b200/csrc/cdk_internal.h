@@ -79,6 +79,10 @@ struct WaveArgs {
   int* fault;                // set when a bounded device wait gave up
   const int* kyof;           // [n] natural frequency at each digit-reversed position; when set
                              // (and ligands have <= 96 atoms) planes are evaluated directly
+  int f16;                   // split-FP16 form: the plane kernel writes FP16 rows (8 per rotation
+                             // and channel: [chunk][re, im]) of the planes times lscale[k]
+  float lscale[KMAX];        // split-FP16 form: 2^sigma_k per channel (a power of two, exact)
+  int* range_err;            // split-FP16 form: set when a scaled ligand value left the FP16 range
   unsigned char* lop;        // when set (n = 64, direct planes): the plane kernel writes the
                              // ligand as split-BF16 x-chunk rows here instead of A:
                              // [nrot/8][K][hi/lo][chunk j < 4][re/im][ncol/4][nrot%8][ncol%4]
@@ -125,8 +129,10 @@ cudaError_t launch_xpass_umma(const WaveArgs& a, const float2* pt, cudaStream_t 
 // from P~, the ligand rows come from the plane kernel (WaveArgs.lop)
 bool stream_supported(int n, int Lb);
 size_t stream_top_bytes(int n, int K);
-size_t stream_lop_bytes_per_rotation(int n, int K);
-cudaError_t launch_top_build(int n, int K, const float2* pt, void* top, cudaStream_t s);
+size_t stream_lop_bytes_per_rotation(int n, int K, bool f16);
+// f16_scale: nullptr = the split-BF16 image; else the split-FP16 image of P~ * f16_scale[k]
+cudaError_t launch_top_build(int n, int K, const float2* pt, void* top, const float* f16_scale,
+                             cudaStream_t s);
 // tmem_ligand: the ligand operand in tensor memory (k_xpass_tmema64), else in shared memory
 cudaError_t launch_xpass_stream(const WaveArgs& a, const void* top, bool tmem_ligand, cudaStream_t s);
 // true when launch_spread_yz takes the direct plane path (the only one that can write lop)
@@ -148,11 +154,12 @@ struct CtxView {
   const float2* phat;
   const float2* tw;
   const int* kyof;
-  unsigned int* h_misc;  // pinned host scratch of the context (4 words)
+  unsigned int* h_misc;  // pinned host scratch of the context (8 words)
   cudaStream_t stream;
   int form;              // CDK_FORM_*
   int tc_variant;        // opts.reserved[3]
   const void* top;       // operator image of the streamed tensor-core x pass (or null)
+  float lscale[KMAX];    // split-FP16 form: ligand scale 2^sigma_k per channel
 };
 
 }  // namespace cdk

@@ -18,6 +18,7 @@
 // in-place FFT stages produce; the receptor spectra are computed by the same stages, so
 // the pointwise product lines up without any permutation.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -422,6 +423,27 @@ __global__ void __launch_bounds__(256) k_spread_yz_direct(WaveArgs a, const int*
           const int x = x0 + d;
           if (x >= xlo && x <= xhi) a.A[(((size_t)r * a.K + k) * a.Lb + x) * NCOL + c] = make_float2(ax[d], ay[d]);
         }
+      } else if (a.f16) {
+        // split-FP16 form: FP16 rows of the 8 planes times 2^sigma_k (exact): per (rotation,
+        // channel) 8 rows [chunk][re, im] of ncol x 16 B in the same 512 B blocks
+        const float sc = a.lscale[k];
+        uint32_t hr[4], hi[4];
+        bool out_of_range = false;
+#pragma unroll
+        for (int d = 0; d < 8; d += 2) {
+          const float x0 = __fmul_rn(ax[d], sc), x1 = __fmul_rn(ax[d + 1], sc);
+          const float y0 = __fmul_rn(ay[d], sc), y1 = __fmul_rn(ay[d + 1], sc);
+          out_of_range |= fmaxf(fmaxf(fabsf(x0), fabsf(x1)), fmaxf(fabsf(y0), fabsf(y1))) > 65000.f;
+          const __half2 pr = __floats2half2_rn(x0, x1), pi = __floats2half2_rn(y0, y1);
+          hr[d / 2] = *reinterpret_cast<const uint32_t*>(&pr);
+          hi[d / 2] = *reinterpret_cast<const uint32_t*>(&pi);
+        }
+        if (out_of_range && a.range_err) atomicOr(a.range_err, 1);
+        uint4* dst = reinterpret_cast<uint4*>(a.lop) +
+                     (((size_t)(r >> 3) * a.K + k) * 8 * (NCOL / 4) + (c >> 2)) * 32 + (r & 7) * 4 + (c & 3);
+        constexpr size_t RS = (size_t)(NCOL / 4) * 32;  // one row
+        dst[(jc * 2 + 0) * RS] = make_uint4(hr[0], hr[1], hr[2], hr[3]);
+        dst[(jc * 2 + 1) * RS] = make_uint4(hi[0], hi[1], hi[2], hi[3]);
       } else {
         // split-BF16 rows of the 8 planes (zero outside [xlo, xhi] by construction): per
         // (rotation, channel) 16 rows [hi, lo][chunk][re, im] of ncol x 16 B, the tensor-core x

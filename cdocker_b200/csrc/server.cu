@@ -267,7 +267,8 @@ void worker_loop(cdk_server* s) {
   a.keys = reinterpret_cast<unsigned long long*>(sc);
   sc += up((size_t)W * sizeof(unsigned long long));
   a.A = reinterpret_cast<float2*>(sc);
-  const size_t rows = s->streamed ? (size_t)((W + 7) & ~7) * stream_lop_bytes_per_rotation(n, K) : 0;
+  const bool f16 = s->streamed && s->v.form == CDK_FORM_FP16X2;
+  const size_t rows = s->streamed ? (size_t)((W + 7) & ~7) * stream_lop_bytes_per_rotation(n, K, f16) : 0;
   unsigned char* lop_base = reinterpret_cast<unsigned char*>(sc);
   sc += up(std::max((size_t)W * K * Lmax * ncol * sizeof(float2), rows));
   a.B = reinterpret_cast<float2*>(sc);
@@ -276,6 +277,9 @@ void worker_loop(cdk_server* s) {
   a.err_count = reinterpret_cast<int*>(s->d_misc);
   a.fault = reinterpret_cast<int*>(s->d_misc + 1);
   a.work = reinterpret_cast<unsigned long long*>(s->d_misc + 2);
+  // split-FP16 form: a value outside the FP16 range invalidates the wave like a box overflow
+  a.range_err = a.err_count;
+  for (int k = 0; k < KMAX; ++k) a.lscale[k] = s->v.lscale[k];
   a.col_tile = s->v.col_tile_opt > 0 ? s->v.col_tile_opt : pick_col_tile(n, K);
   a.kyof = s->v.kyof;
   a.minE = nullptr;
@@ -339,9 +343,10 @@ void worker_loop(cdk_server* s) {
     a.rots = w.d_rots;
     const bool tc_wave = s->streamed && stream_supported(n, lb) && direct_planes(a);
     a.lop = tc_wave ? lop_base : nullptr;
+    a.f16 = (tc_wave && f16) ? 1 : 0;
     launch_prep(a, s->stream);
     launch_spread_yz(a, s->stream);
-    if (tc_wave) launch_xpass_stream(a, s->v.top, s->v.tc_variant == 3, s->stream);
+    if (tc_wave) launch_xpass_stream(a, s->v.top, !f16 && s->v.tc_variant == 3, s->stream);
     else launch_xpass(a, s->stream);
     launch_yz_inv_argmin(a, s->stream);
     launch_finalize_server(a, reinterpret_cast<float*>(s->arena),
@@ -398,7 +403,8 @@ int cdk_server_create(cdk_ctx* ctx, const cdk_server_opts* opts, cdk_server** ou
   // precision-form contexts run the streamed tensor-core x pass on waves it applies to (ligand
   // box <= 32 planes at n = 64, ligands <= 96 atoms on the direct plane path); other waves and
   // FP32 contexts run the FP32 radix x pass
-  s->streamed = s->v.form == CDK_FORM_BF16X3 && (s->v.tc_variant == 0 || s->v.tc_variant == 3) &&
+  s->streamed = ((s->v.form == CDK_FORM_BF16X3 && (s->v.tc_variant == 0 || s->v.tc_variant == 3)) ||
+                 s->v.form == CDK_FORM_FP16X2) &&
                 s->v.kyof != nullptr &&
                 stream_supported(n, std::min(s->opts.max_box, 32));
   if (s->streamed) {
@@ -410,7 +416,9 @@ int cdk_server_create(cdk_ctx* ctx, const cdk_server_opts* opts, cdk_server** ou
     ctx_view(ctx, &s->v);
   }
   const size_t planes = (size_t)W * K * s->opts.max_box * ncol * sizeof(float2);
-  const size_t rows = s->streamed ? (size_t)((W + 7) & ~7) * stream_lop_bytes_per_rotation(n, K) : 0;
+  const size_t rows = s->streamed ? (size_t)((W + 7) & ~7) *
+                                        stream_lop_bytes_per_rotation(n, K, s->v.form == CDK_FORM_FP16X2)
+                                  : 0;
   const size_t scratch = up((size_t)W * s->opts.max_atoms * sizeof(float4)) +
                          up((size_t)W * sizeof(RotRec)) + up((size_t)W * 8) +
                          up(std::max(planes, rows)) + up((size_t)W * n * ncol * sizeof(float2));

@@ -27,6 +27,7 @@
 // the producers wait on before refilling the buffer. All 8 warps run the epilogue. Every wait
 // is bounded; a wait that gives up sets the fault flag, lets issued copies land, frees TMEM.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -42,7 +43,7 @@ constexpr int XS_R = 128;
 constexpr int XS_M = 128;
 constexpr int XS_THREADS = 256;
 constexpr int XS_PRODUCERS = 128;  // warps 0-3: one producer thread per rotation of the tile
-constexpr int XS_MAXSTAGES = 12;
+constexpr int XS_MAXSTAGES = 16;
 constexpr int XS_JMAX = 4;                          // x chunks of 8 planes (Lb <= 32)
 constexpr uint32_t XS_GROUP = (XS_M / 8) * 128;     // 2048 B: one K group of 8 for 128 rows
 constexpr uint32_t XS_STEP = 2 * XS_GROUP;          // 4096 B: one K step of 16
@@ -51,12 +52,19 @@ constexpr uint32_t XS_SSTAGE = 4 * XS_STEP;         // 16 KB ring stage: T hi, T
 // Two shapes: 2 columns per CTA with a 96 KB ring (two CTAs per SM, so one CTA's epilogue and
 // MMA-issue gaps overlap the other's work) when stages are at most 48 KB (ligand box <= 24
 // planes), else 4 columns with a 192 KB ring (one CTA per SM).
-template <int COLS>
+template <int COLS, bool F16 = false>
 struct XsShape {
   static constexpr uint32_t RING = COLS == 2 ? 96 * 1024 : 192 * 1024;
   static constexpr uint32_t TMEM_COLS = COLS * XS_R;
   static constexpr size_t SMEM = (size_t)RING + 1024;
   static constexpr int MIN_BLOCKS = COLS == 2 ? 2 : 1;
+  // ring stage: T hi, T lo, L hi, L lo (split-BF16 form) or T hi, T lo, L (split-FP16 form)
+  static constexpr int LPARTS = F16 ? 1 : 2;
+  static constexpr uint32_t SSTAGE = (2 + LPARTS) * XS_STEP;
+  // kind::f16 instruction descriptor: FP32 accumulation, A and B BF16 (type 1) or FP16 (type 0),
+  // both K-major, N = 128 rotations, M = 128 operator rows
+  static constexpr uint32_t IDESC = (1u << 4) | (F16 ? 0u : (1u << 7) | (1u << 10)) |
+                                    ((uint32_t)(XS_R >> 3) << 17) | ((uint32_t)(XS_M >> 4) << 24);
 };
 constexpr uint32_t XS_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(XS_R >> 3) << 17) |
                               ((uint32_t)(XS_M >> 4) << 24);
@@ -103,13 +111,14 @@ __device__ __forceinline__ bool elect_one() {
   return pred != 0;
 }
 
-__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc,
+                                         uint32_t idesc = XS_IDESC) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
       :
-      : "r"(d_tmem), "l"(a), "l"(b), "r"(XS_IDESC), "r"(acc)
+      : "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc)
       : "memory");
 }
 
@@ -144,9 +153,24 @@ __device__ __forceinline__ void bf16_split(float v, uint16_t& hi, uint16_t& lo) 
 //   odd rows m = 2x' + 1:   part 0: Im P~(x + x'),  part 1: -Re P~(x + x')  (imaginary output)
 // with x = 8 j + d; real and imaginary outputs of x' land in adjacent TMEM lanes. One thread
 // per 16-byte row.
+// Split-FP16 form: the same image of hi/lo FP16 parts of P~ 2^-sigma_k (ChanScale.s[k] =
+// 2^-sigma_k); the ligand rows carry 2^sigma_k, so P~ fits the FP16 range.
+struct ChanScale {
+  float s[KMAX];
+};
+
+__device__ __forceinline__ void f16_split(float v, uint16_t& hi, uint16_t& lo) {
+  const __half h = __float2half_rn(v);
+  const __half l = __float2half_rn(__fsub_rn(v, __half2float(h)));
+  hi = __half_as_ushort(h);
+  lo = __half_as_ushort(l);
+}
+
+template <bool F16>
 __global__ void __launch_bounds__(256) k_top_build(int K, const float2* __restrict__ pt,
-                                                   uint4* __restrict__ top) {
+                                                   uint4* __restrict__ top, ChanScale sc) {
   const int c = blockIdx.x, k = blockIdx.y;
+  const float scale = F16 ? sc.s[k] : 1.f;
   __shared__ float2 s_p[XS_N];
   if (threadIdx.x < XS_N) s_p[threadIdx.x] = pt[((size_t)c * K + k) * XS_N + threadIdx.x];
   __syncthreads();
@@ -165,7 +189,8 @@ __global__ void __launch_bounds__(256) k_top_build(int K, const float2* __restri
       const float2 v = s_p[(8 * j + d + xp) & (XS_N - 1)];
       const float val = imrow ? (part ? -v.x : v.y) : (part ? v.y : v.x);
       uint16_t h, l;
-      bf16_split(val, h, l);
+      if (F16) f16_split(__fmul_rn(val, scale), h, l);
+      else bf16_split(val, h, l);
       e[d] = hl ? l : h;
     }
     dst[row] = make_uint4((uint32_t)e[0] | ((uint32_t)e[1] << 16), (uint32_t)e[2] | ((uint32_t)e[3] << 16),
@@ -173,10 +198,11 @@ __global__ void __launch_bounds__(256) k_top_build(int K, const float2* __restri
   }
 }
 
-template <int COLS>
-__global__ void __launch_bounds__(XS_THREADS, XsShape<COLS>::MIN_BLOCKS)
+template <int COLS, bool F16>
+__global__ void __launch_bounds__(XS_THREADS, XsShape<COLS, F16>::MIN_BLOCKS)
     k_xpass_stream64(WaveArgs a, const unsigned char* __restrict__ top, int jc) {
-  using Shape = XsShape<COLS>;
+  using Shape = XsShape<COLS, F16>;
+  constexpr uint32_t XS_SSTAGE = Shape::SSTAGE;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // keep the ring 1024-aligned whatever the dynamic base
   unsigned char* ring = reinterpret_cast<unsigned char*>(
@@ -288,9 +314,11 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS>::MIN_BLOCKS)
     const int rr = tid;
     const uint32_t row_s = (uint32_t)(rr >> 3) * 128 + (uint32_t)(rr & 7) * 16;
     const int rg = r0 + (rr < nr ? rr : 0);
-    // 16 B units: (((r/8 * K + k) * 16 + row) * ncol/4 + c/4) * 32 + (r%8) * 4 + c%4
+    // 16 B units: (((r/8 * K + k) * ROWS + row) * ncol/4 + c/4) * 32 + (r%8) * 4 + c%4 with
+    // ROWS = 16 split-BF16 rows [hi, lo][chunk][re, im] or 8 FP16 rows [chunk][re, im]
     constexpr size_t RS = (size_t)(XS_NCOL / 4) * 32;
-    const size_t rot_rows = (size_t)(rg >> 3) * K * 16 * RS + (size_t)(c0 >> 2) * 32 + (rg & 7) * 4 + (c0 & 3);
+    constexpr int ROWS = 8 * Shape::LPARTS;
+    const size_t rot_rows = (size_t)(rg >> 3) * K * ROWS * RS + (size_t)(c0 >> 2) * 32 + (rg & 7) * 4 + (c0 & 3);
     // this rotation's chunk ranges, 8 bits per channel
     uint64_t jr_lo = 0, jr_hi = 0;
     for (int k = 0; k < K; ++k) {
@@ -306,7 +334,7 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS>::MIN_BLOCKS)
       const unsigned int jr = (unsigned int)(((k < 8 ? jr_lo : jr_hi) >> (8 * (k & 7))) & 255);
       const int jl = (int)(jr & 15), jh = (int)(jr >> 4);
       for (int c = 0; c < COLS && s >= 0; ++c) {
-        const uint4* src0 = reinterpret_cast<const uint4*>(lop) + rot_rows + (size_t)k * 16 * RS + c;
+        const uint4* src0 = reinterpret_cast<const uint4*>(lop) + rot_rows + (size_t)k * ROWS * RS + c;
         const unsigned char* tsrc = top + ((size_t)(c0 + c) * K + k) * 2 * XS_TILE;
         for (int j = jlo; j <= jhi; ++j, ++s) {
           if (s >= nb) {
@@ -332,7 +360,7 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS>::MIN_BLOCKS)
           }
           const bool have = jl <= j && j <= jh;
 #pragma unroll
-          for (int hl = 0; hl < 2; ++hl)
+          for (int hl = 0; hl < Shape::LPARTS; ++hl)
 #pragma unroll
             for (int part = 0; part < 2; ++part) {
               const uint4* src = src0 + (size_t)((hl * 4 + j) * 2 + part) * RS;
@@ -370,9 +398,10 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS>::MIN_BLOCKS)
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const uint64_t ah = desc0 + (uint64_t)b * (XS_SSTAGE >> 4);
           const uint32_t acc = (ai > 0 || j > jlo) ? 1u : 0u;  // first product of column c
-          if (elect_one()) umma_f16(d, ah, ah + 2 * TU, acc);
-          if (elect_one()) umma_f16(d, ah, ah + 3 * TU, 1u);
-          if (elect_one()) umma_f16(d, ah + TU, ah + 2 * TU, 1u);
+          // T_hi L_hi, T_hi L_lo, T_lo L_hi (split BF16) or T_hi L, T_lo L (split FP16)
+          if (elect_one()) umma_f16(d, ah, ah + 2 * TU, acc, Shape::IDESC);
+          if (!F16 && elect_one()) umma_f16(d, ah, ah + 3 * TU, 1u, Shape::IDESC);
+          if (elect_one()) umma_f16(d, ah + TU, ah + 2 * TU, 1u, Shape::IDESC);
           if (elect_one())
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                              smem_u32(&s_empty[b]))
@@ -779,28 +808,32 @@ size_t stream_top_bytes(int n, int K) {
   return n == 64 ? (size_t)XS_NCOL * K * 2 * XS_TILE : 0;
 }
 
-size_t stream_lop_bytes_per_rotation(int n, int K) {
-  return n == 64 ? (size_t)K * XS_NCOL * 256 : 0;
+size_t stream_lop_bytes_per_rotation(int n, int K, bool f16) {
+  return n == 64 ? (size_t)K * XS_NCOL * (f16 ? 128 : 256) : 0;
 }
 
-cudaError_t launch_top_build(int n, int K, const float2* pt, void* top, cudaStream_t s) {
-  if (n != 64) return cudaErrorInvalidValue;
-  k_top_build<<<dim3(XS_NCOL, K), 256, 0, s>>>(K, pt, reinterpret_cast<uint4*>(top));
+cudaError_t launch_top_build(int n, int K, const float2* pt, void* top, const float* f16_scale,
+                             cudaStream_t s) {
+  if (n != 64 || K > KMAX) return cudaErrorInvalidValue;
+  ChanScale sc{};
+  for (int k = 0; k < K; ++k) sc.s[k] = f16_scale ? f16_scale[k] : 1.f;
+  if (f16_scale) k_top_build<true><<<dim3(XS_NCOL, K), 256, 0, s>>>(K, pt, reinterpret_cast<uint4*>(top), sc);
+  else k_top_build<false><<<dim3(XS_NCOL, K), 256, 0, s>>>(K, pt, reinterpret_cast<uint4*>(top), sc);
   return cudaGetLastError();
 }
 
-template <int COLS>
+template <int COLS, bool F16>
 cudaError_t launch_stream_cols(const WaveArgs& a, const void* top, int jc, cudaStream_t s) {
-  using Shape = XsShape<COLS>;
-  cudaError_t e = cudaFuncSetAttribute(k_xpass_stream64<COLS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  using Shape = XsShape<COLS, F16>;
+  cudaError_t e = cudaFuncSetAttribute(k_xpass_stream64<COLS, F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)Shape::SMEM);
   if (e != cudaSuccess) return e;
   // all of the unified L1 as shared memory, so two 2-column CTAs fit one SM
-  e = cudaFuncSetAttribute(k_xpass_stream64<COLS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+  e = cudaFuncSetAttribute(k_xpass_stream64<COLS, F16>, cudaFuncAttributePreferredSharedMemoryCarveout,
                            (int)cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
   dim3 grid((a.nrot + XS_R - 1) / XS_R, XS_NCOL / COLS);
-  k_xpass_stream64<COLS><<<grid, XS_THREADS, Shape::SMEM, s>>>(a, reinterpret_cast<const unsigned char*>(top), jc);
+  k_xpass_stream64<COLS, F16><<<grid, XS_THREADS, Shape::SMEM, s>>>(a, reinterpret_cast<const unsigned char*>(top), jc);
   return cudaGetLastError();
 }
 
@@ -808,15 +841,18 @@ cudaError_t launch_xpass_stream(const WaveArgs& a, const void* top, bool tmem_li
   if (!stream_supported(a.n, a.Lb) || !a.lop || !top) return cudaErrorInvalidValue;
   const int jc = (a.Lb + 7) / 8;  // K-steps a valid rotation can touch
   if (tmem_ligand) {
+    if (a.f16) return cudaErrorInvalidValue;  // the tensor-memory ligand kernel is split-BF16 only
     cudaError_t e = cudaFuncSetAttribute(k_xpass_tmema64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TA_SMEM);
     if (e != cudaSuccess) return e;
     dim3 grid((a.nrot + TA_R - 1) / TA_R, XS_NCOL / TA_COLS);
     k_xpass_tmema64<<<grid, TA_THREADS, TA_SMEM, s>>>(a, reinterpret_cast<const unsigned char*>(top), jc);
     return cudaGetLastError();
   }
-  // two stages of 4 tiles of jc steps must fit the 96 KB ring of the 2-column shape
-  if (2 * 4 * (uint32_t)jc * XS_STEP <= XsShape<2>::RING) return launch_stream_cols<2>(a, top, jc, s);
-  return launch_stream_cols<4>(a, top, jc, s);
+  // ligand boxes of up to 24 planes: 2 columns, two CTAs per SM; larger boxes: 4 columns
+  if (a.f16) {
+    return jc <= 3 ? launch_stream_cols<2, true>(a, top, jc, s) : launch_stream_cols<4, true>(a, top, jc, s);
+  }
+  return jc <= 3 ? launch_stream_cols<2, false>(a, top, jc, s) : launch_stream_cols<4, false>(a, top, jc, s);
 }
 
 }  // namespace cdk

@@ -38,6 +38,10 @@ extern "C" {
 
 #define CDK_FORM_FP32 0   /* FP32 radix FFT passes (the plain form) */
 #define CDK_FORM_BF16X3 1 /* split-BF16 (hi*hi + hi*lo + lo*hi) DFT contractions, FP32 acc. */
+#define CDK_FORM_FP16X2 2 /* split-FP16 operator x FP16 ligand rows (two products), per-channel
+                             power-of-two scaling, FP32 acc.: about 1e-4 relative error; half the
+                             ligand bytes and two thirds of the MMAs of BF16X3 (n = 64; other sizes
+                             and ligands above 96 atoms run the BF16X3 kernels) */
 
 typedef struct cdk_ctx cdk_ctx;
 
@@ -254,8 +258,9 @@ int cdk_server_destroy(cdk_server* s);
  * [14] x-pass rotations per CTA, [15] graph state (0 off, 1 shape seen, 2 replaying),
  * [16] x-pass kind (0 FP32 radix, 1 mma.sync, 2 tcgen05 with in-kernel operand builds,
  * 3 tcgen05 with streamed operands in shared memory, 4 tcgen05 with streamed operands, the
- * ligand in tensor memory), [17] tensor-core K-steps the streamed x pass issued (one
- * step = three 128 x 128 x 16 BF16 MMAs, 1,572,864 flops). */
+ * ligand in tensor memory, 5 tcgen05 with streamed operands, split-FP16 form),
+ * [17] tensor-core K-steps the streamed x pass issued (one step = three 128 x 128 x 16 BF16
+ * MMAs, 1,572,864 flops; in the split-FP16 form two FP16 MMAs, 1,048,576 flops). */
 #define CDK_NSTATS 18
 int cdk_ctx_stats(cdk_ctx* ctx, double* out, int n);
 

@@ -1,11 +1,11 @@
-"""Precision form (CDK_FORM_BF16X3): the x pass as a split-BF16 circulant contraction on the
-tensor cores. Bar: per-rotation minimum energy within 1e-3 relative of the FP64 oracle (floor
-1 kcal/mol), best translation identical except at near-ties of that tolerance; FP64 re-score
-of the top poses."""
+"""Tensor-core forms (CDK_FORM_BF16X3, CDK_FORM_FP16X2): the x pass as a split-BF16 (or
+split-FP16 operator x FP16 ligand) circulant contraction on the tensor cores. Bar: per-rotation
+minimum energy within 1e-3 relative of the FP64 oracle (floor 1 kcal/mol), best translation
+identical except at near-ties of that tolerance; FP64 re-score of the top poses."""
 import numpy as np
 import pytest
 
-from cdocker_b200 import CDK_FORM_BF16X3, Receptor, synth
+from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP16X2, Receptor, synth
 from cdocker_b200.poses import rescore_top
 from oracle import oracle as O
 from tests.parity import check_search, rel_err
@@ -15,11 +15,16 @@ pytestmark = pytest.mark.gpu
 TOL_TC = 1e-3
 
 
+@pytest.mark.parametrize("form", [CDK_FORM_BF16X3, CDK_FORM_FP16X2])
 @pytest.mark.parametrize("name,nconf,nq", [("c0_32", 1, 500), ("c1_64", 4, 25), ("c4_128", 1, 4)])
-def test_tc_form_vs_fp64(name, nconf, nq, grids_cache):
+def test_tc_form_vs_fp64(name, nconf, nq, form, grids_cache):
+    """Both tensor-core forms against FP64; the split-FP16 form runs its own kernel at 64^3 and
+    the split-BF16 kernels at the other grid sizes."""
     w = synth.make_workload(name, seed=5, n_conf=nconf, n_q=nq, grids_cache=grids_cache)
-    with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3) as rec:
+    with Receptor(w.grids, w.spacing, form=form) as rec:
         minE, idx = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+        if form == CDK_FORM_FP16X2 and name == "c1_64":
+            assert rec.stats()["xpass_kind"] == "tcgen05_streamed_fp16"
     _, ridx, r64 = O.search_direct(w.grids, w.spacing, w.coor, w.charge, w.eps, w.slot, w.quats,
                                    prec=1)
     qq = w.quats.reshape(-1, 4)
@@ -91,17 +96,19 @@ def test_streamed_falls_back_for_large_ligands(grids_cache):
     assert rel_err(etc, e32).max() <= TOL_TC
 
 
+@pytest.mark.parametrize("form", [CDK_FORM_BF16X3, CDK_FORM_FP16X2])
 @pytest.mark.parametrize("n_atoms,radius,n_q,wave", [(6, 1.2, 40, 0),    # box 7 planes: one K-step, 6-stage ring
                                                      (60, 6.8, 12, 0),   # box 30 planes: 4-column shape
                                                      (40, 4.7, 37, 29)])  # ragged waves (not multiples of 8)
-def test_streamed_shapes_vs_fp64(grids_cache, n_atoms, radius, n_q, wave):
-    """The streamed tensor-core x pass across ligand boxes (1 to 4 K-steps, both CTA shapes)
-    and ragged waves, against the FP64 oracle."""
+def test_streamed_shapes_vs_fp64(grids_cache, n_atoms, radius, n_q, wave, form):
+    """The streamed tensor-core x pass of both forms across ligand boxes (1 to 4 K-steps, both
+    CTA shapes) and ragged waves, against the FP64 oracle."""
     w = synth.make_workload("c1_64", seed=31, n_conf=1, n_q=n_q, grids_cache=grids_cache,
                             n_atoms=n_atoms, ligand_radius=radius)
-    with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3, wave_rotations=wave) as rec:
+    with Receptor(w.grids, w.spacing, form=form, wave_rotations=wave) as rec:
         minE, idx = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
-        assert rec.stats()["xpass_kind"] == "tcgen05_streamed"
+        assert rec.stats()["xpass_kind"] == ("tcgen05_streamed_fp16" if form == CDK_FORM_FP16X2
+                                             else "tcgen05_streamed")
     _, ridx, r64 = O.search_direct(w.grids, w.spacing, w.coor, w.charge, w.eps, w.slot, w.quats,
                                    prec=1)
     qq = w.quats.reshape(-1, 4)

@@ -3,7 +3,7 @@ request searched alone, admission waits for arena space, and latency stats are r
 import numpy as np
 import pytest
 
-from cdocker_b200 import CDK_FORM_BF16X3, Receptor, synth
+from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP16X2, Receptor, synth
 from cdocker_b200.serving import Server, make_requests, poisson_arrivals, run_load
 
 pytestmark = pytest.mark.gpu
@@ -65,12 +65,13 @@ def test_poisson_load_reports_latency(receptor_c1):
     assert res["requests"] == len(arr) and res["p99_ms"] >= res["p50_ms"] > 0
 
 
-def test_precision_form_server_runs_tensor_core_waves(grids_cache):
+@pytest.mark.parametrize("form", [CDK_FORM_BF16X3, CDK_FORM_FP16X2])
+def test_precision_form_server_runs_tensor_core_waves(grids_cache, form):
     """A precision-form receptor serves its waves on the streamed tensor-core x pass; each
     rotation's column of the contraction is independent of the other rotations in its tile, so
     shared waves reproduce each request searched alone."""
     w = synth.make_workload("c1_64", seed=4, n_conf=1, n_q=1, grids_cache=grids_cache)
-    with Receptor(w.all_grids, w.spacing, max_atoms=96, form=CDK_FORM_BF16X3) as rec:
+    with Receptor(w.all_grids, w.spacing, max_atoms=96, form=form) as rec:
         reqs = _reqs(w, 4, seed=21, atoms=(10, 60), confs=(2, 6), rots=(100, 400))
         alone = [rec.search(r["coor"], r["charge"], r["eps"], _full_slot(r), r["quats"])
                  for r in reqs]
