@@ -294,6 +294,8 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   a.f16 = f16 ? 1 : 0;
   for (int k = 0; k < KMAX; ++k) a.lscale[k] = c->lscale[k];
   a.range_err = reinterpret_cast<int*>(c->d_misc + 4);
+  // the shared-memory streamed x pass writes B in plane groups (whole sectors per store)
+  a.bgroup = (streamed && !tmem_ligand) ? stream_bgroup() : 1;
   a.col_tile = c->opts.col_tile > 0 ? c->opts.col_tile : pick_col_tile(n, K);
   a.kyof = (c->opts.reserved[1] == 0) ? c->d_kyof : nullptr;  // reserved[1] = 1: FFT planes
   a.chunk = 0;

@@ -66,7 +66,9 @@ struct WaveArgs {
   float4* rot_xyz;           // [nrot][max_atoms]
   RotRec* rec;               // [nrot]
   float2* A;                 // [nrot][K][Lb][ncol]
-  float2* B;                 // [nrot][n][ncol]
+  float2* B;                 // [nrot][n][ncol], or with bgroup G > 1 [nrot][n/G][ncol/2][G][2]:
+                             // the x planes grouped by G, 16 B (two columns) per (plane, pair)
+  int bgroup;                // 0 or 1: plain B layout; 2, 4, 8: grouped (streamed x pass only)
   unsigned long long* keys;  // [nrot]
   const float2* phat;        // [n][K][ncol] (kx position-major)
   const float2* tw;          // [n]
@@ -130,6 +132,8 @@ cudaError_t launch_xpass_umma(const WaveArgs& a, const float2* pt, cudaStream_t 
 bool stream_supported(int n, int Lb);
 size_t stream_top_bytes(int n, int K);
 size_t stream_lop_bytes_per_rotation(int n, int K, bool f16);
+// plane group of the B layout the shared-memory streamed x pass writes (CDK_B_GROUP overrides)
+int stream_bgroup();
 // f16_scale: nullptr = the split-BF16 image; else the split-FP16 image of P~ * f16_scale[k]
 cudaError_t launch_top_build(int n, int K, const float2* pt, void* top, const float* f16_scale,
                              cudaStream_t s);

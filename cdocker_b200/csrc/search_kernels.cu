@@ -626,9 +626,12 @@ __global__ void __launch_bounds__(256) k_yz_inv_argmin(WaveArgs a) {
   if (x >= Wx) return;
   const int tid = threadIdx.x, nthr = blockDim.x;
   for (int i = tid; i < N; i += nthr) tw[i] = a.tw[i];
-  const float4* src = reinterpret_cast<const float4*>(a.B + ((size_t)r * N + x) * NCOL);
+  // plane x: NCOL / 2 column pairs, 16 B each, contiguous (plain layout) or every G-th of the
+  // plane group (grouped layout, G planes per 16 B x column-pair block)
+  const int G = a.bgroup > 1 ? a.bgroup : 1;
+  const float4* src = reinterpret_cast<const float4*>(a.B + ((size_t)r * N + (x - x % G)) * NCOL) + x % G;
   float4* dst = reinterpret_cast<float4*>(O);
-  for (int i = tid; i < NCOL / 2; i += nthr) dst[i] = src[i];
+  for (int i = tid; i < NCOL / 2; i += nthr) dst[i] = src[(size_t)i * G];
   __syncthreads();
   fft_lines<N, true>(O, NZH, 1, NZH, tw, tid, nthr);  // y: positions -> natural rows
   const int npairs = (Wy + 1) / 2;

@@ -344,6 +344,7 @@ void worker_loop(cdk_server* s) {
     const bool tc_wave = s->streamed && stream_supported(n, lb) && direct_planes(a);
     a.lop = tc_wave ? lop_base : nullptr;
     a.f16 = (tc_wave && f16) ? 1 : 0;
+    a.bgroup = (tc_wave && (f16 || s->v.tc_variant != 3)) ? stream_bgroup() : 1;
     launch_prep(a, s->stream);
     launch_spread_yz(a, s->stream);
     if (tc_wave) launch_xpass_stream(a, s->v.top, !f16 && s->v.tc_variant == 3, s->stream);

@@ -31,6 +31,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstdlib>
+
 #include "cdk_internal.h"
 
 namespace cdk {
@@ -442,6 +444,10 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS, F16>::MIN_BLOCKS)
     const int q = warp & 3;
     const int xp = 16 * q + (lane >> 1);
     const bool writer = (lane & 1) == 0;
+    // grouped B layout: the 16 writer lanes' planes x' = 16 q .. 16 q + 15 fill G-plane blocks
+    // of 16 G contiguous bytes per column pair (whole sectors for G >= 2)
+    const int G = a.bgroup > 1 ? a.bgroup : 1;
+    const size_t xoff = (size_t)(xp - xp % G) * (XS_NCOL / 2) + xp % G;  // in float4 units
     for (int jr = 2 * (warp >> 2); jr < 2 * (warp >> 2) + 2; ++jr) {
       float v[COLS][32];
 #pragma unroll
@@ -454,9 +460,9 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS, F16>::MIN_BLOCKS)
         for (int c = 0; c < COLS; ++c) im[c] = __shfl_down_sync(0xffffffffu, v[c][t], 1);
         const int rr = 32 * jr + t;
         if (writer && rr < nr && xp < s_W[rr]) {
-          float4* dst = reinterpret_cast<float4*>(a.B + ((size_t)(r0 + rr) * XS_N + xp) * XS_NCOL + c0);
+          float4* dst = reinterpret_cast<float4*>(a.B + (size_t)(r0 + rr) * XS_N * XS_NCOL) + xoff + (size_t)(c0 / 2) * G;
 #pragma unroll
-          for (int c = 0; c < COLS; c += 2) dst[c / 2] = make_float4(v[c][t], im[c], v[c + 1][t], im[c + 1]);
+          for (int c = 0; c < COLS; c += 2) dst[(size_t)(c / 2) * G] = make_float4(v[c][t], im[c], v[c + 1][t], im[c + 1]);
         }
       }
     }
@@ -801,6 +807,15 @@ __global__ void __launch_bounds__(TA_THREADS, 1) k_xpass_tmema64(WaveArgs a, con
 }
 
 }  // namespace
+
+int stream_bgroup() {
+  static const int g = [] {
+    const char* e = std::getenv("CDK_B_GROUP");
+    const int v = e ? std::atoi(e) : 2;
+    return (v == 1 || v == 2 || v == 4 || v == 8) ? v : 2;
+  }();
+  return g;
+}
 
 bool stream_supported(int n, int Lb) { return n == 64 && Lb >= 1 && Lb <= 8 * XS_JMAX; }
 
