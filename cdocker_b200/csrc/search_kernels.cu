@@ -143,6 +143,16 @@ __global__ void __launch_bounds__(128) k_prep(WaveArgs a) {
     for (int d = 0; d < 3; ++d) atomicMax(&s_ext[warp][d], ci[d] + 2);
   }
   __syncwarp();
+  if (a.f16 && lane < a.K && a.range_err) {
+    // split-FP16 form: |A(x, ky, kz)| <= sum over the channel's atoms of |s_a| (x weights and
+    // |Fy|, |Fz| are at most 1), so the scaled ligand rows fit FP16 when this bound does
+    float bound = 0.f;
+    for (int i = 0; i < nA; ++i) {
+      if (lane == elec) bound += fabsf(prm[i].charge);
+      else if (prm[i].slot == lane) bound += fabsf(prm[i].w_vdw);
+    }
+    if (bound * a.lscale[lane] > 60000.f) atomicOr(a.range_err, 1);
+  }
   RotRec* rec = a.rec + r;
   if (lane < KMAX) {
     const bool used = lane < a.K && s_hi[warp][lane] >= 0;
@@ -287,7 +297,7 @@ __global__ void __launch_bounds__(256) k_spread_yz(WaveArgs a) {
 constexpr int kDirectMaxAtoms = 96;
 
 template <int N, bool LOP>
-__global__ void __launch_bounds__(256) k_spread_yz_direct(WaveArgs a, const int* __restrict__ kyof,
+__global__ void __launch_bounds__(256, 5) k_spread_yz_direct(WaveArgs a, const int* __restrict__ kyof,
                                                            int cap) {
   constexpr int NZH = N / 2 + 1;
   constexpr int NCOL = N * NZH;
@@ -296,7 +306,9 @@ __global__ void __launch_bounds__(256) k_spread_yz_direct(WaveArgs a, const int*
   int4* s_apk = reinterpret_cast<int4*>(tw + N);                // [cap] (x cell, w(xi), w(xi+1), -)
   float2* Fy = reinterpret_cast<float2*>(s_apk + cap);          // [cap][N] by ky position
   float2* Fz = Fy + (size_t)cap * N;                            // [cap][NZH]
-  int* s_atom = reinterpret_cast<int*>(Fz + (size_t)cap * NZH);  // [cap]
+  int2* s_yz = reinterpret_cast<int2*>(Fz + (size_t)cap * NZH);  // [cap] y and z cells
+  float2* s_rr = reinterpret_cast<float2*>(s_yz + cap);           // [cap] y and z ratios
+  int* s_atom = reinterpret_cast<int*>(s_rr + cap);               // [cap]
   __shared__ int s_cnt;
   __shared__ uint32_t s_cm[N / 8][3];  // per 8-plane chunk: the channel atoms touching it (bit j)
   const int k = blockIdx.x, r = blockIdx.y;
@@ -327,30 +339,34 @@ __global__ void __launch_bounds__(256) k_spread_yz_direct(WaveArgs a, const int*
   }
   __syncthreads();
   const int na = s_cnt;
-  // factor tables and per-atom x cell / weights
-  for (int i = tid; i < na * (N + NZH); i += nthr) {
-    const int j = i / (N + NZH), f = i - j * (N + NZH);
+  // per atom: cells, ratios and x weights (FillLigandGrid's double arithmetic, once per atom)
+  for (int j = tid; j < na; j += nthr) {
     const int at = s_atom[j];
     const float4 p = a.rot_xyz[(size_t)r * a.max_atoms + at];
+    const int xi = cell_of(p.x, mn0, h), yi = cell_of(p.y, mn1, h), zi = cell_of(p.z, mn2, h);
+    const double xr = ratio_of(p.x, mn0, h, xi);
+    const double sc = elec ? (double)prm[at].charge : (double)prm[at].w_vdw;
+    s_apk[j] = make_int4(xi, __float_as_int((float)(sc * (1.0 - xr))),
+                         __float_as_int((xi + 1 < N) ? (float)(sc * xr) : 0.f), 0);
+    s_yz[j] = make_int2(yi, zi);
+    s_rr[j] = make_float2((float)ratio_of(p.y, mn1, h, yi), (float)ratio_of(p.z, mn2, h, zi));
+  }
+  __syncthreads();
+  // factor tables
+  for (int i = tid; i < na * (N + NZH); i += nthr) {
+    const int j = i / (N + NZH), f = i - j * (N + NZH);
     if (f < N) {
-      const int yi = cell_of(p.y, mn1, h);
-      const float ry = (float)ratio_of(p.y, mn1, h, yi);
+      const int yi = s_yz[j].x;
+      const float ry = s_rr[j].x;
       const int ky = kyof[f];  // natural frequency of position f
       const float2 w0 = tw[(yi * ky) % N], w1 = tw[((yi + 1) * ky) % N];
       Fy[(size_t)j * N + f] = make_float2((1.f - ry) * w0.x + ry * w1.x, (1.f - ry) * w0.y + ry * w1.y);
     } else {
       const int kz = f - N;
-      const int zi = cell_of(p.z, mn2, h);
-      const float rz = (float)ratio_of(p.z, mn2, h, zi);
+      const int zi = s_yz[j].y;
+      const float rz = s_rr[j].y;
       const float2 w0 = tw[(zi * kz) % N], w1 = tw[((zi + 1) * kz) % N];
       Fz[(size_t)j * NZH + kz] = make_float2((1.f - rz) * w0.x + rz * w1.x, (1.f - rz) * w0.y + rz * w1.y);
-    }
-    if (f == 0) {
-      const int xi = cell_of(p.x, mn0, h);
-      const double xr = ratio_of(p.x, mn0, h, xi);
-      const double sc = elec ? (double)prm[at].charge : (double)prm[at].w_vdw;
-      s_apk[j] = make_int4(xi, __float_as_int((float)(sc * (1.0 - xr))),
-                           __float_as_int((xi + 1 < N) ? (float)(sc * xr) : 0.f), 0);
     }
   }
   __syncthreads();
@@ -426,19 +442,17 @@ __global__ void __launch_bounds__(256) k_spread_yz_direct(WaveArgs a, const int*
       } else if (a.f16) {
         // split-FP16 form: FP16 rows of the 8 planes times 2^sigma_k (exact): per (rotation,
         // channel) 8 rows [chunk][re, im] of ncol x 16 B in the same 512 B blocks
+        // (k_prep has checked that the scaled planes stay inside the FP16 range)
         const float sc = a.lscale[k];
         uint32_t hr[4], hi[4];
-        bool out_of_range = false;
 #pragma unroll
         for (int d = 0; d < 8; d += 2) {
           const float x0 = __fmul_rn(ax[d], sc), x1 = __fmul_rn(ax[d + 1], sc);
           const float y0 = __fmul_rn(ay[d], sc), y1 = __fmul_rn(ay[d + 1], sc);
-          out_of_range |= fmaxf(fmaxf(fabsf(x0), fabsf(x1)), fmaxf(fabsf(y0), fabsf(y1))) > 65000.f;
           const __half2 pr = __floats2half2_rn(x0, x1), pi = __floats2half2_rn(y0, y1);
           hr[d / 2] = *reinterpret_cast<const uint32_t*>(&pr);
           hi[d / 2] = *reinterpret_cast<const uint32_t*>(&pi);
         }
-        if (out_of_range && a.range_err) atomicOr(a.range_err, 1);
         uint4* dst = reinterpret_cast<uint4*>(a.lop) +
                      (((size_t)(r >> 3) * a.K + k) * 8 * (NCOL / 4) + (c >> 2)) * 32 + (r & 7) * 4 + (c & 3);
         constexpr size_t RS = (size_t)(NCOL / 4) * 32;  // one row
@@ -788,7 +802,7 @@ constexpr size_t plane_smem() {
 template <int N>
 size_t direct_smem(int cap) {
   return sizeof(float2) * (N + (size_t)cap * (N + N / 2 + 1)) + sizeof(int4) * cap +
-         sizeof(int) * cap;
+         sizeof(int) * cap + (sizeof(int2) + sizeof(float2)) * cap;
 }
 
 template <int N>
