@@ -294,10 +294,63 @@ __global__ void __launch_bounds__(256) k_spread_yz(WaveArgs a) {
 // CTA per (rotation, channel): per-atom factor tables in shared memory, then every touched
 // plane's n*(n/2+1) outputs, written in the (ky position, kz) order of the FFT path.
 // Atoms are visited in ascending order for every plane: deterministic.
+// One column's 8-plane chunk jc of the plane kernel, written as FP32 planes (A), FP16 rows or
+// split-BF16 rows (lop).
+template <int N, bool LOP>
+__device__ __forceinline__ void plane_chunk_write(const WaveArgs& a, int r, int k, int jc, int x0,
+                                                  int xlo, int xhi, int c, const float* ax,
+                                                  const float* ay) {
+  constexpr int NCOL = N * (N / 2 + 1);
+  if constexpr (!LOP) {
+#pragma unroll
+    for (int d = 0; d < 8; ++d) {
+      const int x = x0 + d;
+      if (x >= xlo && x <= xhi) a.A[(((size_t)r * a.K + k) * a.Lb + x) * NCOL + c] = make_float2(ax[d], ay[d]);
+    }
+  } else if (a.f16) {
+    // split-FP16 form: FP16 rows of the 8 planes times 2^sigma_k (exact): per (rotation,
+    // channel) 8 rows [chunk][re, im] of ncol x 16 B in the same 512 B blocks
+    // (k_prep has checked that the scaled planes stay inside the FP16 range)
+    const float sc = a.lscale[k];
+    uint32_t hr[4], hi[4];
+#pragma unroll
+    for (int d = 0; d < 8; d += 2) {
+      const float xa = __fmul_rn(ax[d], sc), xb = __fmul_rn(ax[d + 1], sc);
+      const float ya = __fmul_rn(ay[d], sc), yb = __fmul_rn(ay[d + 1], sc);
+      const __half2 pr = __floats2half2_rn(xa, xb), pi = __floats2half2_rn(ya, yb);
+      hr[d / 2] = *reinterpret_cast<const uint32_t*>(&pr);
+      hi[d / 2] = *reinterpret_cast<const uint32_t*>(&pi);
+    }
+    uint4* dst = reinterpret_cast<uint4*>(a.lop) +
+                 (((size_t)(r >> 3) * a.K + k) * 8 * (NCOL / 4) + (c >> 2)) * 32 + (r & 7) * 4 + (c & 3);
+    constexpr size_t RS = (size_t)(NCOL / 4) * 32;  // one row
+    dst[(jc * 2 + 0) * RS] = make_uint4(hr[0], hr[1], hr[2], hr[3]);
+    dst[(jc * 2 + 1) * RS] = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+  } else {
+    // split-BF16 rows of the 8 planes (zero outside [xlo, xhi] by construction): per
+    // (rotation, channel) 16 rows [hi, lo][chunk][re, im] of ncol x 16 B, the tensor-core x
+    // pass's K order, in 512 B blocks of (8 rotations x 4 columns) x 16 B
+    uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+    for (int d = 0; d < 8; d += 2) {
+      split_bf16x2(ax[d], ax[d + 1], rh[d / 2], rl[d / 2]);
+      split_bf16x2(ay[d], ay[d + 1], ih[d / 2], il[d / 2]);
+    }
+    uint4* dst = reinterpret_cast<uint4*>(a.lop) +
+                 (((size_t)(r >> 3) * a.K + k) * 16 * (NCOL / 4) + (c >> 2)) * 32 + (r & 7) * 4 + (c & 3);
+    constexpr size_t RS = (size_t)(NCOL / 4) * 32;  // one row
+    dst[((0 * 4 + jc) * 2 + 0) * RS] = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+    dst[((0 * 4 + jc) * 2 + 1) * RS] = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+    dst[((1 * 4 + jc) * 2 + 0) * RS] = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+    dst[((1 * 4 + jc) * 2 + 1) * RS] = make_uint4(il[0], il[1], il[2], il[3]);
+  }
+}
+
+constexpr int kPlaneColsPerThread = 2;  // columns per thread in the plane kernel
 constexpr int kDirectMaxAtoms = 96;
 
 template <int N, bool LOP>
-__global__ void __launch_bounds__(256, 5) k_spread_yz_direct(WaveArgs a, const int* __restrict__ kyof,
+__global__ void __launch_bounds__(256, kPlaneColsPerThread == 1 ? 5 : 4) k_spread_yz_direct(WaveArgs a, const int* __restrict__ kyof,
                                                            int cap) {
   constexpr int NZH = N / 2 + 1;
   constexpr int NCOL = N * NZH;
@@ -387,36 +440,57 @@ __global__ void __launch_bounds__(256, 5) k_spread_yz_direct(WaveArgs a, const i
   // Chunks of 8 planes: every thread owns columns, accumulates a chunk's planes in registers
   // and visits the atoms touching the chunk in ascending order; an atom adds to planes xi and
   // xi + 1, whose offsets in the chunk are the same for the whole CTA (a uniform switch).
-  for (int c = tid; c < NCOL; c += nthr) {
-    const int kyp = c / NZH, kz = c - kyp * NZH;
+  // CPT columns per thread (c, c + NCOL / CPT, ...): the atom visit (list walk, weights, the
+  // offset switch) is shared by the columns, each column keeping its own accumulation order.
+  constexpr int CPT = kPlaneColsPerThread;
+  static_assert(NCOL % CPT == 0, "column split");
+  for (int cb = tid; cb < NCOL / CPT; cb += nthr) {
+    int kyp[CPT], kz[CPT];
+#pragma unroll
+    for (int u = 0; u < CPT; ++u) {
+      const int c = cb + u * (NCOL / CPT);
+      kyp[u] = c / NZH;
+      kz[u] = c - kyp[u] * NZH;
+    }
     for (int q = 0; q < njc; ++q) {
       const int jc = jc0 + q;
       const int x0 = 8 * jc;
-      float ax[8], ay[8];
+      float ax[CPT][8], ay[CPT][8];
 #pragma unroll
-      for (int d = 0; d < 8; ++d) ax[d] = ay[d] = 0.f;
+      for (int u = 0; u < CPT; ++u)
+#pragma unroll
+        for (int d = 0; d < 8; ++d) ax[u][d] = ay[u][d] = 0.f;
       // only the atoms touching this chunk, in ascending order (the same for the whole CTA)
       for (int wd = 0; wd < 3; ++wd) {
         for (unsigned int mask = s_cm[q][wd]; mask; mask &= mask - 1) {
           const int j = 32 * wd + __ffs(mask) - 1;
           const int4 pk = s_apk[j];
           const int o = pk.x - x0;
-          const float2 fy = Fy[(size_t)j * N + kyp];
-          const float2 fz = Fz[(size_t)j * NZH + kz];
-          const float gx = fy.x * fz.x - fy.y * fz.y;
-          const float gy = fy.x * fz.y + fy.y * fz.x;
+          float gx[CPT], gy[CPT];
+#pragma unroll
+          for (int u = 0; u < CPT; ++u) {
+            const float2 fy = Fy[(size_t)j * N + kyp[u]];
+            const float2 fz = Fz[(size_t)j * NZH + kz[u]];
+            gx[u] = fy.x * fz.x - fy.y * fz.y;
+            gy[u] = fy.x * fz.y + fy.y * fz.x;
+          }
           const float w0 = __int_as_float(pk.y), w1 = __int_as_float(pk.z);
           switch (o) {
-#define CDK_PLANE_PAIR(D)                    \
-  case D:                                    \
-    ax[D] += w0 * gx;                        \
-    ay[D] += w0 * gy;                        \
-    ax[D + 1] += w1 * gx;                    \
-    ay[D + 1] += w1 * gy;                    \
+#define CDK_PLANE_PAIR(D)                                                  \
+  case D:                                                                  \
+    _Pragma("unroll") for (int u = 0; u < CPT; ++u) {                      \
+      ax[u][D] += w0 * gx[u];                                              \
+      ay[u][D] += w0 * gy[u];                                              \
+      ax[u][D + 1] += w1 * gx[u];                                          \
+      ay[u][D + 1] += w1 * gy[u];                                          \
+    }                                                                      \
     break;
             case -1:
-              ax[0] += w1 * gx;
-              ay[0] += w1 * gy;
+#pragma unroll
+              for (int u = 0; u < CPT; ++u) {
+                ax[u][0] += w1 * gx[u];
+                ay[u][0] += w1 * gy[u];
+              }
               break;
             CDK_PLANE_PAIR(0)
             CDK_PLANE_PAIR(1)
@@ -427,55 +501,18 @@ __global__ void __launch_bounds__(256, 5) k_spread_yz_direct(WaveArgs a, const i
             CDK_PLANE_PAIR(6)
 #undef CDK_PLANE_PAIR
             default:  // o == 7: plane xi + 1 is the next chunk's
-              ax[7] += w0 * gx;
-              ay[7] += w0 * gy;
+#pragma unroll
+              for (int u = 0; u < CPT; ++u) {
+                ax[u][7] += w0 * gx[u];
+                ay[u][7] += w0 * gy[u];
+              }
               break;
           }
         }
       }
-      if constexpr (!LOP) {
 #pragma unroll
-        for (int d = 0; d < 8; ++d) {
-          const int x = x0 + d;
-          if (x >= xlo && x <= xhi) a.A[(((size_t)r * a.K + k) * a.Lb + x) * NCOL + c] = make_float2(ax[d], ay[d]);
-        }
-      } else if (a.f16) {
-        // split-FP16 form: FP16 rows of the 8 planes times 2^sigma_k (exact): per (rotation,
-        // channel) 8 rows [chunk][re, im] of ncol x 16 B in the same 512 B blocks
-        // (k_prep has checked that the scaled planes stay inside the FP16 range)
-        const float sc = a.lscale[k];
-        uint32_t hr[4], hi[4];
-#pragma unroll
-        for (int d = 0; d < 8; d += 2) {
-          const float x0 = __fmul_rn(ax[d], sc), x1 = __fmul_rn(ax[d + 1], sc);
-          const float y0 = __fmul_rn(ay[d], sc), y1 = __fmul_rn(ay[d + 1], sc);
-          const __half2 pr = __floats2half2_rn(x0, x1), pi = __floats2half2_rn(y0, y1);
-          hr[d / 2] = *reinterpret_cast<const uint32_t*>(&pr);
-          hi[d / 2] = *reinterpret_cast<const uint32_t*>(&pi);
-        }
-        uint4* dst = reinterpret_cast<uint4*>(a.lop) +
-                     (((size_t)(r >> 3) * a.K + k) * 8 * (NCOL / 4) + (c >> 2)) * 32 + (r & 7) * 4 + (c & 3);
-        constexpr size_t RS = (size_t)(NCOL / 4) * 32;  // one row
-        dst[(jc * 2 + 0) * RS] = make_uint4(hr[0], hr[1], hr[2], hr[3]);
-        dst[(jc * 2 + 1) * RS] = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-      } else {
-        // split-BF16 rows of the 8 planes (zero outside [xlo, xhi] by construction): per
-        // (rotation, channel) 16 rows [hi, lo][chunk][re, im] of ncol x 16 B, the tensor-core x
-        // pass's K order, in 512 B blocks of (8 rotations x 4 columns) x 16 B
-        uint32_t rh[4], rl[4], ih[4], il[4];
-#pragma unroll
-        for (int d = 0; d < 8; d += 2) {
-          split_bf16x2(ax[d], ax[d + 1], rh[d / 2], rl[d / 2]);
-          split_bf16x2(ay[d], ay[d + 1], ih[d / 2], il[d / 2]);
-        }
-        uint4* dst = reinterpret_cast<uint4*>(a.lop) +
-                     (((size_t)(r >> 3) * a.K + k) * 16 * (NCOL / 4) + (c >> 2)) * 32 + (r & 7) * 4 + (c & 3);
-        constexpr size_t RS = (size_t)(NCOL / 4) * 32;  // one row
-        dst[((0 * 4 + jc) * 2 + 0) * RS] = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-        dst[((0 * 4 + jc) * 2 + 1) * RS] = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-        dst[((1 * 4 + jc) * 2 + 0) * RS] = make_uint4(rl[0], rl[1], rl[2], rl[3]);
-        dst[((1 * 4 + jc) * 2 + 1) * RS] = make_uint4(il[0], il[1], il[2], il[3]);
-      }
+      for (int u = 0; u < CPT; ++u)
+        plane_chunk_write<N, LOP>(a, r, k, jc, x0, xlo, xhi, cb + u * (NCOL / CPT), ax[u], ay[u]);
     }
   }
 }
