@@ -439,13 +439,15 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS, F16>::MIN_BLOCKS)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     // ---- epilogue, TMEM -> B without a shared-memory round trip: warp w reads lanes
     // 32 (w % 4) .. + 31 (x' = 16 (w % 4) .. + 15, real and imaginary in adjacent lanes) for
-    // the rotation chunks of its half; an even lane takes its odd neighbour's imaginary part
-    // and writes (re, im) of all the CTA's columns for one (rotation, x'): 16 or 32 B
+    // the rotation chunks of its half. Lanes 2j and 2j + 1 hold x' = 16 (w % 4) + j; per step
+    // of two rotations the even lane writes rotation t and the odd lane rotation t + 1, each
+    // taking its missing half from the other through one shuffle: (re, im) of all the CTA's
+    // columns for one (rotation, x'), 16 or 32 B
     const int q = warp & 3;
     const int xp = 16 * q + (lane >> 1);
-    const bool writer = (lane & 1) == 0;
-    // grouped B layout: the 16 writer lanes' planes x' = 16 q .. 16 q + 15 fill G-plane blocks
-    // of 16 G contiguous bytes per column pair (whole sectors for G >= 2)
+    const int odd = lane & 1;
+    // grouped B layout: the lanes' planes x' = 16 q .. 16 q + 15 fill G-plane blocks of 16 G
+    // contiguous bytes per column pair (whole sectors for G >= 2)
     const int G = a.bgroup > 1 ? a.bgroup : 1;
     const size_t xoff = (size_t)(xp - xp % G) * (XS_NCOL / 2) + xp % G;  // in float4 units
     for (int jr = 2 * (warp >> 2); jr < 2 * (warp >> 2) + 2; ++jr) {
@@ -454,15 +456,21 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS, F16>::MIN_BLOCKS)
       for (int c = 0; c < COLS; ++c)
         tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(c * XS_R + 32 * jr), v[c]);
 #pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        float im[COLS];
+      for (int t = 0; t < 32; t += 2) {
+        float re[COLS], im[COLS];
 #pragma unroll
-        for (int c = 0; c < COLS; ++c) im[c] = __shfl_down_sync(0xffffffffu, v[c][t], 1);
-        const int rr = 32 * jr + t;
-        if (writer && rr < nr && xp < s_W[rr]) {
+        for (int c = 0; c < COLS; ++c) {
+          // even lane: its re of rotation t, the odd lane's im of t; odd lane: the even lane's
+          // re of t + 1, its im of t + 1
+          const float other = __shfl_xor_sync(0xffffffffu, odd ? v[c][t] : v[c][t + 1], 1);
+          re[c] = odd ? other : v[c][t];
+          im[c] = odd ? v[c][t + 1] : other;
+        }
+        const int rr = 32 * jr + t + odd;
+        if (rr < nr && xp < s_W[rr]) {
           float4* dst = reinterpret_cast<float4*>(a.B + (size_t)(r0 + rr) * XS_N * XS_NCOL) + xoff + (size_t)(c0 / 2) * G;
 #pragma unroll
-          for (int c = 0; c < COLS; c += 2) dst[(size_t)(c / 2) * G] = make_float4(v[c][t], im[c], v[c + 1][t], im[c + 1]);
+          for (int c = 0; c < COLS; c += 2) dst[(size_t)(c / 2) * G] = make_float4(re[c], im[c], re[c + 1], im[c + 1]);
         }
       }
     }
