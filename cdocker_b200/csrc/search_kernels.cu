@@ -662,13 +662,18 @@ __global__ void __launch_bounds__(256, 2) k_xpass2(WaveArgs a, int rot_per_cta) 
 // ---------------------------------------------------------------------------------------
 // inverse (y,z) of one (rotation, x in window) plane + min / first argmin
 template <int N>
-__global__ void __launch_bounds__(256) k_yz_inv_argmin(WaveArgs a) {
+__global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveArgs a) {
   constexpr int NZH = N / 2 + 1;
   constexpr int NCOL = N * NZH;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* tw = reinterpret_cast<float2*>(smem_raw);
   float2* O = tw + N;
-  float2* P = O + N * NZH;
+  // n <= 64: the packed rows P overwrite O once O has been read (N/2 x (N+1) <= N x (N/2+1)
+  // entries), so a CTA holds one plane and the SM more CTAs; larger n keep P apart (the pack
+  // would hold too many values in registers)
+  constexpr bool ALIAS = N <= 64;
+  float2* P = ALIAS ? O : O + N * NZH;
+  static_assert((N / 2) * (N + 1) <= N * NZH, "packed rows fit the plane buffer");
   __shared__ unsigned long long s_best[8];
   const int x = blockIdx.x, r = blockIdx.y;
   const RotRec* rec = a.rec + r;
@@ -686,21 +691,37 @@ __global__ void __launch_bounds__(256) k_yz_inv_argmin(WaveArgs a) {
   __syncthreads();
   fft_lines<N, true>(O, NZH, 1, NZH, tw, tid, nthr);  // y: positions -> natural rows
   const int npairs = (Wy + 1) / 2;
-  // pack rows (2p, 2p+1) as one complex line with Hermitian extension over z
-  for (int i = tid; i < npairs * N; i += nthr) {
-    const int p = i / N, k = i - p * N;
-    const float2* A = O + (2 * p) * NZH;
-    const float2* Bv = O + (2 * p + 1) * NZH;
-    float2 z;
-    if (k == 0 || k == N / 2) {
-      z = make_float2(A[k].x, Bv[k].x);
-    } else if (k < N / 2) {
-      z = make_float2(A[k].x - Bv[k].y, A[k].y + Bv[k].x);
-    } else {
-      const int m = N - k;
-      z = make_float2(A[m].x + Bv[m].y, -A[m].y + Bv[m].x);
+  // pack rows (2p, 2p+1) as one complex line with Hermitian extension over z: every thread
+  // reads its items into registers, then (after the barrier) writes them (over O when aliased)
+  constexpr int PK = ALIAS ? (N / 2 * N + 255) / 256 : 1;  // items per thread and round
+  for (int base = 0; base < (ALIAS ? 1 : (N / 2 * N + 255) / 256); ++base) {
+  float2 zv[PK];
+  int zi[PK];
+#pragma unroll
+  for (int t = 0; t < PK; ++t) {
+    const int i = tid + (base + t) * nthr;
+    zi[t] = -1;
+    if (i < npairs * N) {
+      const int p = i / N, k = i - p * N;
+      const float2* A = O + (2 * p) * NZH;
+      const float2* Bv = O + (2 * p + 1) * NZH;
+      float2 z;
+      if (k == 0 || k == N / 2) {
+        z = make_float2(A[k].x, Bv[k].x);
+      } else if (k < N / 2) {
+        z = make_float2(A[k].x - Bv[k].y, A[k].y + Bv[k].x);
+      } else {
+        const int m = N - k;
+        z = make_float2(A[m].x + Bv[m].y, -A[m].y + Bv[m].x);
+      }
+      zv[t] = z;
+      zi[t] = p * (N + 1) + fft_pos<N>(k);
     }
-    P[p * (N + 1) + fft_pos<N>(k)] = z;
+  }
+  if (ALIAS) __syncthreads();
+#pragma unroll
+  for (int t = 0; t < PK; ++t)
+    if (zi[t] >= 0) P[zi[t]] = zv[t];
   }
   __syncthreads();
   if constexpr (FFTPlan<N>::NS == 2) {
@@ -870,7 +891,8 @@ cudaError_t launch_spread_yz_t(const WaveArgs& a, cudaStream_t s) {
 
 template <int N>
 cudaError_t launch_yz_inv_t(const WaveArgs& a, cudaStream_t s) {
-  const size_t sm = plane_smem<N>();
+  // twiddles + one plane (n <= 64: the packed rows alias it) [+ the packed rows]
+  const size_t sm = sizeof(float2) * (N + N * (N / 2 + 1) + (N <= 64 ? 0 : (N / 2) * (N + 1)));
   cudaError_t e = cudaFuncSetAttribute(k_yz_inv_argmin<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   dim3 grid(N, a.nrot);
