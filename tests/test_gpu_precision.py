@@ -116,3 +116,22 @@ def test_streamed_shapes_vs_fp64(grids_cache, n_atoms, radius, n_q, wave, form):
                       lambda r: O.energy_map(w.grids, w.spacing, w.coor[0], w.charge, w.eps,
                                              w.slot, qq[r]), rel_tol=TOL_TC)
     assert st["max_rel"] <= TOL_TC
+
+
+def test_fp16_form_rejects_ligands_outside_its_range(grids_cache):
+    """The split-FP16 form bounds every scaled ligand value by the channel's sum of |charge| or
+    sqrt-epsilon (prep kernel); ligands whose bound leaves the FP16 range are refused with
+    CDK_ERR_UNSUPPORTED instead of overflowing, while the split-BF16 form searches them."""
+    from cdocker_b200 import _lib as L
+    w = synth.make_workload("c1_64", seed=14, n_conf=1, n_q=8, grids_cache=grids_cache)
+    big = (w.charge * 1e4).astype(np.float32)
+    with Receptor(w.grids, w.spacing, form=CDK_FORM_FP16X2) as rec:
+        with pytest.raises(L.CdkError) as e:
+            rec.search(w.coor, big, w.eps, w.slot, w.quats)
+        assert e.value.code == L.CDK_ERR_UNSUPPORTED
+        # the context stays usable for ligands inside the range
+        minE, _ = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+        assert np.all(np.isfinite(minE))
+    with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3) as rec:
+        minE, _ = rec.search(w.coor, big, w.eps, w.slot, w.quats)
+        assert np.all(np.isfinite(minE))
