@@ -308,16 +308,13 @@ __device__ __forceinline__ void plane_chunk_write(const WaveArgs& a, int r, int 
       if (x >= xlo && x <= xhi) a.A[(((size_t)r * a.K + k) * a.Lb + x) * NCOL + c] = make_float2(ax[d], ay[d]);
     }
   } else if (a.f16) {
-    // split-FP16 form: FP16 rows of the 8 planes times 2^sigma_k (exact): per (rotation,
-    // channel) 8 rows [chunk][re, im] of ncol x 16 B in the same 512 B blocks
-    // (k_prep has checked that the scaled planes stay inside the FP16 range)
-    const float sc = a.lscale[k];
+    // split-FP16 form: FP16 rows of the 8 planes times 2^sigma_k (already in the atoms' x
+    // weights): per (rotation, channel) 8 rows [chunk][re, im] of ncol x 16 B in the same 512 B
+    // blocks (k_prep has checked that the scaled planes stay inside the FP16 range)
     uint32_t hr[4], hi[4];
 #pragma unroll
     for (int d = 0; d < 8; d += 2) {
-      const float xa = __fmul_rn(ax[d], sc), xb = __fmul_rn(ax[d + 1], sc);
-      const float ya = __fmul_rn(ay[d], sc), yb = __fmul_rn(ay[d + 1], sc);
-      const __half2 pr = __floats2half2_rn(xa, xb), pi = __floats2half2_rn(ya, yb);
+      const __half2 pr = __floats2half2_rn(ax[d], ax[d + 1]), pi = __floats2half2_rn(ay[d], ay[d + 1]);
       hr[d / 2] = *reinterpret_cast<const uint32_t*>(&pr);
       hi[d / 2] = *reinterpret_cast<const uint32_t*>(&pi);
     }
@@ -392,6 +389,9 @@ __global__ void __launch_bounds__(256, kPlaneColsPerThread == 1 ? 5 : 4) k_sprea
   }
   __syncthreads();
   const int na = s_cnt;
+  // split-FP16 rows carry 2^sigma_k: a power of two, folded exactly into the x weights (every
+  // product and sum below then scales exactly, outside under- and overflow)
+  const float wsc = (LOP && a.f16) ? a.lscale[k] : 1.f;
   // per atom: cells, ratios and x weights (FillLigandGrid's double arithmetic, once per atom)
   for (int j = tid; j < na; j += nthr) {
     const int at = s_atom[j];
@@ -399,8 +399,8 @@ __global__ void __launch_bounds__(256, kPlaneColsPerThread == 1 ? 5 : 4) k_sprea
     const int xi = cell_of(p.x, mn0, h), yi = cell_of(p.y, mn1, h), zi = cell_of(p.z, mn2, h);
     const double xr = ratio_of(p.x, mn0, h, xi);
     const double sc = elec ? (double)prm[at].charge : (double)prm[at].w_vdw;
-    s_apk[j] = make_int4(xi, __float_as_int((float)(sc * (1.0 - xr))),
-                         __float_as_int((xi + 1 < N) ? (float)(sc * xr) : 0.f), 0);
+    s_apk[j] = make_int4(xi, __float_as_int(__fmul_rn((float)(sc * (1.0 - xr)), wsc)),
+                         __float_as_int((xi + 1 < N) ? __fmul_rn((float)(sc * xr), wsc) : 0.f), 0);
     s_yz[j] = make_int2(yi, zi);
     s_rr[j] = make_float2((float)ratio_of(p.y, mn1, h, yi), (float)ratio_of(p.z, mn2, h, zi));
   }
