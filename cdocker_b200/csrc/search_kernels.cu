@@ -691,17 +691,85 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
   __syncthreads();
   fft_lines<N, true>(O, NZH, 1, NZH, tw, tid, nthr);  // y: positions -> natural rows
   const int npairs = (Wy + 1) / 2;
-  // pack rows (2p, 2p+1) as one complex line with Hermitian extension over z: every thread
-  // reads its items into registers, then (after the barrier) writes them (over O when aliased)
-  constexpr int PK = ALIAS ? (N / 2 * N + 255) / 256 : 1;  // items per thread and round
-  for (int base = 0; base < (ALIAS ? 1 : (N / 2 * N + 255) / 256); ++base) {
-  float2 zv[PK];
-  int zi[PK];
+  const float inv = 1.0f / (float)((double)N * N * N);
+  unsigned long long best = ~0ull;
+  if constexpr (ALIAS) {
+    // Rows (2p, 2p+1) as one complex line Z_p(k) = Y(2p, k) + i Y(2p+1, k) with the Hermitian
+    // extension over z, inverse-transformed in two radix stages (N = R0 R1), one work item per
+    // thread and stage (line p fastest). The pack is folded into the first stage's loads and
+    // the window argmin into the last stage, so neither the packed input nor the energies take
+    // a trip through shared memory.
+    using PL = FFTPlan<N>;
+    constexpr int R0 = PL::R0, R1 = PL::R1;
+    static_assert(PL::NS == 2 && R0 * R1 == N && R1 % 2 == 0, "two-stage plan");
+    static_assert((N / 2) * R0 <= 256 && (N / 2) * R1 <= 256, "one item per thread of 256");
+    // item w -> (line w % npairs, block w / npairs); (w + 0.5) / npairs stays >= 1/64 away from
+    // an integer for w < 256, npairs <= 32, far above the float rounding of the product
+    const float rinv = npairs > 0 ? __frcp_rn((float)npairs) : 0.f;
+    // stage 1 (R1-point, no twiddles): block b reads natural frequencies k = b + R0 j, which sit
+    // at digit-reversed positions b R1 + j; k >= N/2 exactly when j >= R1/2
+    const bool has1 = tid < npairs * R0;
+    int l1 = 0, b1 = 0;
+    float2 v1[R1];
+    if (has1) {
+      b1 = (int)(((float)tid + 0.5f) * rinv);
+      l1 = tid - b1 * npairs;
+      const float2* A = O + (2 * l1) * NZH;
+      const float2* Bv = A + NZH;
 #pragma unroll
-  for (int t = 0; t < PK; ++t) {
-    const int i = tid + (base + t) * nthr;
-    zi[t] = -1;
-    if (i < npairs * N) {
+      for (int j = 0; j < R1; ++j) {
+        const int k = b1 + R0 * j;
+        if (j < R1 / 2) {
+          const float2 ak = A[k], bk = Bv[k];
+          v1[j] = make_float2(ak.x - bk.y, ak.y + bk.x);
+          if (j == 0 && b1 == 0) v1[j] = make_float2(ak.x, bk.x);  // k = 0
+        } else {
+          const int m = N - k;
+          const float2 am = A[m], bm = Bv[m];
+          v1[j] = make_float2(am.x + bm.y, -am.y + bm.x);
+          if (j == R1 / 2 && b1 == 0) v1[j] = make_float2(am.x, bm.x);  // k = N/2
+        }
+      }
+    }
+    __syncthreads();  // every read of the y-transformed rows is done: the lines overwrite them
+    if (has1) {
+      Radix<R1, +1>::run(v1);
+      float2* dst = P + l1 * (N + 1) + b1 * R1;
+#pragma unroll
+      for (int j = 0; j < R1; ++j) dst[j] = v1[j];
+    }
+    __syncthreads();
+    // stage 2 (R0-point, twiddles tw[np k]): item np yields z = np + R1 j; line l holds row 2l in
+    // its real part and row 2l + 1 in its imaginary part
+    if (tid < npairs * R1) {
+      const int np = (int)(((float)tid + 0.5f) * rinv);
+      const int l = tid - np * npairs;
+      const float2* src = P + l * (N + 1) + np;
+      float2 v[R0];
+#pragma unroll
+      for (int j = 0; j < R0; ++j) v[j] = src[j * R1];
+#pragma unroll
+      for (int k = 1; k < R0; ++k) v[k] = c_mulc(v[k], tw[np * k]);
+      Radix<R0, +1>::run(v);
+      const int y0 = 2 * l;
+      const bool row0 = y0 < Wy, row1 = y0 + 1 < Wy;
+      const unsigned int lin0 = (unsigned int)((x * N + y0) * N + np);
+#pragma unroll
+      for (int j = 0; j < R0; ++j) {
+        if (np + R1 * j < Wz) {
+          const unsigned long long k0 =
+              ((unsigned long long)order_key(v[j].x * inv) << 32) | (lin0 + (unsigned int)(R1 * j));
+          const unsigned long long k1 =
+              ((unsigned long long)order_key(v[j].y * inv) << 32) | (lin0 + (unsigned int)(N + R1 * j));
+          if (row0) best = k0 < best ? k0 : best;
+          if (row1) best = k1 < best ? k1 : best;
+        }
+      }
+    }
+  } else {
+    // pack rows (2p, 2p+1) as one complex line with Hermitian extension over z (into its own
+    // buffer), inverse-transform the lines, then take the window minimum from shared memory
+    for (int i = tid; i < npairs * N; i += nthr) {
       const int p = i / N, k = i - p * N;
       const float2* A = O + (2 * p) * NZH;
       const float2* Bv = O + (2 * p + 1) * NZH;
@@ -714,32 +782,24 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
         const int m = N - k;
         z = make_float2(A[m].x + Bv[m].y, -A[m].y + Bv[m].x);
       }
-      zv[t] = z;
-      zi[t] = p * (N + 1) + fft_pos<N>(k);
+      P[p * (N + 1) + fft_pos<N>(k)] = z;
     }
-  }
-  if (ALIAS) __syncthreads();
-#pragma unroll
-  for (int t = 0; t < PK; ++t)
-    if (zi[t] >= 0) P[zi[t]] = zv[t];
-  }
-  __syncthreads();
-  if constexpr (FFTPlan<N>::NS == 2) {
-    ifft_lines_slots<N, N / 2>(P, npairs, N + 1, 1, tw, tid, nthr);
-  } else {
-    fft_lines<N, true>(P, npairs, N + 1, 1, tw, tid, nthr);
-  }
-  const float inv = 1.0f / (float)((double)N * N * N);
-  unsigned long long best = ~0ull;
-  // window rows by warp, columns by lane (the key carries the index: order does not matter)
-  for (int y = tid >> 5; y < Wy; y += nthr >> 5) {
-    const float2* row = P + (y >> 1) * (N + 1);
-    for (int z = tid & 31; z < Wz; z += 32) {
-      const float2 v = row[z];
-      const float e = ((y & 1) ? v.y : v.x) * inv;
-      const unsigned int lin = (unsigned int)((x * N + y) * N + z);
-      const unsigned long long key = ((unsigned long long)order_key(e) << 32) | lin;
-      best = key < best ? key : best;
+    __syncthreads();
+    if constexpr (FFTPlan<N>::NS == 2) {
+      ifft_lines_slots<N, N / 2>(P, npairs, N + 1, 1, tw, tid, nthr);
+    } else {
+      fft_lines<N, true>(P, npairs, N + 1, 1, tw, tid, nthr);
+    }
+    // window rows by warp, columns by lane (the key carries the index: order does not matter)
+    for (int y = tid >> 5; y < Wy; y += nthr >> 5) {
+      const float2* row = P + (y >> 1) * (N + 1);
+      for (int z = tid & 31; z < Wz; z += 32) {
+        const float2 v = row[z];
+        const float e = ((y & 1) ? v.y : v.x) * inv;
+        const unsigned int lin = (unsigned int)((x * N + y) * N + z);
+        const unsigned long long key = ((unsigned long long)order_key(e) << 32) | lin;
+        best = key < best ? key : best;
+      }
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
