@@ -561,7 +561,8 @@ def run_ours(args, rank, world, local_rank):
             "metric": METRIC, "value": value, "unit": "rotations/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": H["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32" if head == "fp32" else "bf16x3 (f32 accumulate)",
+            "vs_baseline": None, "dtype": {"fp32": "f32", "bf16x3_tensor_core": "bf16x3 (f32 accumulate)",
+                      "fp16x2_tensor_core": "fp16x2 (f32 accumulate)"}.get(head, head),
             "data": "synthetic",
             "config": {"workload": "config 1: 64^3 grid at 0.5 A, K=9, 2,500-atom synthetic "
                                    "receptor, 40-atom ligand, 100 conformers x 1,000 "

@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(256, kPlaneColsPerThread == 1 ? 5 : 4) k_sprea
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* tw = reinterpret_cast<float2*>(smem_raw);            // [N]
   int4* s_apk = reinterpret_cast<int4*>(tw + N);                // [cap] (x cell, w(xi), w(xi+1), -)
-  float2* Fy = reinterpret_cast<float2*>(s_apk + cap);          // [cap][N] by ky position
+  float2* Fy = reinterpret_cast<float2*>(s_apk + cap);          // [cap][N/2][2]: ky positions p, p + N/2
   float2* Fz = Fy + (size_t)cap * N;                            // [cap][NZH]
   int2* s_yz = reinterpret_cast<int2*>(Fz + (size_t)cap * NZH);  // [cap] y and z cells
   float2* s_rr = reinterpret_cast<float2*>(s_yz + cap);           // [cap] y and z ratios
@@ -413,7 +413,10 @@ __global__ void __launch_bounds__(256, kPlaneColsPerThread == 1 ? 5 : 4) k_sprea
       const float ry = s_rr[j].x;
       const int ky = kyof[f];  // natural frequency of position f
       const float2 w0 = tw[(yi * ky) % N], w1 = tw[((yi + 1) * ky) % N];
-      Fy[(size_t)j * N + f] = make_float2((1.f - ry) * w0.x + ry * w1.x, (1.f - ry) * w0.y + ry * w1.y);
+      // positions f and f + N/2 side by side: a thread's two columns (ky positions p and
+      // p + N/2, the same kz) read both factors in one 16-byte load
+      Fy[(size_t)j * N + (f % (N / 2)) * 2 + f / (N / 2)] =
+          make_float2((1.f - ry) * w0.x + ry * w1.x, (1.f - ry) * w0.y + ry * w1.y);
     } else {
       const int kz = f - N;
       const int zi = s_yz[j].y;
@@ -444,6 +447,7 @@ __global__ void __launch_bounds__(256, kPlaneColsPerThread == 1 ? 5 : 4) k_sprea
   // offset switch) is shared by the columns, each column keeping its own accumulation order.
   constexpr int CPT = kPlaneColsPerThread;
   static_assert(NCOL % CPT == 0, "column split");
+  static_assert(CPT != 2 || (NCOL / 2) % NZH == 0, "paired columns share kz");
   for (int cb = tid; cb < NCOL / CPT; cb += nthr) {
     int kyp[CPT], kz[CPT];
 #pragma unroll
@@ -467,12 +471,22 @@ __global__ void __launch_bounds__(256, kPlaneColsPerThread == 1 ? 5 : 4) k_sprea
           const int4 pk = s_apk[j];
           const int o = pk.x - x0;
           float gx[CPT], gy[CPT];
+          if constexpr (CPT == 2) {
+            // columns c and c + NCOL/2: ky positions p and p + N/2, one kz
+            const float4 fy2 = *reinterpret_cast<const float4*>(Fy + (size_t)j * N + 2 * kyp[0]);
+            const float2 fz = Fz[(size_t)j * NZH + kz[0]];
+            gx[0] = fy2.x * fz.x - fy2.y * fz.y;
+            gy[0] = fy2.x * fz.y + fy2.y * fz.x;
+            gx[1] = fy2.z * fz.x - fy2.w * fz.y;
+            gy[1] = fy2.z * fz.y + fy2.w * fz.x;
+          } else {
 #pragma unroll
-          for (int u = 0; u < CPT; ++u) {
-            const float2 fy = Fy[(size_t)j * N + kyp[u]];
-            const float2 fz = Fz[(size_t)j * NZH + kz[u]];
-            gx[u] = fy.x * fz.x - fy.y * fz.y;
-            gy[u] = fy.x * fz.y + fy.y * fz.x;
+            for (int u = 0; u < CPT; ++u) {
+              const float2 fy = Fy[(size_t)j * N + (kyp[u] % (N / 2)) * 2 + kyp[u] / (N / 2)];
+              const float2 fz = Fz[(size_t)j * NZH + kz[u]];
+              gx[u] = fy.x * fz.x - fy.y * fz.y;
+              gy[u] = fy.x * fz.y + fy.y * fz.x;
+            }
           }
           const float w0 = __int_as_float(pk.y), w1 = __int_as_float(pk.z);
           switch (o) {
@@ -686,10 +700,36 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
   // plane group (grouped layout, G planes per 16 B x column-pair block)
   const int G = a.bgroup > 1 ? a.bgroup : 1;
   const float4* src = reinterpret_cast<const float4*>(a.B + ((size_t)r * N + (x - x % G)) * NCOL) + x % G;
-  float4* dst = reinterpret_cast<float4*>(O);
-  for (int i = tid; i < NCOL / 2; i += nthr) dst[i] = src[(size_t)i * G];
-  __syncthreads();
-  fft_lines<N, true>(O, NZH, 1, NZH, tw, tid, nthr);  // y: positions -> natural rows
+  if constexpr (ALIAS) {
+    // y: positions -> natural rows, the first (R1-point, twiddle-free) stage reading its rows
+    // straight from B: item (column l, block b) takes positions b R1 + j of column l, plane
+    // entry f = row * NZH + l, which is half f % 2 of column pair f / 2
+    using PL = FFTPlan<N>;
+    constexpr int R0 = PL::R0, R1 = PL::R1;
+    static_assert(PL::NS == 2 && StageM<N, 2>::value == 1, "two-stage plan");
+    const float2* src2 = reinterpret_cast<const float2*>(src);
+    for (int w = tid; w < NZH * R0; w += nthr) {
+      const int b = w / NZH, l = w - b * NZH;
+      float2 v[R1];
+#pragma unroll
+      for (int j = 0; j < R1; ++j) {
+        const int f = (b * R1 + j) * NZH + l;
+        v[j] = src2[(size_t)(f >> 1) * 2 * G + (f & 1)];
+      }
+      Radix<R1, +1>::run(v);
+      float2* p = O + l + b * R1 * NZH;
+#pragma unroll
+      for (int j = 0; j < R1; ++j) p[j * NZH] = v[j];
+    }
+    __syncthreads();
+    fft_stage<N, R0, StageM<N, 1>::value, true>(O, NZH, 1, NZH, tw, tid, nthr);
+    __syncthreads();
+  } else {
+    float4* dst = reinterpret_cast<float4*>(O);
+    for (int i = tid; i < NCOL / 2; i += nthr) dst[i] = src[(size_t)i * G];
+    __syncthreads();
+    fft_lines<N, true>(O, NZH, 1, NZH, tw, tid, nthr);  // y: positions -> natural rows
+  }
   const int npairs = (Wy + 1) / 2;
   const float inv = 1.0f / (float)((double)N * N * N);
   unsigned long long best = ~0ull;
