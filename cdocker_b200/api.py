@@ -134,7 +134,7 @@ class Receptor:
                  max_atoms: int = 256, col_tile: int = 0, form: int = L.CDK_FORM_FP32,
                  use_graphs: int = 0, profile: bool = False, fft_planes: bool = False,
                  autotune: bool = False, tc_mma_sync: bool = False, tc_build: bool = False,
-                 tc_tmem_ligand: bool = False):
+                 tc_tmem_ligand: bool = False, group_rotations: bool = True):
         g = _f32(grids)
         if g.ndim != 4:
             raise ValueError("grids must be [K, n, n, n]")
@@ -153,6 +153,7 @@ class Receptor:
         opts.reserved[1] = 1 if fft_planes else 0
         opts.reserved[2] = 1 if autotune else 0
         opts.reserved[3] = 1 if tc_mma_sync else (2 if tc_build else (3 if tc_tmem_ligand else 0))
+        opts.reserved[4] = 0 if group_rotations else 1
         h = C.c_void_p()
         L.check(lib.cdk_ctx_create(g.shape[1], g.shape[2], g.shape[3], self.spacing, self.K,
                                    _pf(g), C.byref(opts), C.byref(h)))

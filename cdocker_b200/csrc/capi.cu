@@ -114,6 +114,7 @@ struct cdk_ctx {
   Arena wave;                 // per-wave scratch
   Arena tables;               // per-search tables
   Arena io;                   // staging of host-buffer searches
+  Arena group;                // rotation grouping of the tensor-core x pass (sorted list, keys)
   unsigned int* d_misc = nullptr;  // [0] diameter bits, [1] flags, [2] error count, [3] fault,
                                    // [4] FP16 range flag
   unsigned long long* d_work = nullptr;  // [0] x planes spread (A), [1] window planes (B),
@@ -334,9 +335,25 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     a.chunk = c->tuned_chunk;
   }
   long launches = 1, waves = 0;
+  // tensor-core x pass: rotations reaching the same ligand-box chunks side by side (fewer
+  // K-steps per 128-rotation tile; reserved[4] = 1 keeps the given order)
+  const RotDesc* order = d_rots;
+  const int jc = (Lb + 7) / 8;
+  if (streamed && c->opts.reserved[4] == 0 && nRot > 128 && jc > 1) {
+    const size_t gb = group_rotations_bytes(nRot);
+    if (!grow(c->group, gb)) {
+      set_error("cudaMalloc of the rotation-grouping scratch failed (" + std::to_string(gb >> 20) + " MiB)");
+      return CDK_ERR_NOMEM;
+    }
+    RotDesc* sorted = nullptr;
+    CDK_CUDA(launch_group_rotations(d_rots, d_confs, d_coor, d_params, nRot, maxAtoms, K, c->spacing, jc,
+                                    c->group.base, &sorted, s));
+    order = sorted;
+    launches += 4;
+  }
   for (long r0 = 0; r0 < nRot; r0 += wave) {
     a.nrot = (int)std::min<long>(wave, nRot - r0);
-    a.rots = d_rots + r0;
+    a.rots = order + r0;
     cudaEvent_t* ev = prof ? &c->kev[(size_t)waves * (kLaunchesPerWave + 1)] : nullptr;
     if (prof) CDK_CUDA(cudaEventRecord(ev[0], s));
     CDK_CUDA(launch_prep(a, s));
@@ -722,6 +739,7 @@ int cdk_ctx_destroy(cdk_ctx* c) {
   cudaFree(c->wave.base);
   cudaFree(c->tables.base);
   cudaFree(c->io.base);
+  cudaFree(c->group.base);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);

@@ -93,6 +93,12 @@ struct WaveArgs {
 
 // Launchers (stream-ordered, no synchronisation). Return cudaError_t of the launch.
 cudaError_t launch_prep(const WaveArgs& a, cudaStream_t s);
+// rotation grouping for the tensor-core x pass (a stable counting sort of the rotation list on
+// which channels reach the ligand box's last 8-plane chunk); scratch of group_rotations_bytes
+size_t group_rotations_bytes(long nrot);
+cudaError_t launch_group_rotations(const RotDesc* rots, const ConfDesc* confs, const float* coords,
+                                   const AtomParam* params, long nrot, int max_atoms, int K, float h,
+                                   int jc, void* scratch, RotDesc** sorted, cudaStream_t s);
 cudaError_t launch_spread_yz(const WaveArgs& a, cudaStream_t s);
 cudaError_t launch_xpass(const WaveArgs& a, cudaStream_t s);
 cudaError_t launch_yz_inv_argmin(const WaveArgs& a, cudaStream_t s);

@@ -1040,6 +1040,122 @@ cudaError_t launch_receptor_t(int K, const float* grids, float2* scratch, float2
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------------------
+// Rotation grouping for the tensor-core x pass. A tile of 128 rotations loads and multiplies,
+// per channel, the union of the 8-plane chunks its rotations touch. Nearly every rotation
+// starts at chunk 0; what varies is whether a channel's atoms reach the box's last chunk. A
+// stable counting sort of the rotation list on one bit per channel (folded into kGroupBits)
+// puts rotations with the same pattern side by side, so tiles skip more chunks. Results do
+// not depend on the order: a chunk a rotation does not touch adds exact zeros to its sums, and
+// every output goes to its rotation's RotDesc::out.
+constexpr int kGroupBits = 10;
+constexpr int kGroupBuckets = 1 << kGroupBits;
+constexpr int kGroupSeg = 1024;  // rotations per histogram / scatter CTA
+
+// warp per rotation: the rotated x coordinates and their minimum exactly as k_prep computes
+// them, then the channels whose atoms reach chunk jc - 1
+__global__ void __launch_bounds__(128) k_group_key(const RotDesc* __restrict__ rots,
+                                                   const ConfDesc* __restrict__ confs,
+                                                   const float* __restrict__ coords,
+                                                   const AtomParam* __restrict__ params, long nrot,
+                                                   int max_atoms, int K, float h, int jc,
+                                                   unsigned short* __restrict__ key) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long r = (long)blockIdx.x * 4 + warp;
+  if (r >= nrot) return;
+  const RotDesc rd = rots[r];
+  const ConfDesc cd = confs[rd.conf];
+  const int nA = min(cd.n_atoms, max_atoms);
+  const float* xyz = coords + (size_t)cd.coord_off * 3;
+  const AtomParam* prm = params + cd.param_off;
+  float mn = INFINITY;
+  for (int i = lane; i < nA; i += 32) {
+    float p[3];
+    rotate_rn(rd.q, xyz[i * 3 + 0], xyz[i * 3 + 1], xyz[i * 3 + 2], p);
+    mn = fminf(mn, p[0]);
+  }
+  for (int o = 16; o > 0; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+  const int elec = K - 1;
+  unsigned int bits = 0;
+  for (int i = lane; i < nA; i += 32) {
+    float p[3];
+    rotate_rn(rd.q, xyz[i * 3 + 0], xyz[i * 3 + 1], xyz[i * 3 + 2], p);
+    if (min((cell_of(p[0], mn, h) + 1) >> 3, jc - 1) == jc - 1) {
+      const int sl = prm[i].slot;
+      if (sl >= 0 && sl < elec) bits |= 1u << (sl % kGroupBits);
+      bits |= 1u << (elec % kGroupBits);
+    }
+  }
+  bits = __reduce_or_sync(0xffffffffu, bits);
+  if (lane == 0) key[r] = (unsigned short)bits;
+}
+
+// per segment of kGroupSeg rotations, the count of each key: counts[key * nseg + segment]
+__global__ void __launch_bounds__(kGroupSeg) k_group_hist(const unsigned short* __restrict__ key,
+                                                          long nrot, int nseg, int* __restrict__ counts) {
+  __shared__ int hcount[kGroupBuckets];
+  for (int b = threadIdx.x; b < kGroupBuckets; b += blockDim.x) hcount[b] = 0;
+  __syncthreads();
+  const long r = (long)blockIdx.x * kGroupSeg + threadIdx.x;
+  if (r < nrot) atomicAdd(&hcount[key[r]], 1);
+  __syncthreads();
+  for (int b = threadIdx.x; b < kGroupBuckets; b += blockDim.x)
+    counts[(size_t)b * nseg + blockIdx.x] = hcount[b];
+}
+
+// exclusive scan of counts in place (key-major, so a key's segments follow one another)
+__global__ void __launch_bounds__(1024) k_group_scan(int* __restrict__ counts, long total) {
+  __shared__ long part[1024];
+  const int tid = threadIdx.x, T = blockDim.x;
+  const long per = (total + T - 1) / T;
+  const long lo = min(total, (long)tid * per), hi = min(total, lo + per);
+  long sum = 0;
+  for (long i = lo; i < hi; ++i) sum += counts[i];
+  part[tid] = sum;
+  __syncthreads();
+  for (int off = 1; off < T; off <<= 1) {
+    const long v = tid >= off ? part[tid - off] : 0;
+    __syncthreads();
+    part[tid] += v;
+    __syncthreads();
+  }
+  long run = part[tid] - sum;
+  for (long i = lo; i < hi; ++i) {
+    const int c = counts[i];
+    counts[i] = (int)run;
+    run += c;
+  }
+}
+
+// stable scatter: the warps of a segment place their rotations in warp order, lanes with the
+// same key by lane order
+__global__ void __launch_bounds__(kGroupSeg) k_group_scatter(const RotDesc* __restrict__ rots,
+                                                             const unsigned short* __restrict__ key,
+                                                             long nrot, int nseg,
+                                                             const int* __restrict__ counts,
+                                                             RotDesc* __restrict__ out) {
+  __shared__ int base[kGroupBuckets];
+  for (int b = threadIdx.x; b < kGroupBuckets; b += blockDim.x) base[b] = counts[(size_t)b * nseg + blockIdx.x];
+  const long r = (long)blockIdx.x * kGroupSeg + threadIdx.x;
+  const bool live = r < nrot;
+  const unsigned int kk = live ? key[r] : 0xffffffffu;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned int same = __match_any_sync(0xffffffffu, kk);
+  const int rank = __popc(same & ((1u << lane) - 1));
+  __syncthreads();
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+    if (warp == w) {
+      const int b0 = live ? base[kk] : 0;
+      __syncwarp();
+      if (live) {
+        out[b0 + rank] = rots[r];
+        if (rank == 0) base[kk] = b0 + __popc(same);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace
 
 int fft_position(int n, int k) {
@@ -1071,6 +1187,31 @@ int pick_col_tile(int n, int K) {
     case 128: return fn<128>(__VA_ARGS__);         \
     default: return cudaErrorInvalidValue;         \
   }
+
+size_t group_rotations_bytes(long nrot) {
+  const long nseg = (nrot + kGroupSeg - 1) / kGroupSeg;
+  return ((size_t)nrot * sizeof(RotDesc) + 255) / 256 * 256 + ((size_t)nrot * 2 + 255) / 256 * 256 +
+         (size_t)kGroupBuckets * nseg * sizeof(int);
+}
+
+cudaError_t launch_group_rotations(const RotDesc* rots, const ConfDesc* confs, const float* coords,
+                                   const AtomParam* params, long nrot, int max_atoms, int K, float h,
+                                   int jc, void* scratch, RotDesc** sorted, cudaStream_t s) {
+  if (nrot <= 0 || jc < 1 || K > KMAX) return cudaErrorInvalidValue;
+  const long nseg = (nrot + kGroupSeg - 1) / kGroupSeg;
+  char* p = static_cast<char*>(scratch);
+  RotDesc* out = reinterpret_cast<RotDesc*>(p);
+  p += ((size_t)nrot * sizeof(RotDesc) + 255) / 256 * 256;
+  unsigned short* key = reinterpret_cast<unsigned short*>(p);
+  p += ((size_t)nrot * 2 + 255) / 256 * 256;
+  int* counts = reinterpret_cast<int*>(p);
+  k_group_key<<<(unsigned)((nrot + 3) / 4), 128, 0, s>>>(rots, confs, coords, params, nrot, max_atoms, K, h, jc, key);
+  k_group_hist<<<(unsigned)nseg, kGroupSeg, 0, s>>>(key, nrot, (int)nseg, counts);
+  k_group_scan<<<1, 1024, 0, s>>>(counts, (long)kGroupBuckets * nseg);
+  k_group_scatter<<<(unsigned)nseg, kGroupSeg, 0, s>>>(rots, key, nrot, (int)nseg, counts, out);
+  *sorted = out;
+  return cudaGetLastError();
+}
 
 cudaError_t launch_prep(const WaveArgs& a, cudaStream_t s) {
   k_prep<<<(a.nrot + 3) / 4, 128, 0, s>>>(a);

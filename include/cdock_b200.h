@@ -59,7 +59,10 @@ typedef struct cdk_opts {
                           streamed operands in shared memory where it applies (n = 64, ligand
                           box <= 32 planes, ligands <= 96 atoms), else the next one;
                           1 = mma.sync; 2 = tcgen05 with operands built inside the kernel;
-                          3 = tcgen05 with streamed operands, the ligand in tensor memory */
+                          3 = tcgen05 with streamed operands, the ligand in tensor memory;
+                          [4] = 1: keep the rotations in the given order in the streamed
+                          tensor-core x pass (by default they are grouped by the ligand-box
+                          chunks their channels reach, which changes no result) */
 } cdk_opts;
 
 /* Library version string. */
