@@ -369,7 +369,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     if (prof) CDK_CUDA(cudaEventRecord(ev[4], s));
     CDK_CUDA(launch_finalize(a, s));
     if (prof) CDK_CUDA(cudaEventRecord(ev[5], s));
-    launches += kLaunchesPerWave;
+    launches += kLaunchesPerWave + (streamed && !tmem_ligand ? 1 : 0);  // + k_tile_plan
     ++waves;
   }
   c->kev_used = prof ? (int)waves : 0;

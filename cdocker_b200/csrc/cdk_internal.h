@@ -46,9 +46,14 @@ struct RotRec {
   int nA;           // atoms
   short xlo[KMAX];  // per channel: first and last x plane touched (xlo > xhi: empty)
   short xhi[KMAX];
+  // streamed tensor-core x pass, first record of each 128-rotation tile only: the tile's stage
+  // plan (4 bits per active channel: id, first and last K-step; then active channels and K-steps
+  // per column), written by k_tile_plan
+  unsigned long long tplan[4];
 };
 // the x ranges are read as 16-byte vectors
-static_assert(offsetof(RotRec, xlo) % 16 == 0 && sizeof(RotRec) % 16 == 0, "RotRec x-range alignment");
+static_assert(offsetof(RotRec, xlo) % 16 == 0 && offsetof(RotRec, tplan) % 16 == 0 && sizeof(RotRec) % 16 == 0,
+              "RotRec vector alignment");
 
 // Everything one wave of rotations needs on the device.
 struct WaveArgs {

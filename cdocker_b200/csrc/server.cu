@@ -359,7 +359,7 @@ void worker_loop(cdk_server* s) {
       s->waves++;
       s->tc_waves += tc_wave ? 1 : 0;
       s->rotations += nr;
-      s->launches += kLaunchesPerWave;
+      s->launches += kLaunchesPerWave + (tc_wave && (f16 || s->v.tc_variant != 3) ? 1 : 0);  // + k_tile_plan
     }
     cur ^= 1;
   }

@@ -200,6 +200,54 @@ __global__ void __launch_bounds__(256) k_top_build(int K, const float2* __restri
   }
 }
 
+// The stage plan of each 128-rotation tile, once per wave, into the tile's first RotRec: the
+// channels any rotation of the tile touches and, per channel, the union of the K-steps (8-plane
+// chunks, clamped to the jc chunks of the box) its rotations touch. Every column CTA of the tile
+// reads it with one load instead of rebuilding it.
+__global__ void __launch_bounds__(XS_R) k_tile_plan(WaveArgs a, int jc) {
+  __shared__ int s_jlo[KMAX], s_jhi[KMAX];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int r0 = blockIdx.x * XS_R;
+  const int nr = min(XS_R, a.nrot - r0);
+  const int K = a.K;
+  if (tid < KMAX) {
+    s_jlo[tid] = XS_JMAX;
+    s_jhi[tid] = -1;
+  }
+  __syncthreads();
+  const RotRec* rec = a.rec + r0 + min(tid, nr - 1);
+  const bool live = tid < nr && rec->valid;
+  for (int k = 0; k < K; ++k) {
+    const int lo = live ? rec->xlo[k] : 1, hi = live ? rec->xhi[k] : 0;
+    const int jl = lo <= hi ? min(lo >> 3, jc - 1) : 15;
+    const int jh = lo <= hi ? min(hi >> 3, jc - 1) : -1;
+    const int wl = __reduce_min_sync(0xffffffffu, jl);
+    const int wh = __reduce_max_sync(0xffffffffu, jh);
+    if (lane == 0) {
+      if (wl < 15) atomicMin(&s_jlo[k], wl);
+      if (wh >= 0) atomicMax(&s_jhi[k], wh);
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    uint64_t pk = 0, pl = 0, ph = 0;
+    unsigned int n = 0, steps = 0;
+    for (int k = 0; k < K; ++k)
+      if (s_jlo[k] <= s_jhi[k]) {
+        pk |= (uint64_t)k << (4 * n);
+        pl |= (uint64_t)s_jlo[k] << (4 * n);
+        ph |= (uint64_t)s_jhi[k] << (4 * n);
+        steps += (unsigned int)(s_jhi[k] - s_jlo[k] + 1);
+        ++n;
+      }
+    unsigned long long* tp = a.rec[r0].tplan;
+    tp[0] = pk;
+    tp[1] = pl;
+    tp[2] = ph;
+    tp[3] = ((unsigned long long)steps << 32) | n;
+  }
+}
+
 template <int COLS, bool F16>
 __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS, F16>::MIN_BLOCKS)
     k_xpass_stream64(WaveArgs a, const unsigned char* __restrict__ top, int jc) {
@@ -214,9 +262,6 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS, F16>::MIN_BLOCKS)
   __shared__ int s_fail;
   __shared__ int s_issued, s_consumed;
   __shared__ uint32_t s_tmem;
-  __shared__ unsigned char s_jr[KMAX][XS_R];  // per channel, rotation: jlo | jhi << 4 (empty: 0x0F)
-  __shared__ int s_jlo[KMAX], s_jhi[KMAX];
-  __shared__ int s_act[KMAX], s_nact;
   __shared__ int s_W[XS_R];
   const int K = a.K;
   // ring: stages of one K-step (operator hi, lo and ligand hi, lo tiles of 4 KB), as many as fit
@@ -239,18 +284,24 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS, F16>::MIN_BLOCKS)
                  "r"(Shape::TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  if (tid < KMAX) {
-    s_jlo[tid] = XS_JMAX;
-    s_jhi[tid] = -1;
-  }
   if (tid == 0) {
     s_fail = 0;
     s_issued = 0;
     s_consumed = 0;
   }
-  __syncthreads();
-  // per-rotation chunk ranges (one vector load of the record's x ranges), block union per
-  // channel by warp reductions
+  // the tile's stage plan (k_tile_plan), one 32-byte load; per active channel 4 bits each of
+  // channel id, first and last K-step, so the loops below read no shared memory but the
+  // mbarriers
+  const uint4* tpv = reinterpret_cast<const uint4*>(a.rec[r0].tplan);
+  const uint4 t01 = tpv[0], t23 = tpv[1];
+  const uint64_t pk = ((uint64_t)t01.y << 32) | t01.x;
+  const uint64_t pl = ((uint64_t)t01.w << 32) | t01.z;
+  const uint64_t ph = ((uint64_t)t23.y << 32) | t23.x;
+  const int nact = (int)t23.z;
+  const int NS = COLS * (int)t23.w;  // stages: one K-step of one (channel, column)
+  // this thread's rotation: its window (epilogue) and, for the producers, its chunk range per
+  // channel (8 bits each: jlo | jhi << 4, 0x0F when empty) from one vector load of the record
+  uint64_t jr_lo = 0, jr_hi = 0;
   if (tid < XS_R) {
     const RotRec* rec = a.rec + r0 + min(tid, nr - 1);
     const bool live = tid < nr && rec->valid;
@@ -264,52 +315,21 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS, F16>::MIN_BLOCKS)
     const short* hi16 = reinterpret_cast<const short*>(&v[2]);
 #pragma unroll
     for (int k = 0; k < KMAX; ++k) {
-      if (k < K) {
-        const int lo = live ? lo16[k] : 1, hi = live ? hi16[k] : 0;
-        int jl = 15, jh = -1;
-        if (lo <= hi) {
-          // valid rotations keep every plane inside the planned box; the clamp only keeps
-          // shared-memory offsets in range whatever the record says
-          jl = min(lo >> 3, jc - 1);
-          jh = min(hi >> 3, jc - 1);
-          s_jr[k][tid] = (unsigned char)(jl | (jh << 4));
-        } else {
-          s_jr[k][tid] = 0x0F;  // jlo 15 > jhi 0: no chunk
-        }
-        const int wl = __reduce_min_sync(0xffffffffu, jl);
-        const int wh = __reduce_max_sync(0xffffffffu, jh);
-        if (lane == 0) {
-          if (wl < 15) atomicMin(&s_jlo[k], wl);
-          if (wh >= 0) atomicMax(&s_jhi[k], wh);
-        }
-      }
+      uint64_t e = 0x0F;
+      const int lo = live ? lo16[k] : 1, hi = live ? hi16[k] : 0;
+      // valid rotations keep every plane inside the planned box; the clamp only keeps
+      // shared-memory offsets in range whatever the record says
+      if (k < K && lo <= hi) e = (uint64_t)(min(lo >> 3, jc - 1) | (min(hi >> 3, jc - 1) << 4));
+      if (k < 8) jr_lo |= e << (8 * k);
+      else jr_hi |= e << (8 * (k - 8));
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (tid == 0) {
-    int n = 0;
-    for (int k = 0; k < K; ++k)
-      if (s_jlo[k] <= s_jhi[k]) s_act[n++] = k;
-    s_nact = n;
-  }
-  __syncthreads();
   const uint32_t tmem = s_tmem;
   const unsigned char* lop = a.lop;
   const uint32_t ring_s = smem_u32(ring);
-  // stage parameters in registers (4 bits per active channel: id, first and last K-step), so
-  // the loops below read no shared memory but the mbarriers
-  uint64_t pk = 0, pl = 0, ph = 0;
-  int NS = 0;  // stages: one K-step of one (channel, column); order channel, column, step
-  for (int i = 0; i < s_nact; ++i) {
-    const int k = s_act[i];
-    pk |= (uint64_t)k << (4 * i);
-    pl |= (uint64_t)s_jlo[k] << (4 * i);
-    ph |= (uint64_t)s_jhi[k] << (4 * i);
-    NS += COLS * (s_jhi[k] - s_jlo[k] + 1);
-  }
-  const int nact = s_nact;
 
   if (tid < XS_PRODUCERS) {
     // ---- producers: thread = rotation rr of the tile; per stage its 4 split rows
@@ -321,13 +341,6 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS, F16>::MIN_BLOCKS)
     constexpr size_t RS = (size_t)(XS_NCOL / 4) * 32;
     constexpr int ROWS = 8 * Shape::LPARTS;
     const size_t rot_rows = (size_t)(rg >> 3) * K * ROWS * RS + (size_t)(c0 >> 2) * 32 + (rg & 7) * 4 + (c0 & 3);
-    // this rotation's chunk ranges, 8 bits per channel
-    uint64_t jr_lo = 0, jr_hi = 0;
-    for (int k = 0; k < K; ++k) {
-      const uint64_t v = s_jr[k][rr];
-      if (k < 8) jr_lo |= v << (8 * k);
-      else jr_hi |= v << (8 * (k - 8));
-    }
     int s = 0, b = 0;
     uint32_t round = 0;  // s / nb
     for (int ai = 0; ai < nact && s >= 0; ++ai) {
@@ -872,6 +885,7 @@ cudaError_t launch_xpass_stream(const WaveArgs& a, const void* top, bool tmem_li
     return cudaGetLastError();
   }
   // ligand boxes of up to 24 planes: 2 columns, two CTAs per SM; larger boxes: 4 columns
+  k_tile_plan<<<(a.nrot + XS_R - 1) / XS_R, XS_R, 0, s>>>(a, jc);
   if (a.f16) {
     return jc <= 3 ? launch_stream_cols<2, true>(a, top, jc, s) : launch_stream_cols<4, true>(a, top, jc, s);
   }
