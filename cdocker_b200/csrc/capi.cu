@@ -252,9 +252,11 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   const size_t lop_per = streamed ? stream_lop_bytes_per_rotation(n, K, f16) : 0;
   int wave = c->opts.wave_rotations;
   if (wave <= 0) {
-    // keep A + B of one wave near 6 GiB: big enough to fill the GPU, small next to HBM
+    // keep A + B of one wave near 16 GiB (under a tenth of the B200's HBM): at 64^3, waves of
+    // ~4,900 rotations instead of ~1,800 make the split-FP16 search 2-4 % faster (fewer kernel
+    // tails per rotation; measured up to 8,192)
     const double per = (streamed ? (double)lop_per : (double)K * Lb * ncol * 8) + (double)n * ncol * 8;
-    wave = (int)std::min<double>(4096.0, std::max(64.0, 6.0 * (1ull << 30) / per));
+    wave = (int)std::min<double>(8192.0, std::max(64.0, 16.0 * (1ull << 30) / per));
   }
   wave = (int)std::min<long>(wave, std::min<long>(nRot, 65535));
   if (wave < 1) wave = 1;
