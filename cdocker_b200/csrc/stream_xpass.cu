@@ -1,9 +1,10 @@
 // stream_xpass.cu -- the precision form's x pass with streamed operands (n = 64).
 //
 // Same contraction as umma_xpass.cu -- per spectral column and channel, the circulant operator
-// T = [[Tr, Ti], [Ti, -Tr]] (T(x', x) = P~((x + x') mod n)) times the ligand's x planes, BF16
-// hi/lo split, three products, FP32 accumulation in tensor memory over all channels -- but no
-// operand is built inside the kernel:
+// T = [[Tr, Ti], [Ti, -Tr]] (T(x', x) = P~((x + x') mod n)) times the ligand's x planes, FP32
+// accumulation in tensor memory over all channels; split-BF16 form: operator and ligand hi/lo,
+// three products; split-FP16 form: operator hi/lo (scaled by 2^-sigma_k), ligand FP16 (scaled
+// by 2^sigma_k), two products -- but no operand is built inside the kernel:
 //  * the operator tiles are precomputed once per receptor (k_top_build) as the exact shared-
 //    memory image of the K-major, no-swizzle layout and arrive by bulk copies (cp.async.bulk
 //    with an mbarrier transaction count);
@@ -13,13 +14,15 @@
 //    four stages of a column quad read each block whole) and arrive by 16-byte cp.async copies; rows of x chunks that a rotation does not occupy
 //    are zero-filled by the copy itself (source size 0, no read).
 // K order: step j (16 wide) = group 2j (re part of planes 8j..8j+7) and group 2j+1 (im part).
-// Steps outside the chunks any rotation of the CTA occupies are neither loaded nor multiplied.
+// Steps outside the chunks any rotation of the tile occupies are neither loaded nor multiplied;
+// k_tile_plan computes that plan once per 128-rotation tile, and the search orders its rotations
+// so that a tile's rotations touch the same chunks.
 //
-// CTA = COLS columns x 128 rotations, 256 threads: 2 columns, a 96 KB ring (6 stages), 256
-// TMEM columns and two CTAs per SM for ligand boxes <= 24 planes, else 4 columns (32 bytes of B
-// per (rotation, x')), a 192 KB ring (12 stages), 512 TMEM columns, one CTA per SM. A stage is
-// one K-step of one (channel, column): operator hi, lo and ligand hi, lo tiles of 4 KB, three
-// MMAs; small stages keep many in flight. Warp-specialized: warps 0-3 produce (thread =
+// CTA = COLS columns x 128 rotations, 256 threads: 2 columns, a 96 KB ring (6 split-BF16 or 8
+// split-FP16 stages), 256 TMEM columns and two CTAs per SM for ligand boxes <= 24 planes, else
+// 4 columns (32 bytes of B per (rotation, x')), a 192 KB ring (12 or 16 stages), 512 TMEM
+// columns, one CTA per SM. A stage is one K-step of one (channel, column): operator hi, lo and
+// ligand (hi, lo) tiles of 4 KB, three (two) MMAs; small stages keep many in flight. Warp-specialized: warps 0-3 produce (thread =
 // rotation; thread 0 also issues the operator bulk copies), each stage's "full" mbarrier
 // completing when every producer's copies
 // have landed (cp.async.mbarrier.arrive.noinc) and the operator bytes arrived; one thread of
