@@ -41,6 +41,9 @@ def test_version_and_defaults():
     o = L.CdkOpts()
     lib.cdk_opts_default(C.byref(o))
     assert o.max_atoms == 256 and o.form == L.CDK_FORM_FP32
+    # every reserved switch off by default: no per-kernel events, direct planes, no autotune,
+    # the streamed tensor-core x pass where it applies, rotations grouped (reserved[4] = 0)
+    assert list(o.reserved) == [0] * 8
 
 
 def test_invalid_arguments_return_status():
