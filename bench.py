@@ -287,10 +287,25 @@ def reference_cufft_sample(w, n_rot: int = 1000) -> dict:
                          "argmin": round(times[4], 1)}}
 
 
+class _RefWorkload:
+    """The benchmark workload's conformer 0 built by the oracle (oracle.reference_inputs): the
+    same grids, ligand, quaternions and slots as make_rank_workload, without loading the
+    product library, so that the reference arm runs no code of this repository's product."""
+
+    def __init__(self, n_q):
+        from oracle import oracle as O
+        d = O.reference_inputs(WORKLOAD, seed=0, n_conf=1, n_q=n_q)
+        for k, v in d.items():
+            setattr(self, k, v)
+        self.w_n = d["n"]
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    w = make_rank_workload(0, 1)
+    from oracle import oracle as O
+    w = _RefWorkload(N_Q)
+    w.n = w.w_n
     cores = os.cpu_count() or 1
     q = w.quats.reshape(-1, 4)
     per_step = cores
@@ -298,7 +313,6 @@ def run_reference(args, rank, world):
     total = args.warmup + args.steps
     for s in range(total):
         qs = q[(s * per_step) % q.shape[0]:][:per_step]
-        from oracle import oracle as O
         t0 = time.perf_counter()
         O.search_direct(w.grids, w.spacing, w.coor[0], w.charge, w.eps, w.slot, qs[None],
                         prec=0, dense=1, nthreads=cores)
@@ -314,7 +328,8 @@ def run_reference(args, rank, world):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "64^3 grid, K=9, 40-atom ligand (config 1); each step a bounded "
                                f"sample of {per_step} rotations",
-                   "grid": 64, "K": 9, "ligand_atoms": 40},
+                   "grid": 64, "K": 9, "ligand_atoms": 40,
+                   "inputs": f"built by the oracle ({w.source}); no product library loaded"},
         "cpu_baseline": {"value": value, "unit": "rotations/s", "cores": cores, "kind": "port",
                          "sample": f"{per_step} rotations per step, cpuNaive dense loop "
                                    "(src/cpuNaive.cpp:82-216) restated in oracle/, "
@@ -331,9 +346,10 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-TENSOR_STEP_FLOP = 3 * 2 * 128 * 128 * 16  # one K-step of the streamed x pass: 3 BF16 MMAs
+TENSOR_STEP_FLOP = 3 * 2 * 128 * 128 * 16  # one K-step of the streamed-tile x pass: 3 BF16 MMAs
 # split-FP16 form: 2 FP16 MMAs per K-step and FP16 ligand rows (half the bytes of split BF16)
 TENSOR_STEP_FLOP_FP16 = 2 * 2 * 128 * 128 * 16
+MMA_UNIT_FLOP = 2 * 128 * 8 * 16  # Hankel x pass work counter unit: 128 x 8 x 16 multiply-adds
 
 
 def FORMS(fp32, bf16x3, fp16x2):
@@ -347,10 +363,11 @@ def _kernel_roofline(stats: dict, n: int, K: int, hbm: float, peak_kind: str, tr
 
     HBM view: algorithmic bytes = the ligand planes it reads (x planes spread), the window
     planes it writes, and per wave the receptor data it needs (FP32 x pass: the K receptor
-    spectra; streamed tensor-core x pass: the operator tiles of the ligand box's K-steps).
-    Tensor view (streamed tensor-core x pass): the BF16 MMA flops it issued (K-steps x 3
-    MMAs of 128 x 128 x 16) over the measured dense BF16 peak; the x pass is then bound by the
-    tensor cores and the shared memory that feeds them, so this is the headline bound."""
+    spectra; Hankel tensor-core x pass: P~ of every column, K x n complex, from which each CTA
+    builds its resident operator; streamed-tile x pass: the operator tiles of the box's K-steps).
+    Tensor view (tensor-core x pass): the MMA flops it issued over the measured dense BF16 peak.
+    The issued flops include the split products and the dense circulant (more than the FFT's
+    algorithmic flops), so the HBM view is the bound reported for the path."""
     ncol = n * (n // 2 + 1)
     waves = max(1, stats["waves"])
     km = stats["kernel_ms"]
@@ -358,11 +375,13 @@ def _kernel_roofline(stats: dict, n: int, K: int, hbm: float, peak_kind: str, tr
     plane = ncol * 8
     rot = stats["rotations"]
     kind = stats.get("xpass_kind")
-    fp16 = kind == "tcgen05_streamed_fp16"
-    streamed = kind == "tcgen05_streamed" or fp16
+    fp16 = kind in ("tcgen05_streamed_fp16", "tcgen05_hankel_fp16")
+    hankel = kind in ("tcgen05_hankel", "tcgen05_hankel_fp16")
+    tiles = kind in ("tcgen05_streamed", "tcgen05_streamed_fp16")
     lig = plane // 2 if fp16 else plane  # ligand bytes per plane: FP16 rows, split BF16 or FP32
     jc = (stats["box"] + 7) // 8
-    receptor = K * ncol * 2 * jc * 4096 if streamed else K * n * plane
+    receptor = (K * ncol * n * 8 if hankel else
+                K * ncol * 2 * jc * 4096 if tiles else K * n * plane)
     alg = {
         "xpass": stats["planes_spread"] * lig + stats["planes_window"] * plane + waves * receptor,
         "spread_yz": stats["planes_spread"] * lig,
@@ -374,20 +393,42 @@ def _kernel_roofline(stats: dict, n: int, K: int, hbm: float, peak_kind: str, tr
     t = km[dom] / waves / 1e3
     achieved = per_launch / t / 1e9
     tr = traffic.get(dom)
-    hbm_view = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "peak_kind": peak_kind,
-                "traffic": (tr * rot / waves) if tr is not None else None,
-                "algorithmic_bytes_per_launch": per_launch}
-    out = {"kernel": dom, **hbm_view, "avg_launch_ms": t * 1e3,
+    out = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+           "frac": achieved / hbm, "peak_kind": peak_kind,
+           "traffic": (tr * rot / waves) if tr is not None else None,
+           "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": t * 1e3,
            "share_of_device_time": km[dom] / max(1e-9, sum(km.values())), "kernel_ms": km}
-    if dom == "xpass" and streamed and stats.get("tensor_steps"):
+    if dom == "xpass" and (hankel or tiles):
         tp, tkind = _tensor_peak()
-        flop = stats["tensor_steps"] * (TENSOR_STEP_FLOP_FP16 if fp16 else TENSOR_STEP_FLOP) / waves
+        if hankel:
+            flop = stats.get("mma_units", 0) * MMA_UNIT_FLOP / waves
+        else:
+            flop = stats["tensor_steps"] * (TENSOR_STEP_FLOP_FP16 if fp16 else TENSOR_STEP_FLOP) / waves
         tach = flop / t / 1e12
-        out.update({"bound": "tensor", "achieved": tach, "peak": tp, "unit": "TFLOP/s",
-                    "frac": tach / tp, "peak_kind": tkind, "flop_per_launch": flop,
-                    "hbm_view": hbm_view})
+        out["tensor_view"] = {"achieved": tach, "peak": tp, "unit": "TFLOP/s", "frac": tach / tp,
+                              "peak_kind": tkind, "flop_per_launch": flop,
+                              "note": "issued MMA flops (split products, dense circulant)"}
     return out
+
+
+def all_rotation_fp64_error(rec, w, e, i, n_q):
+    """Error of every rotation's returned minimum against the FP64 energy of the same pose: the
+    FP64 direct trilinear grid-energy sum on the GPU (cdk_rescore_fp64) of each rotation at its
+    returned translation; |E - E64| / max(|E64|, 1) over all rotations with a window."""
+    valid = np.isfinite(e)
+    idx = np.nonzero(valid)[0]
+    q = w.quats.reshape(-1, 4)
+    e64 = np.full(e.shape[0], np.nan)
+    step = 250_000
+    for b in range(0, idx.size, step):
+        sel = idx[b:b + step]
+        e64[sel] = rec.rescore_fp64(w.coor, w.charge, w.eps, w.slot, (sel // n_q).astype(np.int32),
+                                    q[sel], i[sel])
+    err = np.abs(e[valid].astype(np.float64) - e64[valid]) / np.maximum(np.abs(e64[valid]), 1.0)
+    return {"rotations": int(valid.sum()), "max_rel_err_vs_fp64": float(err.max()) if err.size else None,
+            "median_rel_err_vs_fp64": float(np.median(err)) if err.size else None,
+            "p999_rel_err_vs_fp64": float(np.quantile(err, 0.999)) if err.size else None,
+            "note": "every rotation: returned minimum vs the FP64 energy of its returned pose"}
 
 
 def _accuracy_sample(w, e, i, n_sample=24):
@@ -480,6 +521,10 @@ def run_ours(args, rank, world, local_rank):
         rec, ms, stats, clocks, e, i = timed_form(form)
         forms[name] = {"rec": rec, "ms": ms, "stats": stats, "clocks": clocks, "acc": None,
                        "e": e, "i": i, "value": world * n_rot * args.steps / (ms / 1e3)}
+        # checker, outside the timed region: every rotation's minimum against the FP64 energy
+        # of its returned pose
+        forms[name]["fp64_all"] = (all_rotation_fp64_error(rec, w, e, i, N_Q)
+                                   if rank == 0 and not args.no_check else None)
     clustering = clustering_sample() if rank == 0 else None
     grids_gen = receptor_grids_sample() if rank == 0 else None
     cpu_base, clus_check = None, None
@@ -490,10 +535,12 @@ def run_ours(args, rank, world, local_rank):
         for k, v in acc.items():
             forms[k]["acc"] = v
     agreement = pose_agreement(w, forms) if rank == 0 else None
-    # headline: the fastest form that meets its error bar on the checked sample
+    # headline: the fastest form that meets its error bar on the checked sample (24 rotations
+    # against the full FP64 search) and on every rotation (minimum vs FP64 of its pose)
     bars = {"fp32": 1e-4, "bf16x3_tensor_core": 1e-3, "fp16x2_tensor_core": 1e-3}
     ok = [k for k, v in forms.items()
-          if v["acc"] is None or v["acc"]["max_rel_err_vs_fp64"] <= bars[k]]
+          if (v["acc"] is None or v["acc"]["max_rel_err_vs_fp64"] <= bars[k]) and
+          (v["fp64_all"] is None or v["fp64_all"]["max_rel_err_vs_fp64"] <= bars[k])]
     head = max(ok or list(forms), key=lambda k: forms[k]["value"])
     if world > 1:
         # only rank 0 checked accuracy: every rank times the e2e leg on rank 0's choice
@@ -550,6 +597,7 @@ def run_ours(args, rank, world, local_rank):
         hbm, peak_kind = _peaks()
         nc = 64 * 64 * 33  # half-spectrum points of one grid
         b_rot = 8 * 9 * 64 ** 3 + 16 * 9 * nc + 16 * nc + 8 * 64 ** 3
+        dram_rot = sum(v for k, v in traffic.items() if isinstance(v, (int, float))) if traffic else None
         traffic = {}
         tp = os.path.join(ROOT, "profiles", "dram_bytes_per_rotation.json")
         if os.path.exists(tp):
@@ -577,13 +625,21 @@ def run_ours(args, rank, world, local_rank):
             "e2e": {"value": e2e_val, "unit": "rotations/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "form": head},
             "roofline": _kernel_roofline(H["stats"], 64, 9, hbm, peak_kind, traffic),
-            "fft_roofline": {"bytes_per_rotation": b_rot, "achieved_gbs": rps * b_rot / 1e9,
-                             "peak_gbs": hbm, "frac": rps * b_rot / 1e9 / hbm,
-                             "peak_kind": peak_kind,
-                             "note": "staged-pipeline algorithmic bytes B_rot = 8KN + 16K*Nc + "
-                                     "16Nc + 8N per rotation (Nc = n*n*(n/2+1)), per GPU"},
+            "staged_equivalent": {
+                "bytes_per_rotation": b_rot, "equivalent_gbs": rps * b_rot / 1e9,
+                "note": "not a roofline: the bytes a staged cuFFT pipeline would move per "
+                        "rotation (B_rot = 8KN + 16K*Nc + 16Nc + 8N, Nc = n*n*(n/2+1)) times the "
+                        "rotation rate; the fused path moves far fewer bytes"},
+            "step_dram": {
+                "bytes_per_rotation": dram_rot,
+                "achieved_gbs": rps * dram_rot / 1e9 if dram_rot else None, "peak_gbs": hbm,
+                "frac": rps * dram_rot / 1e9 / hbm if dram_rot else None, "peak_kind": peak_kind,
+                "note": "DRAM bytes per rotation of all kernels of the step (ncu, "
+                        "profiles/dram_bytes_per_rotation.json) times the rotation rate"},
             "forms": {k: {"value": v["value"], "ms_per_step": v["ms"] / args.steps,
-                          "accuracy": v["acc"], "kernel_ms_last_step": v["stats"]["kernel_ms"]}
+                          "accuracy": v["acc"], "all_rotations_vs_fp64": v["fp64_all"],
+                          "xpass_kind": v["stats"]["xpass_kind"],
+                          "kernel_ms_last_step": v["stats"]["kernel_ms"]}
                       for k, v in forms.items()},
         }
         if serving is not None:
@@ -628,28 +684,139 @@ def serving_sample(w, rec_unused, secs: float) -> dict:
 
 
 def serve_sweep(args):
-    """Config 3: one resident 96^3 receptor (6,000 atoms in a 48 A cube, K = 9), requests with
-    ligands of 10-80 atoms, 10-200 conformers, 500-5,000 rotations, Poisson arrivals at five
-    rates; both forms. Prints one JSON line per (form, rate)."""
+    """Config 3: one resident 96^3 receptor (6,000 atoms in a 48 A cube, all 9 grids: 8 vdW +
+    elec), requests with ligands of 10-80 atoms, 10-200 conformers and 500-5,000 rotations,
+    Poisson arrivals; every form. Per form, a burst of requests submitted at once measures the
+    server's capacity (rotations/s); then five Poisson rates at 0.25, 0.5, 0.75, 0.9 and 1.1 of
+    that capacity (the top one saturates the device), each for --serve-secs of arrivals. Prints
+    one JSON line per (form, rate) and a summary line (not the bench line)."""
     from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP16X2, CDK_FORM_FP32, Receptor, synth
     from cdocker_b200.serving import Server, make_requests, poisson_arrivals, run_load
     grids, mid, length = synth.make_receptor(96, 6000, 48.0, seed=0)
     secs = max(2.0, args.serve_secs)
+    mix = dict(atoms=(10, 80), confs=(10, 200), rots=(500, 5000))
+    burst = make_requests(24, 999, 0.5, length, synth.PROBE_RADII, **mix)
+    summary = {}
     for form_name, form in FORMS(CDK_FORM_FP32, CDK_FORM_BF16X3, CDK_FORM_FP16X2):
+        if args.forms not in ("both", "all") and args.forms != form_name:
+            continue
         with Receptor(grids, 0.5, max_atoms=96, form=form) as rec:
-            for rate in (2.0, 5.0, 10.0, 20.0, 40.0):
-                arr = poisson_arrivals(rate, secs, seed=int(rate * 10))
-                reqs = make_requests(len(arr), int(rate * 100), 0.5, length, synth.PROBE_RADII,
-                                     atoms=(10, 80), confs=(10, 200), rots=(500, 5000))
-                with Server(rec, arena_bytes=1 << 30, wave_rotations=1024, max_atoms=96,
-                            max_box=40) as srv:
+            srv_kw = dict(arena_bytes=2 << 30, wave_rotations=1024, max_atoms=96, max_box=40)
+            with Server(rec, **srv_kw) as srv:
+                run_load(srv, burst[:4], np.zeros(4))  # warm-up: module load, scratch first touch
+                cap = run_load(srv, burst, np.zeros(len(burst)))
+                st = srv.stats()
+            capacity = cap["rotations"] / cap["wall_s"]
+            mean_rot = float(np.mean([r["rotations"] for r in burst]))
+            lines = []
+            for frac in (0.25, 0.5, 0.75, 0.9, 1.1):
+                rate = frac * capacity / mean_rot
+                arr = poisson_arrivals(rate, secs, seed=int(frac * 100))
+                reqs = make_requests(len(arr), int(frac * 1000) + 7, 0.5, length, synth.PROBE_RADII, **mix)
+                with Server(rec, **srv_kw) as srv:
                     res = run_load(srv, reqs, arr)
                     st = srv.stats()
-                # the streamed tensor-core x pass exists at 64^3 only: at 96^3 both forms
-                # serve on the FP32 x pass (tc_waves = 0)
                 res.update({"config": "serving, 96^3 K=9, 6,000-atom receptor", "form": form_name,
-                            "rate_hz": rate, "waves": st["waves"], "tc_waves": st["tc_waves"]})
+                            "rate_hz": rate, "load_frac_of_capacity": frac,
+                            "offered_rotations_per_s": rate * mean_rot,
+                            "waves": st["waves"], "tc_waves": st["tc_waves"],
+                            "request_mix": "ligand U(10,80) atoms, conformers U(10,200), rotations "
+                                           "U(500,5000), Poisson arrivals"})
                 print(json.dumps(res), flush=True)
+                lines.append({k: res[k] for k in ("rate_hz", "load_frac_of_capacity", "p50_ms",
+                                                  "p99_ms", "rotations_per_s", "requests")})
+            summary[form_name] = {"capacity_rotations_per_s": capacity,
+                                  "capacity_tc_waves": st["tc_waves"], "rates": lines}
+    print(json.dumps({"serve_sweep": "config 3", "grid": 96, "forms": summary}), flush=True)
+
+
+def config4_run(args):
+    """Config 4, the largest single search: 128^3 grid at 0.5 A, K = 9 (8 vdW + elec) from a
+    12,000-atom synthetic receptor in a 64 A cube; a 60-atom ligand, 500 conformers x 2,000
+    uniform quaternions = 1e6 rotations, streamed in memory-sized waves. Each form (FP32,
+    split-BF16, split-FP16) runs one untimed warm-up search of the first 20 conformers, then the
+    whole search timed on the device (CUDA events on the search stream) with clocks sampled, and
+    the whole search again through cdk_search with host buffers (e2e). The checker then gives
+    the error of every rotation's minimum against the FP64 energy of its returned pose, and the
+    FP64 oracle's full search of 16 rotations (minimum and argmin). Prints one JSON line."""
+    import torch
+    from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP16X2, CDK_FORM_FP32, Receptor, synth
+    from oracle import oracle as O
+    from tests.parity import rel_err
+    n_conf, n_q = args.c4_conformers, args.c4_quaternions
+    t0 = time.perf_counter()
+    w = synth.make_workload("c4_128", seed=0, n_conf=n_conf, n_q=n_q)
+    t_inputs = time.perf_counter() - t0
+    dev = torch.device("cuda", 0)
+    n_atom, n_rot = w.coor.shape[1], n_conf * n_q
+    d_coor = torch.from_numpy(w.coor).to(dev)
+    d_charge = torch.from_numpy(w.charge).to(dev)
+    d_eps = torch.from_numpy(w.eps).to(dev)
+    d_slot = torch.from_numpy(w.slot).to(dev)
+    d_q = torch.from_numpy(w.quats).to(dev)
+    d_e = torch.empty(n_rot, device=dev)
+    d_i = torch.empty(n_rot, 3, dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sample = np.linspace(0, n_rot - 1, 16).astype(int)
+    qq = w.quats.reshape(-1, 4)
+    r64 = np.empty(sample.size)
+    ri = np.empty((sample.size, 3), np.int32)
+    for j, r in enumerate(sample):
+        _, ii, m = O.search_direct(w.grids, w.spacing, w.coor[r // n_q], w.charge, w.eps, w.slot,
+                                   qq[r][None, None], prec=1)
+        r64[j], ri[j] = m[0], ii[0]
+    hbm, peak_kind = _peaks()
+    out = {}
+    for name, form in FORMS(CDK_FORM_FP32, CDK_FORM_BF16X3, CDK_FORM_FP16X2):
+        if args.forms not in ("both", "all") and args.forms != name:
+            continue
+        with Receptor(w.grids, w.spacing, form=form, profile=True) as rec:
+            warm = min(n_conf, 20)
+            rec.search_device(n_atom, warm, d_coor.data_ptr(), d_charge.data_ptr(), d_eps.data_ptr(),
+                              d_slot.data_ptr(), n_q, d_q.data_ptr(), d_e.data_ptr(), d_i.data_ptr(),
+                              stream.cuda_stream)
+            torch.cuda.synchronize(dev)
+            sampler = ClockSampler(0)
+            sampler.start()
+            time.sleep(0.3)
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                ev0.record(stream)
+                rec.search_device(n_atom, n_conf, d_coor.data_ptr(), d_charge.data_ptr(),
+                                  d_eps.data_ptr(), d_slot.data_ptr(), n_q, d_q.data_ptr(),
+                                  d_e.data_ptr(), d_i.data_ptr(), stream.cuda_stream)
+                ev1.record(stream)
+            torch.cuda.synchronize(dev)
+            clocks = sampler.stop()
+            ms = ev0.elapsed_time(ev1)
+            st = rec.stats()
+            e, i = d_e.cpu().numpy(), d_i.cpu().numpy()
+            # e2e: host buffers through cdk_search, copies inside the timing
+            t1 = time.perf_counter()
+            e2, i2 = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+            e2e_s = time.perf_counter() - t1
+            same = bool(np.array_equal(e2.view(np.uint32), e.view(np.uint32)) and np.array_equal(i2, i))
+            allrot = all_rotation_fp64_error(rec, w, e, i, n_q)
+            err = rel_err(e[sample], r64)
+            rl = _kernel_roofline(st, 128, w.K, hbm, peak_kind, {})
+        out[name] = {
+            "rotations_per_s": n_rot / (ms / 1e3), "device_ms": ms,
+            "e2e_rotations_per_s": n_rot / e2e_s, "e2e_identical_to_device_run": same,
+            "xpass_kind": st["xpass_kind"], "waves": st["waves"], "wave_rotations": st["wave_rotations"],
+            "box_planes": st["box"], "kernel_ms": st["kernel_ms"], "clocks": clocks,
+            "all_rotations_vs_fp64": allrot,
+            "fp64_full_search_sample": {"rotations": int(sample.size),
+                                        "max_rel_err": float(err.max()),
+                                        "median_rel_err": float(np.median(err)),
+                                        "best_translation_agreement": float(np.mean(np.all(i[sample] == ri, axis=1)))},
+            "dominant_kernel_roofline": rl,
+        }
+        print(json.dumps({"config4_form": name, **out[name]}), flush=True)
+    line = {"config": "config 4: 128^3 grid at 0.5 A, K=9, 12,000-atom synthetic receptor, 60-atom "
+                      f"ligand, {n_conf} conformers x {n_q} quaternions = {n_rot} rotations, streamed",
+            "unit": "rotations/s", "data": "synthetic", "input_build_s": round(t_inputs, 1),
+            "forms": out}
+    print(json.dumps(line), flush=True)
 
 
 def profile_run(args):
@@ -704,6 +871,11 @@ def main():
     ap.add_argument("--serve-sweep", action="store_true",
                     help="config 3: 96^3 receptor, Poisson request streams at 5 rates; one JSON "
                          "line per rate (not the bench line)")
+    ap.add_argument("--config4", action="store_true",
+                    help="config 4: 128^3, 1e6 rotations, all forms, error vs FP64 on every "
+                         "rotation; one JSON line (not the bench line)")
+    ap.add_argument("--c4-conformers", type=int, default=500)
+    ap.add_argument("--c4-quaternions", type=int, default=2000)
     ap.add_argument("--profile-run", type=int, default=0,
                     help="run one search of this many rotations with per-kernel events and "
                          "print the timings (the small case used for ncu captures)")
@@ -720,6 +892,9 @@ def main():
         return
     if args.serve_sweep:
         serve_sweep(args)
+        return
+    if args.config4:
+        config4_run(args)
         return
     import torch
     import torch.distributed as dist

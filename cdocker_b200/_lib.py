@@ -101,6 +101,8 @@ SIGNATURES = {
     "cdk_server_stats": (C.c_int, [_vp, _dp, C.c_int]),
     "cdk_server_destroy": (C.c_int, [_vp]),
     "cdk_pose_coordinates": (C.c_int, [C.c_int, _fp, _fp, _dp, C.c_float, _ip, _dp]),
+    "cdk_sort_index": (C.c_int, [_fp, C.c_long, C.POINTER(C.c_long)]),
+    "cdk_ctx_top_poses": (C.c_int, [_vp, C.c_int, _ip, _fp, _ip, _dp, _ip]),
     "cdk_cluster_conformers": (C.c_int, [C.c_int, C.c_int, _dp, _dp, _vp, C.c_double, C.c_int,
                                          _ip, _ip]),
     "cdk_pair_rmsd": (C.c_int, [C.c_int, C.c_int, _dp, _vp, _dp]),

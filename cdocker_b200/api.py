@@ -134,7 +134,8 @@ class Receptor:
                  max_atoms: int = 256, col_tile: int = 0, form: int = L.CDK_FORM_FP32,
                  use_graphs: int = 0, profile: bool = False, fft_planes: bool = False,
                  autotune: bool = False, tc_mma_sync: bool = False, tc_build: bool = False,
-                 tc_tmem_ligand: bool = False, group_rotations: bool = True):
+                 group_rotations: bool = True, tc_stream_tiles: bool = False,
+                 tc_cols: int = 0, top_k: int = 0, tie_break: bool = True):
         g = _f32(grids)
         if g.ndim != 4:
             raise ValueError("grids must be [K, n, n, n]")
@@ -152,7 +153,10 @@ class Receptor:
         opts.reserved[0] = 1 if profile else 0
         opts.reserved[1] = 1 if fft_planes else 0
         opts.reserved[2] = 1 if autotune else 0
-        opts.reserved[3] = 1 if tc_mma_sync else (2 if tc_build else (3 if tc_tmem_ligand else 0))
+        opts.reserved[3] = 1 if tc_mma_sync else (2 if tc_build else (3 if tc_stream_tiles else 0))
+        opts.reserved[5] = tc_cols
+        opts.reserved[6] = top_k
+        opts.reserved[7] = 0 if tie_break else 1
         opts.reserved[4] = 0 if group_rotations else 1
         h = C.c_void_p()
         L.check(lib.cdk_ctx_create(g.shape[1], g.shape[2], g.shape[3], self.spacing, self.K,
@@ -221,8 +225,8 @@ class Receptor:
         return out
 
     def stats(self) -> dict:
-        out = np.zeros(18, np.float64)
-        L.check(L.lib().cdk_ctx_stats(self._h, out.ctypes.data_as(_dp), 18))
+        out = np.zeros(21, np.float64)
+        L.check(L.lib().cdk_ctx_stats(self._h, out.ctypes.data_as(_dp), 21))
         names = ["prep", "spread_yz", "xpass", "yz_inv_argmin", "finalize"]
         return {"launches": int(out[0]), "waves": int(out[1]), "rotations": int(out[2]),
                 "device_ms": float(out[3]), "box": int(out[4]), "wave_rotations": int(out[5]),
@@ -231,6 +235,23 @@ class Receptor:
                 "col_tile": int(out[13]), "rotations_per_cta": int(out[14]),
                 "graph_state": int(out[15]),
                 "xpass_kind": ["fp32_radix", "mma_sync", "tcgen05_build",
-                               "tcgen05_streamed", "tcgen05_streamed_tmem",
-                               "tcgen05_streamed_fp16"][int(out[16])],
-                "tensor_steps": int(out[17])}
+                               "tcgen05_streamed", "unused",
+                               "tcgen05_streamed_fp16", "tcgen05_hankel",
+                               "tcgen05_hankel_fp16"][int(out[16])],
+                "tensor_steps": int(out[17]), "mma_units": int(out[18]),
+                "near_ties_rescored": int(out[19]), "near_ties_changed": int(out[20])}
+
+    def top_poses(self):
+        """The FP64 re-scores of each wave's lowest poses from the last search
+        (cdk_ctx_top_poses): rot [m], minE [m], idx [m, 3], e64 [m]; m = waves x k."""
+        cnt = C.c_int(0)
+        L.check(L.lib().cdk_ctx_top_poses(self._h, 0, None, None, None, None, C.byref(cnt)))
+        m = cnt.value
+        rot = np.empty(m, np.int32)
+        e = np.empty(m, np.float32)
+        idx = np.empty((m, 3), np.int32)
+        e64 = np.empty(m, np.float64)
+        if m:
+            L.check(L.lib().cdk_ctx_top_poses(self._h, m, _pi(rot), _pf(e), _pi(idx),
+                                              e64.ctypes.data_as(_dp), C.byref(cnt)))
+        return rot, e, idx, e64

@@ -28,7 +28,7 @@ CXX_FLAGS = ["-O2", "-std=c++14", "-fPIC", "-ffp-contract=off", "-Wno-deprecated
              "-pthread"]
 
 CU_SOURCES = ["search_kernels.cu", "compat_kernels.cu", "capi.cu", "noalloc.cu", "server.cu", "tc_xpass.cu", "umma_xpass.cu",
-              "cluster.cu", "stream_xpass.cu", "receptor_grids.cu"]
+              "cluster.cu", "stream_xpass.cu", "hankel_xpass.cu", "receptor_grids.cu"]
 CPP_SOURCES = ["host/reference_api.cpp"]
 
 

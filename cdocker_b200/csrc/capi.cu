@@ -115,10 +115,11 @@ struct cdk_ctx {
   Arena tables;               // per-search tables
   Arena io;                   // staging of host-buffer searches
   Arena group;                // rotation grouping of the tensor-core x pass (sorted list, keys)
+  Arena topk;                 // precision forms: per wave the k lowest poses with FP64 re-scores
+  int topk_k = 0, topk_waves = 0;  // of the last search
   unsigned int* d_misc = nullptr;  // [0] diameter bits, [1] flags, [2] error count, [3] fault,
                                    // [4] FP16 range flag
-  unsigned long long* d_work = nullptr;  // [0] x planes spread (A), [1] window planes (B),
-                                          // [2] tensor-core K-steps of the streamed x pass
+  unsigned long long* d_work = nullptr;  // [8] work counters (WaveArgs.work)
   unsigned long long* h_work = nullptr;
   unsigned int* h_misc = nullptr;  // pinned mirror
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -226,16 +227,18 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   const size_t ncol = (size_t)n * (n / 2 + 1);
   const bool tc = c->opts.form != CDK_FORM_FP32;
   const bool f16form = c->opts.form == CDK_FORM_FP16X2;
-  // streamed tensor-core x pass: n = 64, box <= 32 planes, direct planes (<= 96 atoms)
+  // tensor-core x pass with streamed ligand rows (direct planes: ligands <= 96 atoms): the
+  // Hankel-operator kernel at every n (box <= 32 planes, operator fits shared memory); the older
+  // 64^3 kernel with streamed operator tiles on request (reserved[3] = 3)
   WaveArgs probe{};
   probe.kyof = (c->opts.reserved[1] == 0) ? c->d_kyof : nullptr;
   probe.max_atoms = maxAtoms;
   probe.atom_cap = maxAtoms;
-  // the split-FP16 form has the streamed kernel only; where that does not apply, the split-BF16
-  // kernels run (more accurate)
-  const int variant = f16form ? 0 : c->opts.reserved[3];
-  const bool streamed = tc && (variant == 0 || variant == 3) && stream_supported(n, Lb) && direct_planes(probe);
-  const bool tmem_ligand = variant == 3;
+  const int variant = c->opts.reserved[3];
+  HankelPlan hp{};
+  const bool hankel = tc && (variant == 0) && direct_planes(probe) &&
+                      hankel_plan(n, K, Lb, f16form, c->opts.reserved[5], &hp);
+  const bool streamed = tc && (variant == 3) && stream_supported(n, Lb) && direct_planes(probe);
   if (streamed && !c->d_top) {
     const size_t tb = stream_top_bytes(n, K);
     if (cudaMalloc(&c->d_top, tb) != cudaSuccess) {
@@ -248,27 +251,45 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     // stream-ordered before the waves
     CDK_CUDA(launch_top_build(n, K, c->d_ptilde, c->d_top, f16form ? osc.data() : nullptr, s));
   }
-  const bool f16 = f16form && streamed;
-  const size_t lop_per = streamed ? stream_lop_bytes_per_rotation(n, K, f16) : 0;
+  std::vector<float> osc(K);
+  for (int k = 0; k < K; ++k) osc[k] = 1.f / c->lscale[k];
+  const bool rows = hankel || streamed;  // the plane kernel writes split / FP16 ligand rows
+  if (tc && f16form && !rows) {
+    set_error("the split-FP16 form runs on the tensor-core x pass with ligand rows only (ligands "
+              "of at most 96 atoms, a ligand box of at most 32 planes, K x n small enough for the "
+              "operator to fit shared memory); use CDK_FORM_BF16X3");
+    return CDK_ERR_UNSUPPORTED;
+  }
+  const bool f16 = f16form && rows;
+  const size_t lop_per = rows ? stream_lop_bytes_per_rotation(n, K, f16) : 0;
   int wave = c->opts.wave_rotations;
   if (wave <= 0) {
-    // keep A + B of one wave near 16 GiB (under a tenth of the B200's HBM): at 64^3, waves of
-    // ~4,900 rotations instead of ~1,800 make the split-FP16 search 2-4 % faster (fewer kernel
-    // tails per rotation; measured up to 8,192)
-    const double per = (streamed ? (double)lop_per : (double)K * Lb * ncol * 8) + (double)n * ncol * 8;
-    wave = (int)std::min<double>(8192.0, std::max(64.0, 16.0 * (1ull << 30) / per));
+    // keep A + B of one wave near 16 GiB at n <= 64 (under a tenth of the B200's HBM): at 64^3,
+    // waves of ~4,900 rotations instead of ~1,800 make the split-FP16 search 2-4 % faster (fewer
+    // kernel tails per rotation; measured up to 8,192); 32 GiB at n >= 96, where a rotation's
+    // rows and window planes take 10-30 MB
+    const double per = (rows ? (double)lop_per : (double)K * Lb * ncol * 8) + (double)n * ncol * 8;
+    const double target = (n <= 64 ? 16.0 : 32.0) * (1ull << 30);
+    wave = (int)std::min<double>(8192.0, std::max(64.0, target / per));
   }
   wave = (int)std::min<long>(wave, std::min<long>(nRot, 65535));
   if (wave < 1) wave = 1;
   const size_t b_rotxyz = align_up((size_t)wave * maxAtoms * sizeof(float4));
   const size_t b_rec = align_up((size_t)wave * sizeof(RotRec));
   const size_t b_keys = align_up((size_t)wave * sizeof(unsigned long long));
-  const size_t b_A = align_up(streamed ? (size_t)((wave + 7) & ~7) * lop_per
-                                       : (size_t)wave * K * Lb * ncol * sizeof(float2));
+  // precision forms: the FP64 near-tie break (reserved[7] = 1 turns it off) keeps every window
+  // plane's two smallest keys; per wave the k lowest poses are re-scored in FP64 (reserved[6]:
+  // 0 = 8 in the precision forms and none in the FP32 form, -1 = none, 1..32 = k)
+  const bool tiebreak = tc && c->opts.reserved[7] == 0;
+  const int topk = c->opts.reserved[6] < 0 ? 0 : c->opts.reserved[6] > 0 ? std::min(c->opts.reserved[6], (int)kTopMax)
+                                                                        : (tc ? 8 : 0);
+  const size_t b_keys2 = tiebreak ? align_up((size_t)wave * n * 2 * sizeof(unsigned long long)) : 0;
+  const size_t b_A = align_up(rows ? (size_t)((wave + 7) & ~7) * lop_per
+                                   : (size_t)wave * K * Lb * ncol * sizeof(float2));
   const size_t b_B = align_up((size_t)wave * n * ncol * sizeof(float2));
-  if (!grow(c->wave, b_rotxyz + b_rec + b_keys + b_A + b_B)) {
+  if (!grow(c->wave, b_rotxyz + b_rec + b_keys + b_A + b_B + b_keys2)) {
     set_error("cudaMalloc of the wave scratch failed (" +
-              std::to_string((b_rotxyz + b_rec + b_keys + b_A + b_B) >> 20) + " MiB)");
+              std::to_string((b_rotxyz + b_rec + b_keys + b_A + b_B + b_keys2) >> 20) + " MiB)");
     return CDK_ERR_NOMEM;
   }
   char* base = static_cast<char*>(c->wave.base);
@@ -285,9 +306,10 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   a.rot_xyz = reinterpret_cast<float4*>(base);
   a.rec = reinterpret_cast<RotRec*>(base + b_rotxyz);
   a.keys = reinterpret_cast<unsigned long long*>(base + b_rotxyz + b_rec);
-  a.A = streamed ? nullptr : reinterpret_cast<float2*>(base + b_rotxyz + b_rec + b_keys);
-  a.lop = streamed ? reinterpret_cast<unsigned char*>(base + b_rotxyz + b_rec + b_keys) : nullptr;
+  a.A = rows ? nullptr : reinterpret_cast<float2*>(base + b_rotxyz + b_rec + b_keys);
+  a.lop = rows ? reinterpret_cast<unsigned char*>(base + b_rotxyz + b_rec + b_keys) : nullptr;
   a.B = reinterpret_cast<float2*>(base + b_rotxyz + b_rec + b_keys + b_A);
+  a.keys2 = tiebreak ? reinterpret_cast<unsigned long long*>(base + b_rotxyz + b_rec + b_keys + b_A + b_B) : nullptr;
   a.phat = c->d_phat;
   a.tw = c->d_tw;
   a.minE = d_minE;
@@ -298,7 +320,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   for (int k = 0; k < KMAX; ++k) a.lscale[k] = c->lscale[k];
   a.range_err = reinterpret_cast<int*>(c->d_misc + 4);
   // the shared-memory streamed x pass writes B in plane groups (whole sectors per store)
-  a.bgroup = (streamed && !tmem_ligand) ? stream_bgroup() : 1;
+  a.bgroup = rows ? stream_bgroup() : 1;
   a.col_tile = c->opts.col_tile > 0 ? c->opts.col_tile : pick_col_tile(n, K);
   a.kyof = (c->opts.reserved[1] == 0) ? c->d_kyof : nullptr;  // reserved[1] = 1: FFT planes
   a.chunk = 0;
@@ -306,7 +328,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     if (c->tuned_col_tile) a.col_tile = c->tuned_col_tile;
     a.chunk = c->tuned_chunk;
   }
-  if (tc && !streamed && xpass_tc_smem_bytes(n, K, Lb) > 227 * 1024) {
+  if (tc && !rows && xpass_tc_smem_bytes(n, K, Lb) > 227 * 1024) {
     set_error("ligand box too large for the tensor-core x pass at this grid size and K");
     return CDK_ERR_UNSUPPORTED;
   }
@@ -316,11 +338,17 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     return CDK_ERR_INVALID;
   }
   CDK_CUDA(cudaMemsetAsync(c->d_misc + 2, 0, 3 * sizeof(unsigned int), s));
-  CDK_CUDA(cudaMemsetAsync(c->d_work, 0, 4 * sizeof(unsigned long long), s));
-  const bool umma = tc && !streamed && c->opts.reserved[3] != 1 && umma_supported(n, Lb);
+  CDK_CUDA(cudaMemsetAsync(c->d_work, 0, 8 * sizeof(unsigned long long), s));
+  const bool umma = tc && !rows && c->opts.reserved[3] != 1 && umma_supported(n, Lb);
   a.work = c->d_work;
   const bool prof = c->opts.reserved[0] != 0;
   const long nwaves = (nRot + wave - 1) / wave;
+  c->topk_k = topk;
+  c->topk_waves = 0;
+  if (topk > 0 && !grow(c->topk, (size_t)nwaves * topk * sizeof(TopPose))) {
+    set_error("cudaMalloc of the top-pose buffer failed");
+    return CDK_ERR_NOMEM;
+  }
   if (prof) {
     const size_t need = (size_t)nwaves * (kLaunchesPerWave + 1);
     while (c->kev.size() < need) {
@@ -330,7 +358,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     }
   }
   c->kev_used = 0;
-  if (c->opts.reserved[2] && c->tuned_Lb != Lb && !streamed) {
+  if (c->opts.reserved[2] && c->tuned_Lb != Lb && !rows) {
     int rc = autotune_xpass(c, a, d_rots, nRot, wave, tc, s);
     if (rc) return rc;
     a.col_tile = c->tuned_col_tile ? c->tuned_col_tile : a.col_tile;
@@ -341,7 +369,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   // K-steps per 128-rotation tile; reserved[4] = 1 keeps the given order)
   const RotDesc* order = d_rots;
   const int jc = (Lb + 7) / 8;
-  if (streamed && c->opts.reserved[4] == 0 && nRot > 128 && jc > 1) {
+  if (rows && c->opts.reserved[4] == 0 && nRot > 128 && jc > 1) {
     const size_t gb = group_rotations_bytes(nRot);
     if (!grow(c->group, gb)) {
       set_error("cudaMalloc of the rotation-grouping scratch failed (" + std::to_string(gb >> 20) + " MiB)");
@@ -362,27 +390,32 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     if (prof) CDK_CUDA(cudaEventRecord(ev[1], s));
     CDK_CUDA(launch_spread_yz(a, s));
     if (prof) CDK_CUDA(cudaEventRecord(ev[2], s));
-    if (streamed) CDK_CUDA(launch_xpass_stream(a, c->d_top, tmem_ligand, s));
+    if (hankel) CDK_CUDA(launch_xpass_hankel(a, c->d_ptilde, osc.data(), hp, s));
+    else if (streamed) CDK_CUDA(launch_xpass_stream(a, c->d_top, s));
     else if (umma) CDK_CUDA(launch_xpass_umma(a, c->d_ptilde, s));
     else if (tc) CDK_CUDA(launch_xpass_tc(a, c->d_ptilde, s));
     else CDK_CUDA(launch_xpass(a, s));
     if (prof) CDK_CUDA(cudaEventRecord(ev[3], s));
     CDK_CUDA(launch_yz_inv_argmin(a, s));
+    if (tiebreak) CDK_CUDA(launch_tiebreak(a, c->d_grids, f16form ? 1e-3f : 1e-4f, s));
+    if (topk > 0)
+      CDK_CUDA(launch_topk_rescore(a, c->d_grids, topk, static_cast<TopPose*>(c->topk.base) + (size_t)waves * topk, s));
     if (prof) CDK_CUDA(cudaEventRecord(ev[4], s));
     CDK_CUDA(launch_finalize(a, s));
     if (prof) CDK_CUDA(cudaEventRecord(ev[5], s));
-    launches += kLaunchesPerWave + (streamed && !tmem_ligand ? 1 : 0);  // + k_tile_plan
+    launches += kLaunchesPerWave + (rows ? 1 : 0) + (tiebreak ? 1 : 0) + (topk > 0 ? 1 : 0);  // + k_tile_plan
     ++waves;
   }
   c->kev_used = prof ? (int)waves : 0;
+  c->topk_waves = topk > 0 ? (int)waves : 0;
   c->stats[0] = (double)launches;
   c->stats[1] = (double)waves;
   c->stats[2] = (double)nRot;
   c->stats[4] = (double)Lb;
   c->stats[5] = (double)wave;
-  c->stats[13] = streamed ? 4.0 : (double)a.col_tile;
-  c->stats[14] = streamed || umma ? 128.0 : (double)(a.chunk > 0 ? a.chunk : (tc ? 64 : 32));
-  c->stats[16] = f16 ? 5.0 : streamed ? (tmem_ligand ? 4.0 : 3.0) : umma ? 2.0 : tc ? 1.0 : 0.0;
+  c->stats[13] = hankel ? (double)hp.cols : streamed ? 4.0 : (double)a.col_tile;
+  c->stats[14] = rows || umma ? 128.0 : (double)(a.chunk > 0 ? a.chunk : (tc ? 64 : 32));
+  c->stats[16] = hankel ? (f16 ? 7.0 : 6.0) : streamed ? (f16 ? 5.0 : 3.0) : umma ? 2.0 : tc ? 1.0 : 0.0;
   c->stats[15] = (double)(c->gkey_seen);
   return CDK_OK;
 }
@@ -512,10 +545,13 @@ int check_errors_after(cdk_ctx* c, cudaStream_t s) {
   }
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, c->ev0, c->ev1) == cudaSuccess) c->stats[3] = ms;
-  CDK_CUDA(cudaMemcpy(c->h_work, c->d_work, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  CDK_CUDA(cudaMemcpy(c->h_work, c->d_work, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   c->stats[6] = (double)c->h_work[0];
   c->stats[7] = (double)c->h_work[1];
   c->stats[17] = (double)c->h_work[2];
+  c->stats[18] = (double)c->h_work[3];
+  c->stats[19] = (double)c->h_work[4];
+  c->stats[20] = (double)c->h_work[5];
   for (int k = 0; k < kLaunchesPerWave; ++k) c->stats[8 + k] = 0.0;
   for (int w = 0; w < c->kev_used; ++w) {
     cudaEvent_t* ev = &c->kev[(size_t)w * (kLaunchesPerWave + 1)];
@@ -556,6 +592,9 @@ bool ctx_view(const cdk_ctx* c, CtxView* v) {
   v->form = c->opts.form;
   v->tc_variant = c->opts.reserved[3];
   v->top = c->d_top;
+  v->ptilde = c->d_ptilde;
+  v->grids = c->d_grids;
+  v->tiebreak = c->opts.form != CDK_FORM_FP32 && c->opts.reserved[7] == 0;
   for (int k = 0; k < KMAX; ++k) v->lscale[k] = c->lscale[k];
   return true;
 }
@@ -669,8 +708,8 @@ int cdk_ctx_create(int nx, int ny, int nz, float spacing, int K, const float* gr
   CTX_CUDA(cudaMalloc(&c->d_tw, sizeof(float2) * n));
   CTX_CUDA(cudaMalloc(&c->d_misc, 8 * sizeof(unsigned int)));
   CTX_CUDA(cudaMallocHost(&c->h_misc, 8 * sizeof(unsigned int)));
-  CTX_CUDA(cudaMalloc(&c->d_work, 4 * sizeof(unsigned long long)));
-  CTX_CUDA(cudaMallocHost(&c->h_work, 4 * sizeof(unsigned long long)));
+  CTX_CUDA(cudaMalloc(&c->d_work, 8 * sizeof(unsigned long long)));
+  CTX_CUDA(cudaMallocHost(&c->h_work, 8 * sizeof(unsigned long long)));
   std::vector<float2> tw(n);
   for (int j = 0; j < n; ++j) {
     const double ang = -2.0 * M_PI * j / n;
@@ -742,6 +781,7 @@ int cdk_ctx_destroy(cdk_ctx* c) {
   cudaFree(c->tables.base);
   cudaFree(c->io.base);
   cudaFree(c->group.base);
+  cudaFree(c->topk.base);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -954,6 +994,30 @@ int cdk_sum_grids(const void* d_ligand_F, void* d_sum_F, int K, int odist, int i
   }
   CDK_CUDA(launch_sum_grids(static_cast<const float2*>(d_ligand_F), static_cast<float2*>(d_sum_F),
                             K, odist, idist, Q, static_cast<cudaStream_t>(stream)));
+  return CDK_OK;
+}
+
+int cdk_ctx_top_poses(cdk_ctx* c, int cap, int* rot, float* minE, int* idx, double* e64, int* count) {
+  if (!c || !count || cap < 0 || (cap > 0 && (!rot || !minE || !idx || !e64))) {
+    set_error("invalid argument");
+    return CDK_ERR_INVALID;
+  }
+  const int total = c->topk_k * c->topk_waves;
+  *count = total;
+  if (total == 0 || cap == 0) return CDK_OK;
+  CDK_CUDA(cudaSetDevice(c->dev));
+  std::vector<TopPose> h((size_t)total);
+  CDK_CUDA(cudaMemcpy(h.data(), c->topk.base, sizeof(TopPose) * total, cudaMemcpyDeviceToHost));
+  const int n = c->n;
+  for (int i = 0; i < total && i < cap; ++i) {
+    rot[i] = h[i].out;
+    minE[i] = h[i].e;
+    e64[i] = h[i].e64;
+    const int lin = h[i].lin;
+    idx[3 * i + 0] = lin < 0 ? -1 : lin / (n * n);
+    idx[3 * i + 1] = lin < 0 ? -1 : (lin / n) % n;
+    idx[3 * i + 2] = lin < 0 ? -1 : lin % n;
+  }
   return CDK_OK;
 }
 

@@ -75,12 +75,16 @@ struct WaveArgs {
                              // the x planes grouped by G, 16 B (two columns) per (plane, pair)
   int bgroup;                // 0 or 1: plain B layout; 2, 4, 8: grouped (streamed x pass only)
   unsigned long long* keys;  // [nrot]
+  unsigned long long* keys2; // precision forms' near-tie break: [nrot][n][2] the two smallest
+                             // keys of every window plane (null: not kept)
   const float2* phat;        // [n][K][ncol] (kx position-major)
   const float2* tw;          // [n]
   float* minE;               // output base (indexed by RotDesc.out)
   int* idx;
   int* err_count;
-  unsigned long long* work;  // [0] x planes spread, [1] window planes (work counters)
+  unsigned long long* work;  // work counters: [0] x planes spread, [1] window planes,
+                             // [2] tensor-core column K-steps, [3] MMA units, [4] near-tie
+                             // re-scores, [5] near-tie translations changed
   int col_tile;
   int chunk;                 // rotations per CTA in the x pass (0 = default)
   int* fault;                // set when a bounded device wait gave up
@@ -98,6 +102,19 @@ struct WaveArgs {
 
 // Launchers (stream-ordered, no synchronisation). Return cudaError_t of the launch.
 cudaError_t launch_prep(const WaveArgs& a, cudaStream_t s);
+// A wave's lowest-energy pose with its FP64 re-score (precision forms, per wave).
+constexpr int kTopMax = 32;
+struct TopPose {
+  int out;     // the rotation's output slot (RotDesc.out); -1: unused
+  int lin;     // kept translation, linear index (x * n + y) * n + z
+  float e;     // the search's energy there
+  int pad;
+  double e64;  // its FP64 direct grid-energy sum
+};
+cudaError_t launch_topk_rescore(const WaveArgs& a, const float* grids, int k, TopPose* out, cudaStream_t s);
+// FP64 near-tie break of the argmin over the planes' two smallest keys (a.keys2), before
+// launch_finalize; grids: the receptor grids [K][n][n][n]
+cudaError_t launch_tiebreak(const WaveArgs& a, const float* grids, float tol, cudaStream_t s);
 // rotation grouping for the tensor-core x pass (a stable counting sort of the rotation list on
 // which channels reach the ligand box's last 8-plane chunk); scratch of group_rotations_bytes
 size_t group_rotations_bytes(long nrot);
@@ -148,10 +165,25 @@ int stream_bgroup();
 // f16_scale: nullptr = the split-BF16 image; else the split-FP16 image of P~ * f16_scale[k]
 cudaError_t launch_top_build(int n, int K, const float2* pt, void* top, const float* f16_scale,
                              cudaStream_t s);
-// tmem_ligand: the ligand operand in tensor memory (k_xpass_tmema64), else in shared memory
-cudaError_t launch_xpass_stream(const WaveArgs& a, const void* top, bool tmem_ligand, cudaStream_t s);
+cudaError_t launch_xpass_stream(const WaveArgs& a, const void* top, cudaStream_t s);
 // true when launch_spread_yz takes the direct plane path (the only one that can write lop)
 bool direct_planes(const WaveArgs& a);
+
+// tcgen05 x pass with the Hankel operator resident in shared memory (any n, ligand box <= 32
+// planes): its shape for (n, K, box, form) and its launch (k_tile_plan, then the x pass)
+struct HankelPlan {
+  int cols;         // spectral columns per CTA (1 or 2)
+  int G;            // 128-byte groups of one Hankel buffer
+  int jc;           // 8-plane K-steps of the ligand box
+  int nb;           // ring stages
+  size_t smem;      // dynamic shared memory per CTA
+  int ctas_per_sm;  // 1 or 2
+};
+bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out);
+cudaError_t launch_xpass_hankel(const WaveArgs& a, const float2* pt, const float* f16_scale,
+                                const HankelPlan& p, cudaStream_t s);
+// the stage plan of every 128-rotation tile of a wave into the tile's first RotRec
+cudaError_t launch_tile_plan(const WaveArgs& a, int jc, cudaStream_t s);
 
 // Digit-reversed position of natural frequency k for the radix plan of length n.
 int fft_position(int n, int k);
@@ -174,6 +206,9 @@ struct CtxView {
   int form;              // CDK_FORM_*
   int tc_variant;        // opts.reserved[3]
   const void* top;       // operator image of the streamed tensor-core x pass (or null)
+  const float2* ptilde;  // precision forms: P~ [ncol][K][n], the Hankel x pass's operator source
+  const float* grids;    // receptor grids [K][n][n][n] (FP64 re-scores)
+  bool tiebreak;         // precision forms: FP64 near-tie break of the argmin
   float lscale[KMAX];    // split-FP16 form: ligand scale 2^sigma_k per channel
 };
 

@@ -1,0 +1,574 @@
+// hankel_xpass.cu -- the precision forms' x pass on tcgen05 with the operator resident in
+// shared memory (every grid size n in {32, 64, 96, 128}).
+//
+// For one spectral column c and channel k, the x-direction forward DFT, the conjugate product
+// with the receptor spectrum and the inverse DFT collapse into one circulant contraction
+//     B(x') = sum_x P~((x + x') mod n) L(x)              (P~: receptor over (y,z) only, x n)
+// with real outputs  Re B(x') = sum_x Re P~ Re L + Im P~ Im L
+// and  imaginary     Im B(x') = sum_x Im P~ Re L - Re P~ Im L.
+// Here the rotations are the MMA's M dimension (128 per tile, one TMEM lane each) and the
+// outputs x' its N dimension (N = the tile's largest window, rounded up to 16, so rows that no
+// rotation of the tile keeps are never computed). K = 16 per step: the real parts of one
+// 8-plane chunk of the ligand (K core matrix 0) and their imaginary parts (core matrix 1).
+//
+// The operator is a Hankel matrix in (x', x): entry P~(x + x'). For output group i (x' = 8i..
+// 8i+7) and K-step j (x = 8j..8j+7) its 8 x 8 core matrix is H[i + j], where
+//     H[g][r][d] = P~((8g + r + d) mod n)     (16-byte row r of 8 values d)
+// so one buffer of n/8 + jc - 1 such 128-byte groups holds every K-step's tile at once: the
+// shared-memory descriptor of K-step j starts at group j and steps 128 bytes per output group
+// (SBO = 128). Three buffers per (channel, hi/lo part) -- Re P~, Im P~ and -Re P~ -- give the
+// real-output operand (core matrices Re | Im: LBO = one buffer) and the imaginary-output operand
+// (Im | -Re). The whole column's operator (all channels, hi and lo) is built once per CTA from
+// P~ and stays resident: no operator bytes are streamed per tile.
+//
+// CTA = COLS columns, persistent over the wave's 128-rotation tiles; 288 threads:
+//   warps 0-3  producers: thread = rotation of the tile; per stage (one K-step of one channel,
+//              all COLS columns) 16-byte cp.async copies of its ligand rows (rows of chunks the
+//              rotation does not touch are zero-filled by the copy itself), then one
+//              cp.async-completion arrival on the stage's "full" mbarrier;
+//   warp 4     MMA issuer: one elected lane issues per stage and column 2 (real, imaginary) x
+//              2 (split-FP16: operator hi, lo) or x 3 (split-BF16: hi*hi, lo*hi, hi*lo) MMAs,
+//              commits each stage to its "empty" mbarrier and each tile to a TMEM "full"
+//              mbarrier;
+//   warps 5-8  epilogue: TMEM -> B of tile t while the MMAs of tile t+1 accumulate into the
+//              other of two TMEM accumulator sets (TMEM "empty" mbarrier per set).
+// Every wait is bounded; a wait that gives up sets the fault flag, the other roles stop at their
+// next wait, issued copies land and TMEM is freed.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "cdk_internal.h"
+
+namespace cdk {
+namespace {
+
+constexpr int HX_R = 128;               // rotations per tile (MMA M)
+constexpr int HX_THREADS = 288;         // 9 warps
+constexpr int HX_PRODUCERS = 128;       // warps 0-3
+constexpr int HX_MMA_WARP = 4;
+constexpr int HX_MAXSTAGES = 32;
+constexpr int HX_JMAX = 4;              // 8-plane chunks of the ligand box (Lb <= 32)
+constexpr uint32_t HX_CORE = 128;       // one 8 x 16-byte core matrix
+constexpr uint32_t HX_TILE = 16 * HX_CORE * 2;  // 4 KB: 128 rotations x K 16 (one part)
+constexpr long kWaitLimit = 1l << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// shared-memory matrix descriptor: K-major, no swizzle (LBO: K direction, SBO: M/N direction)
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const volatile int* stop) {
+  for (long i = 0; i < kWaitLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (i > 32) {
+      if (stop && *stop) return false;  // another role gave up: stop waiting
+      __nanosleep(40);
+    }
+  }
+  return false;
+}
+
+__device__ __forceinline__ bool elect_one() {
+  uint32_t pred = 0;
+  asm volatile(
+      "{\n\t.reg .pred P;\n\t"
+      "elect.sync _|P, 0xffffffff;\n\t"
+      "selp.b32 %0, 1, 0, P;\n\t}"
+      : "=r"(pred));
+  return pred != 0;
+}
+
+__device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      :
+      : "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// hi/lo parts of a value (16-bit patterns): split BF16, or split FP16 of a pre-scaled value
+template <bool F16>
+__device__ __forceinline__ void split16(float v, uint16_t& hi, uint16_t& lo) {
+  if constexpr (F16) {
+    const __half h = __float2half_rn(v);
+    const __half l = __float2half_rn(__fsub_rn(v, __half2float(h)));
+    hi = __half_as_ushort(h);
+    lo = __half_as_ushort(l);
+  } else {
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    const __nv_bfloat16 l = __float2bfloat16_rn(__fsub_rn(v, __bfloat162float(h)));
+    hi = __bfloat16_as_ushort(h);
+    lo = __bfloat16_as_ushort(l);
+  }
+}
+
+struct HxScale {
+  float s[KMAX];  // split-FP16 form: 2^-sigma_k per channel (the ligand rows carry 2^sigma_k)
+};
+
+// The tile's stage plan, read from its first rotation record (k_tile_plan): per active channel
+// 4 bits each of channel id, first and last K-step; the stage count, the channel count and the
+// largest window of the tile's valid rotations.
+struct TilePlan {
+  uint64_t pk, pl, ph;
+  int nact, steps, wmax;
+};
+
+__device__ __forceinline__ TilePlan load_plan(const RotRec* rec0) {
+  const uint4* tpv = reinterpret_cast<const uint4*>(rec0->tplan);
+  const uint4 t01 = tpv[0], t23 = tpv[1];
+  TilePlan p;
+  p.pk = ((uint64_t)t01.y << 32) | t01.x;
+  p.pl = ((uint64_t)t01.w << 32) | t01.z;
+  p.ph = ((uint64_t)t23.y << 32) | t23.x;
+  p.nact = (int)(t23.z & 0xFFFFu);
+  p.wmax = (int)(t23.z >> 16);
+  p.steps = (int)t23.w;
+  return p;
+}
+
+// N of the tile's MMAs: its largest window rounded up to 16 (M = 128 needs N % 16 == 0)
+__device__ __forceinline__ int tile_n(int wmax) { return max(16, (wmax + 15) & ~15); }
+
+template <bool F16>
+__device__ __forceinline__ uint32_t make_idesc(int n) {
+  // kind::f16: D f32 (bit 4), A/B BF16 (type 1 at bits 7, 10) or FP16 (type 0), both K-major,
+  // N >> 3 at bit 17, M >> 4 at bit 24
+  return (1u << 4) | (F16 ? 0u : ((1u << 7) | (1u << 10))) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(HX_R >> 4) << 24);
+}
+
+// Shared-memory plan of one CTA (bytes), shared by the kernel and its launcher.
+struct HxLayout {
+  uint32_t S;         // one Hankel buffer: G groups x 128 B
+  uint32_t op;        // the column operator: COLS x K x (hi, lo) x 3 buffers
+  uint32_t stage;     // one ring stage: COLS x LPARTS x 4 KB
+  uint32_t build;     // scratch of the operator build (inside the ring area)
+};
+
+__host__ __device__ inline HxLayout hx_layout(int n, int K, int cols, bool f16, int G) {
+  HxLayout L;
+  L.S = (uint32_t)G * HX_CORE;
+  L.op = (uint32_t)cols * K * 2 * 3 * L.S;
+  L.stage = (uint32_t)cols * (f16 ? 1 : 2) * HX_TILE;
+  // P~ of the CTA's columns (float2) + their four split arrays (re hi, re lo, im hi, im lo)
+  L.build = (uint32_t)cols * K * n * 8 + (uint32_t)cols * K * 4 * n * 2;
+  return L;
+}
+
+template <int N, int COLS, bool F16>
+__global__ void __launch_bounds__(HX_THREADS, 2)
+    k_xpass_hankel(WaveArgs a, const float2* __restrict__ pt, HxScale sc, int jc, int G, int nb) {
+  constexpr int NCOL = N * (N / 2 + 1);
+  constexpr int LPARTS = F16 ? 1 : 2;
+  constexpr int NMAX = N;                          // TMEM columns of one output block (re or im)
+  constexpr uint32_t DSET = (uint32_t)COLS * 2 * NMAX;  // one accumulator set
+  constexpr uint32_t TCOLS = (2 * DSET <= 32) ? 32 : (2 * DSET <= 64) ? 64 : (2 * DSET <= 128) ? 128
+                             : (2 * DSET <= 256) ? 256 : 512;
+  static_assert(2 * DSET <= 512, "two accumulator sets fit tensor memory");
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  __shared__ __align__(8) uint64_t s_full[HX_MAXSTAGES];
+  __shared__ __align__(8) uint64_t s_empty[HX_MAXSTAGES];
+  __shared__ __align__(8) uint64_t s_tfull[2];
+  __shared__ __align__(8) uint64_t s_tempty[2];
+  __shared__ volatile int s_fail;
+  __shared__ uint32_t s_tmem;
+  const int K = a.K;
+  const HxLayout L = hx_layout(N, K, COLS, F16, G);
+  unsigned char* op = base;              // resident operator
+  unsigned char* ring = base + L.op;     // ring stages (the operator build uses it first)
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int c0 = blockIdx.x * COLS;
+  const int ntiles = (a.nrot + HX_R - 1) / HX_R;
+
+  if (tid == 0) {
+    for (int b = 0; b < nb; ++b) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_full[b])), "r"(HX_PRODUCERS));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_empty[b])));
+    }
+    for (int d = 0; d < 2; ++d) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_tfull[d])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(smem_u32(&s_tempty[d])));
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_fail = 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(TCOLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+
+  // ---- operator build: P~ of the CTA's columns -> split arrays -> Hankel rows
+  {
+    float2* s_pt = reinterpret_cast<float2*>(ring);                           // [cols][K][N]
+    uint16_t* s_sp = reinterpret_cast<uint16_t*>(ring + (size_t)COLS * K * N * 8);  // [cols][K][4][N]
+    for (int i = tid; i < COLS * K * N; i += HX_THREADS) {
+      const int cc = i / (K * N), rem = i - cc * K * N;
+      s_pt[i] = pt[((size_t)(c0 + cc) * K) * N + rem];
+    }
+    __syncthreads();
+    for (int i = tid; i < COLS * K * N; i += HX_THREADS) {
+      const int k = (i / N) % K;
+      const float scale = F16 ? sc.s[k] : 1.f;
+      const float2 v = s_pt[i];
+      uint16_t h, l;
+      uint16_t* dst = s_sp + (size_t)(i / N) * 4 * N + (i % N);
+      split16<F16>(F16 ? __fmul_rn(v.x, scale) : v.x, h, l);
+      dst[0] = h;
+      dst[N] = l;
+      split16<F16>(F16 ? __fmul_rn(v.y, scale) : v.y, h, l);
+      dst[2 * N] = h;
+      dst[3 * N] = l;
+    }
+    __syncthreads();
+    // rows: [cc][k][hl][buf (Re, Im, -Re)][g][r] x 16 B, H[g][r][d] = P~((8g + r + d) mod N);
+    // -Re is the negated Re split (negation is exact)
+    const int rows = COLS * K * 2 * 3 * G * 8;
+    for (int i = tid; i < rows; i += HX_THREADS) {
+      const int r = i & 7;
+      const int g = (i >> 3) % G;
+      const int t = (i >> 3) / G;  // ((cc * K + k) * 2 + hl) * 3 + buf
+      const int buf = t % 3, hl = (t / 3) & 1, ck = t / 6;
+      const uint16_t* src = s_sp + (size_t)ck * 4 * N + (size_t)((buf == 1 ? 2 : 0) + hl) * N;
+      const uint16_t neg = buf == 2 ? 0x8000u : 0u;
+      uint32_t w[4];
+#pragma unroll
+      for (int d = 0; d < 8; d += 2) {
+        const uint32_t e0 = src[(8 * g + r + d) % N] ^ neg, e1 = src[(8 * g + r + d + 1) % N] ^ neg;
+        w[d / 2] = e0 | (e1 << 16);
+      }
+      *reinterpret_cast<uint4*>(op + (size_t)i * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    // the rows are read by the tensor cores (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = s_tmem;
+  const uint32_t ring_s = smem_u32(ring);
+  const uint32_t op_s = smem_u32(op);
+
+  if (warp < HX_PRODUCERS / 32) {
+    // ---- producers
+    const int rr = tid;
+    const uint32_t row_s = (uint32_t)(rr >> 3) * HX_CORE + (uint32_t)(rr & 7) * 16;
+    constexpr size_t RS = (size_t)(NCOL / 4) * 32;  // one ligand row (16 B units)
+    constexpr int ROWS = 8 * LPARTS;                // rows per (rotation, channel)
+    int s = 0;
+    for (int t = 0; t < ntiles; ++t) {
+      const int r0 = t * HX_R;
+      const int nr = min(HX_R, a.nrot - r0);
+      const TilePlan p = load_plan(a.rec + r0);
+      if (p.steps == 0) continue;
+      const RotRec* rec = a.rec + r0 + min(rr, nr - 1);
+      const bool live = rr < nr && rec->valid;
+      // this rotation's chunk range per channel, 8 bits each (0x0F: none)
+      uint64_t jr_lo = 0, jr_hi = 0;
+      {
+        uint4 v[4];
+        const uint4* xr = reinterpret_cast<const uint4*>(rec->xlo);  // xlo[16] then xhi[16]
+#pragma unroll
+        for (int i = 0; i < 4; ++i) v[i] = xr[i];
+        const short* lo16 = reinterpret_cast<const short*>(&v[0]);
+        const short* hi16 = reinterpret_cast<const short*>(&v[2]);
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) {
+          uint64_t e = 0x0F;
+          const int lo = live ? lo16[k] : 1, hi = live ? hi16[k] : 0;
+          if (k < K && lo <= hi) e = (uint64_t)(min(lo >> 3, jc - 1) | (min(hi >> 3, jc - 1) << 4));
+          if (k < 8) jr_lo |= e << (8 * k);
+          else jr_hi |= e << (8 * (k - 8));
+        }
+      }
+      const int rg = r0 + (rr < nr ? rr : 0);
+      const size_t rot_rows = (size_t)(rg >> 3) * K * ROWS * RS + (size_t)(c0 >> 2) * 32 + (rg & 7) * 4 + (c0 & 3);
+      bool ok = true;
+      for (int ai = 0; ai < p.nact && ok; ++ai) {
+        const int k = (int)((p.pk >> (4 * ai)) & 15);
+        const int jlo = (int)((p.pl >> (4 * ai)) & 15), jhi = (int)((p.ph >> (4 * ai)) & 15);
+        const unsigned int jr = (unsigned int)(((k < 8 ? jr_lo : jr_hi) >> (8 * (k & 7))) & 255);
+        const int jl = (int)(jr & 15), jh = (int)(jr >> 4);
+        const uint4* src0 = reinterpret_cast<const uint4*>(a.lop) + rot_rows + (size_t)k * ROWS * RS;
+        for (int j = jlo; j <= jhi; ++j, ++s) {
+          const int b = s % nb;
+          if (s >= nb && !mbar_wait(smem_u32(&s_empty[b]), (uint32_t)((s / nb) - 1) & 1u, &s_fail)) {
+            s_fail = 1;
+            ok = false;
+            break;
+          }
+          const uint32_t st = ring_s + (uint32_t)b * L.stage;
+          const bool have = jl <= j && j <= jh;
+#pragma unroll
+          for (int cc = 0; cc < COLS; ++cc)
+#pragma unroll
+            for (int hl = 0; hl < LPARTS; ++hl)
+#pragma unroll
+              for (int part = 0; part < 2; ++part) {
+                const uint4* src = src0 + (size_t)((hl * 4 + j) * 2 + part) * RS + cc;
+                const uint32_t dst = st + (uint32_t)(cc * LPARTS + hl) * HX_TILE + (uint32_t)part * (HX_TILE / 2) + row_s;
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(have ? 16 : 0)
+                             : "memory");
+              }
+          asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&s_full[b])) : "memory");
+        }
+      }
+      if (!ok) break;
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  } else if (warp == HX_MMA_WARP) {
+    // ---- MMA issuer: the whole warp runs the loop (uniform descriptors), one lane issues
+    int s = 0, u = 0;
+    bool good = true;
+    for (int t = 0; t < ntiles && good; ++t) {
+      const TilePlan p = load_plan(a.rec + t * HX_R);
+      if (p.steps == 0) continue;
+      const int d = u & 1;
+      if (u >= 2 && !__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_tempty[d]), (uint32_t)((u >> 1) - 1) & 1u, &s_fail))) {
+        if (lane == 0) s_fail = 1;
+        good = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int nt = tile_n(p.wmax);
+      const uint32_t idesc = make_idesc<F16>(nt);
+      const uint32_t dset = tmem + (uint32_t)d * DSET;
+      bool first = true;
+      for (int ai = 0; ai < p.nact && good; ++ai) {
+        const int k = (int)((p.pk >> (4 * ai)) & 15);
+        const int jlo = (int)((p.pl >> (4 * ai)) & 15), jhi = (int)((p.ph >> (4 * ai)) & 15);
+        for (int j = jlo; j <= jhi; ++j, ++s) {
+          const int b = s % nb;
+          if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_full[b]), (uint32_t)(s / nb) & 1u, &s_fail))) {
+            if (lane == 0) s_fail = 1;
+            good = false;
+            break;
+          }
+          // the producers' cp.async writes (generic proxy) reach the tensor core (async proxy)
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t acc0 = first ? 0u : 1u;
+#pragma unroll
+          for (int cc = 0; cc < COLS; ++cc) {
+            const uint32_t st = ring_s + (uint32_t)b * L.stage + (uint32_t)(cc * LPARTS) * HX_TILE;
+            const uint64_t ahi = make_desc(st, HX_TILE / 2, HX_CORE);
+            const uint32_t obase = op_s + (uint32_t)(((cc * K + k) * 2) * 3) * L.S + (uint32_t)j * HX_CORE;
+            const uint64_t bre_hi = make_desc(obase, L.S, HX_CORE);          // Re | Im
+            const uint64_t bim_hi = make_desc(obase + L.S, L.S, HX_CORE);    // Im | -Re
+            const uint64_t bre_lo = make_desc(obase + 3 * L.S, L.S, HX_CORE);
+            const uint64_t bim_lo = make_desc(obase + 4 * L.S, L.S, HX_CORE);
+            const uint32_t dre = dset + (uint32_t)(cc * 2 * NMAX), dim = dre + NMAX;
+            if (elect_one()) umma(dre, ahi, bre_hi, idesc, acc0);
+            if (elect_one()) umma(dim, ahi, bim_hi, idesc, acc0);
+            if constexpr (!F16) {
+              const uint64_t alo = make_desc(st + HX_TILE, HX_TILE / 2, HX_CORE);
+              if (elect_one()) umma(dre, alo, bre_hi, idesc, 1u);
+              if (elect_one()) umma(dim, alo, bim_hi, idesc, 1u);
+            }
+            if (elect_one()) umma(dre, ahi, bre_lo, idesc, 1u);
+            if (elect_one()) umma(dim, ahi, bim_lo, idesc, 1u);
+          }
+          if (elect_one()) umma_commit(smem_u32(&s_empty[b]));
+          __syncwarp();
+          first = false;
+        }
+      }
+      if (!good) break;
+      if (elect_one()) umma_commit(smem_u32(&s_tfull[d]));
+      __syncwarp();
+      if (lane == 0 && a.work) {
+        // column K-steps, and the issued MMA work in units of 128 x 8 x 16 multiply-adds
+        atomicAdd(a.work + 2, (unsigned long long)p.steps * COLS);
+        atomicAdd(a.work + 3, (unsigned long long)p.steps * COLS * 2 * (F16 ? 2 : 3) * (nt >> 3));
+      }
+      ++u;
+    }
+    // the newest commit completes after every earlier MMA of this warp
+    if (lane == 0 && s > 0 && !mbar_wait(smem_u32(&s_empty[(s - 1) % nb]), (uint32_t)((s - 1) / nb) & 1u, nullptr))
+      s_fail = 1;
+    __syncwarp();
+  } else {
+    // ---- epilogue: TMEM lane quarter q = rotations 32 q .. 32 q + 31
+    const int q = warp & 3;
+    const int rl = 32 * q + lane;
+    const int G2 = a.bgroup > 1 ? a.bgroup : 1;
+    int u = 0;
+    for (int t = 0; t < ntiles; ++t) {
+      const int r0 = t * HX_R;
+      const int nr = min(HX_R, a.nrot - r0);
+      const TilePlan p = load_plan(a.rec + r0);
+      if (p.steps == 0) continue;
+      const int d = u & 1;
+      if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_tfull[d]), (uint32_t)(u >> 1) & 1u, &s_fail))) {
+        if (lane == 0) s_fail = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int nt = tile_n(p.wmax);
+      const RotRec* rec = a.rec + r0 + min(rl, nr - 1);
+      const int Wr = (rl < nr && rec->valid) ? rec->W[0] : 0;
+      float4* rowp = reinterpret_cast<float4*>(a.B + (size_t)(r0 + min(rl, nr - 1)) * N * NCOL);
+      const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)d * DSET;
+      for (int x0 = 0; x0 < nt; x0 += 16) {
+        float re[COLS][16], im[COLS][16];
+#pragma unroll
+        for (int cc = 0; cc < COLS; ++cc) {
+          tmem_ld16(tbase + (uint32_t)(cc * 2 * NMAX + x0), re[cc]);
+          tmem_ld16(tbase + (uint32_t)(cc * 2 * NMAX + NMAX + x0), im[cc]);
+        }
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int xp = x0 + i;
+          if (xp < Wr) {
+            // plane-group layout of B: float4 (re, im of column pair 2m, 2m + 1) at
+            // (xp - xp % G) NCOL / 2 + m G + xp % G
+            const size_t f4 = (size_t)(xp - xp % G2) * (NCOL / 2) + (size_t)(c0 >> 1) * G2 + xp % G2;
+            if constexpr (COLS == 2) {
+              rowp[f4] = make_float4(re[0][i], im[0][i], re[1][i], im[1][i]);
+            } else {
+              reinterpret_cast<float2*>(rowp + f4)[c0 & 1] = make_float2(re[0][i], im[0][i]);
+            }
+          }
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&s_tempty[d])) : "memory");
+      ++u;
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (tid == 0 && s_fail) atomicOr(a.fault, 1);
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS));
+  }
+}
+
+constexpr size_t kSmemCap = 227 * 1024;   // dynamic shared memory of one CTA
+constexpr size_t kSmemHalf = 110 * 1024;  // per CTA when two share an SM
+
+template <int N, int COLS, bool F16>
+cudaError_t launch_hx(const WaveArgs& a, const float2* pt, const HxScale& sc, int jc, int G, int nb,
+                      size_t smem, cudaStream_t s) {
+  constexpr int NCOL = N * (N / 2 + 1);
+  auto kern = k_xpass_hankel<N, COLS, F16>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  kern<<<NCOL / COLS, HX_THREADS, smem, s>>>(a, pt, sc, jc, G, nb);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+// Shape of the x pass for (n, K, ligand box, form): columns per CTA, Hankel groups, ring stages
+// and dynamic shared memory. cols_pref: 0 = automatic, 1 or 2 = that many columns (2 only where
+// the operator of two columns fits). Returns false when the operator and a minimal ring do not
+// fit one CTA (large K at large n) or the box exceeds 32 planes.
+bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out) {
+  if (!(n == 32 || n == 64 || n == 96 || n == 128) || K < 1 || K > KMAX || Lb < 1 || Lb > 8 * HX_JMAX)
+    return false;
+  const int jc = (Lb + 7) / 8;
+  const int G = n / 8 + jc - 1;
+  for (int cols : {2, 1}) {
+    if (cols_pref && cols != cols_pref) continue;
+    if (cols == 2 && n > 64) continue;  // the tensor memory of two double-buffered columns
+    const HxLayout L = hx_layout(n, K, cols, f16, G);
+    // two CTAs per SM when the tensor memory allows (<= 256 columns each) and the operator
+    // leaves room for a ring of at least 8 stages; else one CTA with the largest ring
+    const bool two = 2 * 2 * cols * n <= 256;
+    for (int pass = two ? 0 : 1; pass < 2; ++pass) {
+      const size_t cap = (pass == 0 ? kSmemHalf : kSmemCap) - 1024;
+      if (cap <= L.op) continue;
+      const int nb = (int)std::min<size_t>(HX_MAXSTAGES, (cap - L.op) / L.stage);
+      if (nb < (pass == 0 ? 8 : 4) || (size_t)nb * L.stage < L.build) continue;
+      out->cols = cols;
+      out->G = G;
+      out->jc = jc;
+      out->nb = nb;
+      out->smem = (size_t)L.op + (size_t)nb * L.stage + 1024;
+      // a CTA that takes all 512 tensor-memory columns must have its SM alone: its shared
+      // memory then keeps a second CTA out (tcgen05.alloc would otherwise stall it)
+      if (pass == 1) out->smem = std::max(out->smem, (size_t)120 * 1024);
+      out->ctas_per_sm = pass == 0 ? 2 : 1;
+      return true;
+    }
+  }
+  return false;
+}
+
+cudaError_t launch_xpass_hankel(const WaveArgs& a, const float2* pt, const float* f16_scale,
+                                const HankelPlan& p, cudaStream_t s) {
+  if (!a.lop || !pt || a.K > KMAX) return cudaErrorInvalidValue;
+  HxScale sc{};
+  for (int k = 0; k < a.K; ++k) sc.s[k] = (a.f16 && f16_scale) ? f16_scale[k] : 1.f;
+  // the stage plan of every 128-rotation tile (channels, K-steps, largest window)
+  cudaError_t e = launch_tile_plan(a, p.jc, s);
+  if (e != cudaSuccess) return e;
+#define CDK_HX(NN)                                                                               \
+  case NN:                                                                                       \
+    if (a.f16) return p.cols == 2 ? launch_hx<NN, (NN <= 64 ? 2 : 1), true>(a, pt, sc, p.jc, p.G, p.nb, p.smem, s) \
+                                  : launch_hx<NN, 1, true>(a, pt, sc, p.jc, p.G, p.nb, p.smem, s);             \
+    return p.cols == 2 ? launch_hx<NN, (NN <= 64 ? 2 : 1), false>(a, pt, sc, p.jc, p.G, p.nb, p.smem, s)       \
+                       : launch_hx<NN, 1, false>(a, pt, sc, p.jc, p.G, p.nb, p.smem, s);
+  switch (a.n) {
+    CDK_HX(32)
+    CDK_HX(64)
+    CDK_HX(96)
+    CDK_HX(128)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef CDK_HX
+}
+
+}  // namespace cdk

@@ -342,6 +342,18 @@ int cdk_pose_coordinates(int nAtom, const float* coor, const float* quat, const 
   return CDK_OK;
 }
 
+// sort_index over float minima (include/GeneDiverseConformations.h:9-20): std::sort of the
+// indices with strict <, so ties come out in the order the reference's own call leaves them.
+int cdk_sort_index(const float* v, long n, long* out) {
+  if (n < 0 || (n > 0 && (!v || !out))) {
+    set_error("invalid argument");
+    return CDK_ERR_INVALID;
+  }
+  const std::vector<size_t> id = sort_index(std::vector<float>(v, v + n));
+  for (long i = 0; i < n; ++i) out[i] = (long)id[i];
+  return CDK_OK;
+}
+
 int cdk_quaternion_uniform_sampling(uint64_t seed, int nConf, int nQ, float* out) {
   if (!out || nConf < 0 || nQ < 0) {
     set_error("invalid argument");

@@ -1,20 +1,26 @@
 // noalloc.cu -- a search entry point that allocates no device memory.
 //
-// Some callers cannot call cudaMalloc at the time they search: code that records the search
-// into a CUDA graph (allocation is not allowed while a stream is being captured), real-time
-// loops that must not hit the allocator's device-wide synchronisation, and hosts whose memory
-// is owned by a pool that forbids outside allocations. cdk_search_device grows its wave and
-// table scratch with cudaMalloc on demand; cdk_search_device_noalloc runs the same kernels
-// with all of that scratch carved from one file-scope device array of fixed size instead.
+// Some callers cannot let a library call cudaMalloc while they search: real-time loops that
+// must not hit the allocator (cudaMalloc and cudaFree can synchronise the whole device and
+// take unbounded time), and hosts whose device memory is owned by a pool or arena that
+// forbids outside allocations. cdk_search_device grows its wave and table scratch with
+// cudaMalloc on demand; cdk_search_device_noalloc runs the same FP32-form kernels with all of
+// that scratch carved from one file-scope device array of fixed size instead.
 //
 // Limits and sharing rules:
+//  * FP32-form contexts only. The tensor-core forms need an operator image that the context
+//    builds with cudaMalloc on first use; a precision-form context is rejected with
+//    CDK_ERR_UNSUPPORTED instead of silently searching in another form.
 //  * g_noalloc_scratch is CDK_NOALLOC_SCRATCH_BYTES (64 MiB). Every GPU that loads this
 //    library holds it until the process exits. A call splits its rotations into waves that
 //    fit the array; a search whose single rotation does not fit (very large grid x ligand
 //    box) is rejected with CDK_ERR_UNSUPPORTED.
 //  * Host code cannot use the array's name as a device address. The first call on each
 //    device, with that device current, looks the address up with cudaGetSymbolAddress and
-//    caches it; make that first call before any stream capture begins.
+//    caches it for the life of the process. The cache does not survive cudaDeviceReset (or
+//    any teardown of the device's primary context): do not call this entry point after one.
+//  * The call synchronises its stream twice (to read back the ligand-box plan and, at the
+//    end, the overflow count), so it cannot be recorded into a CUDA graph.
 //  * All calls share the array and it keeps the previous call's contents. The counters the
 //    search relies on are cleared at the start of every call; everything else is written
 //    before it is read. Calls that overlap on the GPU (two streams, two host threads) race on
@@ -139,6 +145,11 @@ extern "C" int cdk_search_device_noalloc(cdk_ctx* ctx, int nAtom, int nConf,
   if (nRot > (1l << 31) / 4) {
     set_error("too many rotations in one call");
     return CDK_ERR_INVALID;
+  }
+  if (v.form != CDK_FORM_FP32) {
+    set_error("cdk_search_device_noalloc runs the FP32 form only; this context uses a "
+              "tensor-core form (use cdk_search_device)");
+    return CDK_ERR_UNSUPPORTED;
   }
   NA_CUDA(cudaSetDevice(v.dev));
   void* base = nullptr;

@@ -143,15 +143,21 @@ __global__ void __launch_bounds__(128) k_prep(WaveArgs a) {
     for (int d = 0; d < 3; ++d) atomicMax(&s_ext[warp][d], ci[d] + 2);
   }
   __syncwarp();
-  if (a.f16 && lane < a.K && a.range_err) {
+  bool range_bad = false;
+  if (a.f16 && a.range_err) {
     // split-FP16 form: |A(x, ky, kz)| <= sum over the channel's atoms of |s_a| (x weights and
     // |Fy|, |Fz| are at most 1), so the scaled ligand rows fit FP16 when this bound does
-    float bound = 0.f;
-    for (int i = 0; i < nA; ++i) {
-      if (lane == elec) bound += fabsf(prm[i].charge);
-      else if (prm[i].slot == lane) bound += fabsf(prm[i].w_vdw);
+    bool bad = false;
+    if (lane < a.K) {
+      float bound = 0.f;
+      for (int i = 0; i < nA; ++i) {
+        if (lane == elec) bound += fabsf(prm[i].charge);
+        else if (prm[i].slot == lane) bound += fabsf(prm[i].w_vdw);
+      }
+      bad = bound * a.lscale[lane] > 60000.f;
     }
-    if (bound * a.lscale[lane] > 60000.f) atomicOr(a.range_err, 1);
+    range_bad = __any_sync(0xffffffffu, bad);
+    if (range_bad && lane == 0) atomicOr(a.range_err, 1);
   }
   RotRec* rec = a.rec + r;
   if (lane < KMAX) {
@@ -160,10 +166,14 @@ __global__ void __launch_bounds__(128) k_prep(WaveArgs a) {
     rec->xhi[lane] = used ? (short)s_hi[warp][lane] : (short)0;
   }
   if (lane == 0) {
+    // err 1: the x planes of a channel leave the planned box, or y/z cells the grid;
+    // err 2: a scaled ligand value would leave the FP16 range (split-FP16 form). Either makes
+    // the rotation invalid (no kernel after this one touches it)
     int err = 0;
-    // the x planes of every channel must fit the planned box, y/z cells the grid
     if (valid && (s_ext[warp][0] - 1 >= a.Lb || s_ext[warp][1] > a.n || s_ext[warp][2] > a.n))
       err = 1;
+    else if (valid && range_bad)
+      err = 2;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       rec->mn[d] = mn[d];
@@ -674,8 +684,28 @@ __global__ void __launch_bounds__(256, 2) k_xpass2(WaveArgs a, int rot_per_cta) 
 }
 
 // ---------------------------------------------------------------------------------------
-// inverse (y,z) of one (rotation, x in window) plane + min / first argmin
-template <int N>
+// keep the two smallest keys (b1 < b2) of a stream of distinct keys
+__device__ __forceinline__ void top2_insert(unsigned long long k, unsigned long long& b1, unsigned long long& b2) {
+  if (k < b1) {
+    b2 = b1;
+    b1 = k;
+  } else if (k < b2) {
+    b2 = k;
+  }
+}
+// merge another pair of two smallest into (b1, b2)
+__device__ __forceinline__ void top2_merge(unsigned long long o1, unsigned long long o2, unsigned long long& b1,
+                                           unsigned long long& b2) {
+  const unsigned long long n1 = o1 < b1 ? o1 : b1;
+  const unsigned long long hi = o1 < b1 ? b1 : o1;
+  const unsigned long long lo2 = o2 < b2 ? o2 : b2;
+  b2 = hi < lo2 ? hi : lo2;
+  b1 = n1;
+}
+
+// inverse (y,z) of one (rotation, x in window) plane + min / first argmin; TOP2: also the
+// plane's second-smallest key, for the FP64 near-tie break (WaveArgs.keys2)
+template <int N, bool TOP2>
 __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveArgs a) {
   constexpr int NZH = N / 2 + 1;
   constexpr int NCOL = N * NZH;
@@ -688,7 +718,7 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
   constexpr bool ALIAS = N <= 64;
   float2* P = ALIAS ? O : O + N * NZH;
   static_assert((N / 2) * (N + 1) <= N * NZH, "packed rows fit the plane buffer");
-  __shared__ unsigned long long s_best[8];
+  __shared__ unsigned long long s_best[8], s_best2[8];
   const int x = blockIdx.x, r = blockIdx.y;
   const RotRec* rec = a.rec + r;
   if (!rec->valid) return;
@@ -732,7 +762,7 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
   }
   const int npairs = (Wy + 1) / 2;
   const float inv = 1.0f / (float)((double)N * N * N);
-  unsigned long long best = ~0ull;
+  unsigned long long best = ~0ull, best2 = ~0ull;
   if constexpr (ALIAS) {
     // Rows (2p, 2p+1) as one complex line Z_p(k) = Y(2p, k) + i Y(2p+1, k) with the Hermitian
     // extension over z, inverse-transformed in two radix stages (N = R0 R1), one work item per
@@ -801,8 +831,13 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
               ((unsigned long long)order_key(v[j].x * inv) << 32) | (lin0 + (unsigned int)(R1 * j));
           const unsigned long long k1 =
               ((unsigned long long)order_key(v[j].y * inv) << 32) | (lin0 + (unsigned int)(N + R1 * j));
-          if (row0) best = k0 < best ? k0 : best;
-          if (row1) best = k1 < best ? k1 : best;
+          if constexpr (TOP2) {
+            if (row0) top2_insert(k0, best, best2);
+            if (row1) top2_insert(k1, best, best2);
+          } else {
+            if (row0) best = k0 < best ? k0 : best;
+            if (row1) best = k1 < best ? k1 : best;
+          }
         }
       }
     }
@@ -838,20 +873,179 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
         const float e = ((y & 1) ? v.y : v.x) * inv;
         const unsigned int lin = (unsigned int)((x * N + y) * N + z);
         const unsigned long long key = ((unsigned long long)order_key(e) << 32) | lin;
-        best = key < best ? key : best;
+        if constexpr (TOP2) top2_insert(key, best, best2);
+        else best = key < best ? key : best;
       }
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
-    unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
-    best = other < best ? other : best;
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
+    if constexpr (TOP2) {
+      const unsigned long long other2 = __shfl_xor_sync(0xffffffffu, best2, o);
+      top2_merge(other, other2, best, best2);
+    } else {
+      best = other < best ? other : best;
+    }
   }
-  if ((tid & 31) == 0) s_best[tid >> 5] = best;
+  if ((tid & 31) == 0) {
+    s_best[tid >> 5] = best;
+    if constexpr (TOP2) s_best2[tid >> 5] = best2;
+  }
   __syncthreads();
   if (tid == 0) {
-    for (int w = 1; w < (nthr >> 5); ++w) best = s_best[w] < best ? s_best[w] : best;
-    best = s_best[0] < best ? s_best[0] : best;
+    for (int w = 1; w < (nthr >> 5); ++w) {
+      if constexpr (TOP2) top2_merge(s_best[w], s_best2[w], best, best2);
+      else best = s_best[w] < best ? s_best[w] : best;
+    }
     atomicMin(a.keys + r, best);
+    if constexpr (TOP2) {
+      a.keys2[((size_t)r * N + x) * 2] = best;
+      a.keys2[((size_t)r * N + x) * 2 + 1] = best2;
+    }
+  }
+}
+
+// FP64 energy of rotation r at translation (ti, tj, tk): the direct trilinear grid-energy sum
+// over its rotated atoms (k_prep's rot_xyz and min corner), cells and ratios in
+// FillLigandGrid's arithmetic, accumulated in double across the warp's lanes (atoms).
+__device__ double pose_energy_fp64(const WaveArgs& a, const float* grids, int r, int ti, int tj, int tk,
+                                   int lane) {
+  const RotRec* rec = a.rec + r;
+  const RotDesc rd = a.rots[r];
+  const ConfDesc cd = a.confs[rd.conf];
+  const AtomParam* prm = a.params + cd.param_off;
+  const int n = a.n, K = a.K;
+  const size_t Ng = (size_t)n * n * n;
+  const float h = a.spacing;
+  double e = 0.0;
+  for (int i = lane; i < rec->nA; i += 32) {
+    const float4 p4 = a.rot_xyz[(size_t)r * a.max_atoms + i];
+    const float p[3] = {p4.x, p4.y, p4.z};
+    int ci[3];
+    double rr[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      ci[d] = cell_of(p[d], rec->mn[d], h);
+      rr[d] = ratio_of(p[d], rec->mn[d], h, ci[d]);
+    }
+    const AtomParam ap = prm[i];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int dx = (c >> 2) & 1, dy = (c >> 1) & 1, dz = c & 1;
+      const int gx = ci[0] + dx + ti, gy = ci[1] + dy + tj, gz = ci[2] + dz + tk;
+      if (gx >= n || gy >= n || gz >= n) continue;
+      const double w = (dx ? rr[0] : 1.0 - rr[0]) * (dy ? rr[1] : 1.0 - rr[1]) * (dz ? rr[2] : 1.0 - rr[2]);
+      const size_t g = ((size_t)gx * n + gy) * n + gz;
+      if (ap.slot >= 0 && ap.slot < K - 1) e += (double)ap.w_vdw * w * (double)grids[(size_t)ap.slot * Ng + g];
+      e += (double)ap.charge * w * (double)grids[(size_t)(K - 1) * Ng + g];
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+  return e;
+}
+
+// FP64 near-tie break of the argmin (precision forms), warp per rotation: the two smallest keys
+// over the rotation's window planes; when the second energy lies within tol * max(|E1|, 1) of
+// the first, both translations are re-scored in FP64 (pose_energy_fp64) and the lower one is
+// kept -- the smaller linear index (x-major first) on an exact FP64 tie. The reported energy
+// stays the search's own value at the kept translation. work[4] counts re-scored rotations,
+// work[5] the ones whose translation changed.
+__global__ void __launch_bounds__(128) k_tiebreak(WaveArgs a, const float* __restrict__ grids, float tol) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = blockIdx.x * 4 + warp;
+  if (r >= a.nrot) return;
+  const RotRec* rec = a.rec + r;
+  if (!rec->valid) return;
+  const int n = a.n;
+  unsigned long long b1 = ~0ull, b2 = ~0ull;
+  for (int x = lane; x < rec->W[0]; x += 32)
+    top2_merge(a.keys2[((size_t)r * n + x) * 2], a.keys2[((size_t)r * n + x) * 2 + 1], b1, b2);
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long o1 = __shfl_xor_sync(0xffffffffu, b1, o);
+    const unsigned long long o2 = __shfl_xor_sync(0xffffffffu, b2, o);
+    top2_merge(o1, o2, b1, b2);
+  }
+  if (b1 == ~0ull || b2 == ~0ull) return;
+  const float e1 = key_to_float((unsigned int)(b1 >> 32)), e2 = key_to_float((unsigned int)(b2 >> 32));
+  if (!(e2 - e1 <= tol * fmaxf(fabsf(e1), 1.f))) return;
+  const unsigned int l1 = (unsigned int)b1, l2 = (unsigned int)b2;
+  const double f1 = pose_energy_fp64(a, grids, r, l1 / (n * n), (l1 / n) % n, l1 % n, lane);
+  const double f2 = pose_energy_fp64(a, grids, r, l2 / (n * n), (l2 / n) % n, l2 % n, lane);
+  if (lane == 0) {
+    const bool flip = f2 < f1 || (f2 == f1 && l2 < l1);
+    if (flip) a.keys[r] = b2;
+    if (a.work) {
+      atomicAdd(a.work + 4, 1ull);
+      if (flip) atomicAdd(a.work + 5, 1ull);
+    }
+  }
+}
+
+// FP64 re-score of the k lowest-energy poses of a wave (precision forms), one CTA: the k
+// smallest final keys (energy, then the rotation's place in the wave) by k rounds of a block
+// minimum over each thread's own sorted candidates, then one warp per pose for its FP64 direct
+// grid-energy sum at its kept translation. out[j]: the rotation's output slot, the search's
+// energy, its translation's linear index and the FP64 energy; unused slots get out = -1.
+__global__ void __launch_bounds__(256) k_topk_rescore(WaveArgs a, const float* __restrict__ grids, int k,
+                                                      TopPose* __restrict__ out) {
+  __shared__ unsigned long long s_min[8];
+  __shared__ unsigned long long s_pick[kTopMax];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // per thread: its kTopMax smallest (energy bits, rotation) keys, ascending
+  unsigned long long cand[kTopMax];
+#pragma unroll
+  for (int j = 0; j < kTopMax; ++j) cand[j] = ~0ull;
+  for (int r = tid; r < a.nrot; r += blockDim.x) {
+    const RotRec* rec = a.rec + r;
+    const unsigned long long key = a.keys[r];
+    if (!rec->valid || key == ~0ull) continue;
+    unsigned long long c = (key & 0xffffffff00000000ull) | (unsigned int)r;
+#pragma unroll
+    for (int j = 0; j < kTopMax; ++j) {
+      const unsigned long long lo = c < cand[j] ? c : cand[j];
+      c = c < cand[j] ? cand[j] : c;
+      cand[j] = lo;
+    }
+  }
+  int head = 0;
+  for (int j = 0; j < k; ++j) {
+    unsigned long long m = head < kTopMax ? cand[0] : ~0ull;
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long v = __shfl_xor_sync(0xffffffffu, m, o);
+      m = v < m ? v : m;
+    }
+    if (lane == 0) s_min[warp] = m;
+    __syncthreads();
+    unsigned long long g = s_min[0];
+    for (int w = 1; w < 8; ++w) g = s_min[w] < g ? s_min[w] : g;
+    if (tid == 0) s_pick[j] = g;
+    // the owner pops its head (keys are unique: one rotation each)
+    if (g != ~0ull && cand[0] == g) {
+#pragma unroll
+      for (int q = 0; q + 1 < kTopMax; ++q) cand[q] = cand[q + 1];
+      cand[kTopMax - 1] = ~0ull;
+      ++head;
+    }
+    __syncthreads();
+  }
+  for (int j = warp; j < k; j += 8) {
+    const unsigned long long g = s_pick[j];
+    TopPose tp;
+    tp.out = -1;
+    tp.lin = -1;
+    tp.e = INFINITY;
+    tp.e64 = 0.0;
+    if (g != ~0ull) {
+      const int r = (int)(unsigned int)g;
+      const unsigned int lin = (unsigned int)a.keys[r];
+      const int n = a.n;
+      const double e64 = pose_energy_fp64(a, grids, r, lin / (n * n), (lin / n) % n, lin % n, lane);
+      tp.out = a.rots[r].out;
+      tp.lin = (int)lin;
+      tp.e = key_to_float((unsigned int)(a.keys[r] >> 32));
+      tp.e64 = e64;
+    }
+    if (lane == 0) out[j] = tp;
   }
 }
 
@@ -860,7 +1054,7 @@ __global__ void k_finalize(WaveArgs a) {
   if (r >= a.nrot) return;
   const int out = a.rots[r].out;
   const RotRec* rec = a.rec + r;
-  if (rec->err) atomicAdd(a.err_count, 1);
+  if (rec->err == 1) atomicAdd(a.err_count, 1);  // err 2 is reported through range_err
   if (rec->valid) {
     unsigned long long planes = 0;
     for (int k = 0; k < a.K; ++k)
@@ -887,9 +1081,17 @@ __global__ void k_finalize_server(WaveArgs a, float* ebase, int* ibase) {
   if (r >= a.nrot) return;
   const RotDesc rd = a.rots[r];
   const RotRec* rec = a.rec + r;
-  if (rec->err) atomicAdd(a.err_count, 1);
   const unsigned long long key = a.keys[r];
   int* idx = ibase + rd.pad0;
+  if (rec->err) {
+    // a rotation that could not be searched: NaN energy and index -2 (box overflow) or -3
+    // (FP16 range), which the server reads back to fail exactly the requests that hold one
+    if (rec->err == 1) atomicAdd(a.err_count, 1);
+    else atomicOr(a.range_err, 1);
+    ebase[rd.out] = __int_as_float(0x7fc00000);
+    idx[0] = idx[1] = idx[2] = rec->err == 1 ? -2 : -3;
+    return;
+  }
   if (!rec->valid || key == ~0ull) {
     ebase[rd.out] = INFINITY;
     idx[0] = idx[1] = idx[2] = -1;
@@ -969,7 +1171,6 @@ cudaError_t launch_spread_yz_t(const WaveArgs& a, cudaStream_t s) {
   if (a.kyof && cap <= kDirectMaxAtoms) {
     const size_t sm = direct_smem<N>(cap);
     if (a.lop) {
-      if (N != 64) return cudaErrorInvalidValue;
       cudaError_t e = cudaFuncSetAttribute(k_spread_yz_direct<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       if (e != cudaSuccess) return e;
       k_spread_yz_direct<N, true><<<dim3(a.K, a.nrot), 256, sm, s>>>(a, a.kyof, cap);
@@ -993,10 +1194,11 @@ template <int N>
 cudaError_t launch_yz_inv_t(const WaveArgs& a, cudaStream_t s) {
   // twiddles + one plane (n <= 64: the packed rows alias it) [+ the packed rows]
   const size_t sm = sizeof(float2) * (N + N * (N / 2 + 1) + (N <= 64 ? 0 : (N / 2) * (N + 1)));
-  cudaError_t e = cudaFuncSetAttribute(k_yz_inv_argmin<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  auto kern = a.keys2 ? k_yz_inv_argmin<N, true> : k_yz_inv_argmin<N, false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   dim3 grid(N, a.nrot);
-  k_yz_inv_argmin<N><<<grid, 256, sm, s>>>(a);
+  kern<<<grid, 256, sm, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -1229,6 +1431,16 @@ cudaError_t launch_xpass(const WaveArgs& a, cudaStream_t s) {
 }
 cudaError_t launch_yz_inv_argmin(const WaveArgs& a, cudaStream_t s) {
   CDK_DISPATCH_N(a.n, launch_yz_inv_t, a, s);
+}
+cudaError_t launch_topk_rescore(const WaveArgs& a, const float* grids, int k, TopPose* out, cudaStream_t s) {
+  if (!grids || !out || k < 1 || k > kTopMax) return cudaErrorInvalidValue;
+  k_topk_rescore<<<1, 256, 0, s>>>(a, grids, k, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_tiebreak(const WaveArgs& a, const float* grids, float tol, cudaStream_t s) {
+  if (!a.keys2 || !grids) return cudaErrorInvalidValue;
+  k_tiebreak<<<(a.nrot + 3) / 4, 128, 0, s>>>(a, grids, tol);
+  return cudaGetLastError();
 }
 cudaError_t launch_finalize(const WaveArgs& a, cudaStream_t s) {
   k_finalize<<<(a.nrot + 255) / 256, 256, 0, s>>>(a);

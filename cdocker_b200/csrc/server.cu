@@ -94,8 +94,23 @@ struct Request {
   bool admitted = false, finished = false;
   std::vector<float> out_e;
   std::vector<int> out_i;
-  int status = CDK_OK;
+  int status = CDK_OK;    // first error of any wave that held rotations of this request
+  std::string errmsg;
+  bool scan = false;      // a wave of this request flagged rotations: scan its outputs
 };
+
+// first error wins; later ones keep the original cause
+void fail_request(Request* r, int code, const std::string& msg) {
+  if (r->status == CDK_OK) {
+    r->status = code;
+    r->errmsg = msg;
+  }
+}
+
+// Per-wave status words on the device (one block per wave slot, cleared before the wave's
+// launches and read back after them): [0] rotations over the planned box, [1] a bounded device
+// wait gave up, [2] a scaled ligand value left the FP16 range.
+constexpr int kSlotWords = 16;
 
 struct WaveSlot {
   RotDesc* h_rots = nullptr;  // pinned
@@ -103,6 +118,8 @@ struct WaveSlot {
   cudaEvent_t done = nullptr;
   std::vector<std::pair<uint64_t, long>> parts;  // (request, rotations of it in this wave)
   bool busy = false;
+  unsigned int* h_status = nullptr;  // pinned mirror of the slot's status words
+  cudaError_t launch_err = cudaSuccess;  // first failed launch of this wave
 };
 
 }  // namespace
@@ -121,8 +138,10 @@ struct cdk_server {
   ConfDesc* d_confs = nullptr;    // conformer table, one slot range per request
   int conf_cap = 0;
   void* scratch = nullptr;        // wave scratch (rot_xyz, rec, keys, A or split rows, B)
-  bool streamed = false;          // precision form: streamed tensor-core x pass where it applies
-  unsigned int* d_misc = nullptr;  // [0] overflow count, [2..5] work counters
+  bool streamed = false;          // precision form: tensor-core x pass with ligand rows where it applies
+  float osc[KMAX] = {};           // split-FP16 form: operator scale 2^-sigma_k per channel
+  unsigned int* d_misc = nullptr;  // [16 s .. 16 s + 2] status words of wave slot s; work
+                                   // counters (4 x u64) at byte 128
   WaveSlot slots[2];
   RangeAlloc* alloc = nullptr;
   RangeAlloc* conf_alloc = nullptr;
@@ -137,6 +156,7 @@ struct cdk_server {
   std::thread worker;
   // statistics
   long waves = 0, rotations = 0, launches = 0, tc_waves = 0;
+  long inject_fault_wave = -1;  // opts.reserved[0] > 0: wave number whose fault word the host sets
   double busy_ms = 0.0;
   std::vector<double> latencies;
   std::string error;
@@ -202,9 +222,13 @@ void admit(cdk_server* s) {
   }
 }
 
-// a finished wave: count completed rotations, finish requests whose last rotation it held
-void retire(cdk_server* s, WaveSlot& w) {
-  cudaEventSynchronize(w.done);
+// a finished wave: its status words fail the requests it held (wave-wide causes: a failed
+// launch, a device wait that gave up; per-rotation causes -- box overflow, FP16 range -- only
+// mark the requests for a scan of their own outputs), then requests whose last rotation it
+// held are completed: results copied back, arena space released
+void retire(cdk_server* s, WaveSlot& w, int slot) {
+  cudaError_t se = cudaEventSynchronize(w.done);
+  const unsigned int* st = w.h_status;
   std::vector<Request*> finished;
   {
     std::lock_guard<std::mutex> lk(s->mu);
@@ -212,28 +236,51 @@ void retire(cdk_server* s, WaveSlot& w) {
       auto it = s->all.find(pr.first);
       if (it == s->all.end()) continue;
       Request* r = it->second;
+      if (w.launch_err != cudaSuccess)
+        fail_request(r, CDK_ERR_CUDA, std::string("a kernel launch of its wave failed: ") +
+                                          cudaGetErrorString(w.launch_err));
+      else if (se != cudaSuccess)
+        fail_request(r, CDK_ERR_CUDA, std::string("its wave did not complete: ") + cudaGetErrorString(se));
+      else if (st[1] != 0)
+        fail_request(r, CDK_ERR_CUDA, "a bounded device wait (tensor-core commit) gave up in its wave; "
+                                      "results are invalid");
+      else if (st[0] != 0 || st[2] != 0)
+        r->scan = true;
       r->done_rot += pr.second;
       if (r->done_rot == r->nRot) finished.push_back(r);
     }
   }
+  (void)slot;
   w.parts.clear();
   w.busy = false;
-  if (s->d_misc) {
-    unsigned int ovf = 0;
-    cudaMemcpy(&ovf, s->d_misc, sizeof(unsigned int), cudaMemcpyDeviceToHost);
-    if (ovf) {
-      std::lock_guard<std::mutex> lk(s->mu);
-      for (Request* r : finished) r->status = CDK_ERR_OVERFLOW;
-    }
-  }
+  w.launch_err = cudaSuccess;
   for (Request* r : finished) {
     r->out_e.resize(r->nRot);
     r->out_i.resize(3 * r->nRot);
-    cudaMemcpy(r->out_e.data(), s->arena + r->off_e, sizeof(float) * r->nRot,
-               cudaMemcpyDeviceToHost);
-    cudaMemcpy(r->out_i.data(), s->arena + r->off_i, sizeof(int) * 3 * r->nRot,
-               cudaMemcpyDeviceToHost);
+    cudaError_t e1 = cudaMemcpy(r->out_e.data(), s->arena + r->off_e, sizeof(float) * r->nRot,
+                                cudaMemcpyDeviceToHost);
+    cudaError_t e2 = cudaMemcpy(r->out_i.data(), s->arena + r->off_i, sizeof(int) * 3 * r->nRot,
+                                cudaMemcpyDeviceToHost);
     std::lock_guard<std::mutex> lk(s->mu);
+    if (e1 != cudaSuccess || e2 != cudaSuccess)
+      fail_request(r, CDK_ERR_CUDA, std::string("copy of the results failed: ") +
+                                        cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+    if (r->scan) {
+      // k_finalize_server marks a rotation that could not be searched with index -2 (box
+      // overflow) or -3 (FP16 range)
+      long ovf = 0, rng = 0;
+      for (long g = 0; g < r->nRot; ++g) {
+        ovf += r->out_i[3 * g] == -2;
+        rng += r->out_i[3 * g] == -3;
+      }
+      if (ovf)
+        fail_request(r, CDK_ERR_OVERFLOW, std::to_string(ovf) +
+                                              " rotation(s) of this request overflowed the planned ligand box");
+      else if (rng)
+        fail_request(r, CDK_ERR_UNSUPPORTED,
+                     "a scaled ligand value of this request left the FP16 range of the split-FP16 form "
+                     "(charges or sqrt-epsilon sums too large for this receptor); use CDK_FORM_BF16X3");
+    }
     r->t_done = Clock::now();
     r->finished = true;
     s->latencies.push_back(ms_between(r->t_submit, r->t_done));
@@ -272,13 +319,13 @@ void worker_loop(cdk_server* s) {
   unsigned char* lop_base = reinterpret_cast<unsigned char*>(sc);
   sc += up(std::max((size_t)W * K * Lmax * ncol * sizeof(float2), rows));
   a.B = reinterpret_cast<float2*>(sc);
+  sc += up((size_t)W * n * ncol * sizeof(float2));
+  // precision forms: every window plane's two smallest keys for the FP64 near-tie break, as
+  // in a plain search (so results are the same alone and in the mix)
+  a.keys2 = s->v.tiebreak ? reinterpret_cast<unsigned long long*>(sc) : nullptr;
   a.phat = s->v.phat;
   a.tw = s->v.tw;
-  a.err_count = reinterpret_cast<int*>(s->d_misc);
-  a.fault = reinterpret_cast<int*>(s->d_misc + 1);
-  a.work = reinterpret_cast<unsigned long long*>(s->d_misc + 2);
-  // split-FP16 form: a value outside the FP16 range invalidates the wave like a box overflow
-  a.range_err = a.err_count;
+  a.work = reinterpret_cast<unsigned long long*>(s->d_misc + 32);
   for (int k = 0; k < KMAX; ++k) a.lscale[k] = s->v.lscale[k];
   a.col_tile = s->v.col_tile_opt > 0 ? s->v.col_tile_opt : pick_col_tile(n, K);
   a.kyof = s->v.kyof;
@@ -288,7 +335,7 @@ void worker_loop(cdk_server* s) {
   for (;;) {
     // build the next wave from the admitted requests
     WaveSlot& w = s->slots[cur];
-    if (w.busy) retire(s, w);
+    if (w.busy) retire(s, w, cur);
     int nr = 0, lb = 2, cap = 1;
     {
       std::unique_lock<std::mutex> lk(s->mu);
@@ -302,7 +349,7 @@ void worker_loop(cdk_server* s) {
         WaveSlot& other = s->slots[cur ^ 1];
         if (other.busy) {
           lk.unlock();
-          retire(s, other);
+          retire(s, other, cur ^ 1);
           continue;
         }
         if (s->stop && s->waiting.empty()) break;
@@ -336,35 +383,61 @@ void worker_loop(cdk_server* s) {
         cap = std::max(cap, r->nAtom);
       }
     }
-    cudaMemcpyAsync(w.d_rots, w.h_rots, sizeof(RotDesc) * nr, cudaMemcpyHostToDevice, s->stream);
+    // this slot's status words: cleared before the wave, read back after it
+    unsigned int* d_st = s->d_misc + kSlotWords * cur;
+    a.err_count = reinterpret_cast<int*>(d_st);
+    a.fault = reinterpret_cast<int*>(d_st + 1);
+    a.range_err = reinterpret_cast<int*>(d_st + 2);
+    cudaError_t le = cudaMemcpyAsync(w.d_rots, w.h_rots, sizeof(RotDesc) * nr, cudaMemcpyHostToDevice, s->stream);
+    auto note = [&](cudaError_t e) {
+      if (le == cudaSuccess && e != cudaSuccess) le = e;
+    };
+    note(cudaMemsetAsync(d_st, 0, kSlotWords * sizeof(unsigned int), s->stream));
     a.nrot = nr;
     a.Lb = lb;
     a.atom_cap = cap;
     a.rots = w.d_rots;
-    const bool tc_wave = s->streamed && stream_supported(n, lb) && direct_planes(a);
+    HankelPlan hp{};
+    const bool tc_wave = s->streamed && direct_planes(a) && hankel_plan(n, K, lb, f16, 0, &hp);
     a.lop = tc_wave ? lop_base : nullptr;
     a.f16 = (tc_wave && f16) ? 1 : 0;
-    a.bgroup = (tc_wave && (f16 || s->v.tc_variant != 3)) ? stream_bgroup() : 1;
-    launch_prep(a, s->stream);
-    launch_spread_yz(a, s->stream);
-    if (tc_wave) launch_xpass_stream(a, s->v.top, !f16 && s->v.tc_variant == 3, s->stream);
-    else launch_xpass(a, s->stream);
-    launch_yz_inv_argmin(a, s->stream);
-    launch_finalize_server(a, reinterpret_cast<float*>(s->arena),
-                           reinterpret_cast<int*>(s->arena), s->stream);
-    cudaEventRecord(w.done, s->stream);
+    a.bgroup = tc_wave ? stream_bgroup() : 1;
+    if (le == cudaSuccess) {
+      note(launch_prep(a, s->stream));
+      note(launch_spread_yz(a, s->stream));
+      note(tc_wave ? launch_xpass_hankel(a, s->v.ptilde, s->osc, hp, s->stream) : launch_xpass(a, s->stream));
+      note(launch_yz_inv_argmin(a, s->stream));
+      if (a.keys2)
+        note(launch_tiebreak(a, s->v.grids, s->v.form == CDK_FORM_FP16X2 ? 1e-3f : 1e-4f, s->stream));
+      note(launch_finalize_server(a, reinterpret_cast<float*>(s->arena),
+                                  reinterpret_cast<int*>(s->arena), s->stream));
+    }
+    if (s->waves == s->inject_fault_wave) {
+      // fault injection from the host (a test switch): the word a bounded device wait sets
+      // when it gives up, written after the wave's kernels
+      const unsigned int one = 1;
+      note(cudaMemcpyAsync(d_st + 1, &one, sizeof(one), cudaMemcpyHostToDevice, s->stream));
+      note(cudaStreamSynchronize(s->stream));
+    }
+    note(cudaMemcpyAsync(w.h_status, d_st, 4 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s->stream));
+    note(cudaEventRecord(w.done, s->stream));
+    w.launch_err = le;
+    if (le != cudaSuccess) {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->error = std::string("wave launch: ") + cudaGetErrorString(le);
+    }
     w.busy = true;
     {
       std::lock_guard<std::mutex> lk(s->mu);
       s->waves++;
       s->tc_waves += tc_wave ? 1 : 0;
       s->rotations += nr;
-      s->launches += kLaunchesPerWave + (tc_wave && (f16 || s->v.tc_variant != 3) ? 1 : 0);  // + k_tile_plan
+      s->launches += kLaunchesPerWave + (tc_wave ? 1 : 0) + (a.keys2 ? 1 : 0);  // + k_tile_plan, tie break
     }
     cur ^= 1;
   }
-  for (auto& w : s->slots)
-    if (w.busy) retire(s, w);
+  for (int k = 0; k < 2; ++k)
+    if (s->slots[k].busy) retire(s, s->slots[k], k);
 }
 
 }  // namespace
@@ -401,28 +474,23 @@ int cdk_server_create(cdk_ctx* ctx, const cdk_server_opts* opts, cdk_server** ou
   const int n = s->v.n, K = s->v.K, W = s->opts.wave_rotations;
   const size_t ncol = (size_t)n * (n / 2 + 1);
   auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
-  // precision-form contexts run the streamed tensor-core x pass on waves it applies to (ligand
-  // box <= 32 planes at n = 64, ligands <= 96 atoms on the direct plane path); other waves and
-  // FP32 contexts run the FP32 radix x pass
-  s->streamed = ((s->v.form == CDK_FORM_BF16X3 && (s->v.tc_variant == 0 || s->v.tc_variant == 3)) ||
+  // precision-form contexts run the tensor-core x pass (resident Hankel operator, streamed
+  // ligand rows) on waves it applies to (ligand box <= 32 planes, ligands <= 96 atoms on the
+  // direct plane path); other waves and FP32 contexts run the FP32 radix x pass
+  HankelPlan probe{};
+  s->streamed = ((s->v.form == CDK_FORM_BF16X3 && s->v.tc_variant == 0) ||
                  s->v.form == CDK_FORM_FP16X2) &&
-                s->v.kyof != nullptr &&
-                stream_supported(n, std::min(s->opts.max_box, 32));
-  if (s->streamed) {
-    const int rc = ctx_ensure_top(ctx);
-    if (rc != CDK_OK) {
-      delete s;
-      return rc;
-    }
-    ctx_view(ctx, &s->v);
-  }
+                s->v.kyof != nullptr && s->v.ptilde != nullptr &&
+                hankel_plan(n, K, std::min(s->opts.max_box, 32), s->v.form == CDK_FORM_FP16X2, 0, &probe);
+  for (int k = 0; k < KMAX; ++k) s->osc[k] = s->v.lscale[k] != 0.f ? 1.f / s->v.lscale[k] : 1.f;
   const size_t planes = (size_t)W * K * s->opts.max_box * ncol * sizeof(float2);
   const size_t rows = s->streamed ? (size_t)((W + 7) & ~7) *
                                         stream_lop_bytes_per_rotation(n, K, s->v.form == CDK_FORM_FP16X2)
                                   : 0;
   const size_t scratch = up((size_t)W * s->opts.max_atoms * sizeof(float4)) +
                          up((size_t)W * sizeof(RotRec)) + up((size_t)W * 8) +
-                         up(std::max(planes, rows)) + up((size_t)W * n * ncol * sizeof(float2));
+                         up(std::max(planes, rows)) + up((size_t)W * n * ncol * sizeof(float2)) +
+                         (s->v.tiebreak ? up((size_t)W * n * 2 * sizeof(unsigned long long)) : 0);
   auto fail = [&](const std::string& m, int code) {
     set_error(m);
     cdk_server_destroy(s);
@@ -434,14 +502,16 @@ int cdk_server_create(cdk_ctx* ctx, const cdk_server_opts* opts, cdk_server** ou
   if (cudaMalloc(&s->arena, s->opts.arena_bytes) != cudaSuccess ||
       cudaMalloc(&s->d_confs, sizeof(ConfDesc) * (size_t)s->opts.max_conformers) != cudaSuccess ||
       cudaMalloc(&s->scratch, scratch) != cudaSuccess ||
-      cudaMalloc(&s->d_misc, 64) != cudaSuccess)
+      cudaMalloc(&s->d_misc, 256) != cudaSuccess)
     return fail("server device allocation failed (" + std::to_string((s->opts.arena_bytes + scratch) >> 20) + " MiB)", CDK_ERR_NOMEM);
-  cudaMemset(s->d_misc, 0, 64);
+  cudaMemset(s->d_misc, 0, 256);
+  s->inject_fault_wave = s->opts.reserved[0] > 0 ? (long)s->opts.reserved[0] - 1 : -1;
   s->arena_bytes = s->opts.arena_bytes;
   s->conf_cap = s->opts.max_conformers;
   for (auto& w : s->slots) {
     if (cudaMallocHost(&w.h_rots, sizeof(RotDesc) * W) != cudaSuccess ||
         cudaMalloc(&w.d_rots, sizeof(RotDesc) * W) != cudaSuccess ||
+        cudaMallocHost(&w.h_status, 4 * sizeof(unsigned int)) != cudaSuccess ||
         cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming) != cudaSuccess)
       return fail("server wave buffers failed", CDK_ERR_NOMEM);
   }
@@ -527,6 +597,7 @@ int cdk_server_poll(cdk_server* s, uint64_t ticket, int wait_ms, float* minE, in
   }
   if (!r->finished) return CDK_ERR_BUSY;
   const int status = r->status;
+  const std::string msg = r->errmsg;
   if (minE) std::memcpy(minE, r->out_e.data(), sizeof(float) * r->nRot);
   if (idx) std::memcpy(idx, r->out_i.data(), sizeof(int) * 3 * r->nRot);
   if (timing) {
@@ -536,7 +607,7 @@ int cdk_server_poll(cdk_server* s, uint64_t ticket, int wait_ms, float* minE, in
   }
   s->all.erase(it);
   delete r;
-  if (status != CDK_OK) set_error("a rotation of this request overflowed the planned box");
+  if (status != CDK_OK) set_error(msg);
   return status;
 }
 
@@ -572,6 +643,7 @@ int cdk_server_destroy(cdk_server* s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (auto& w : s->slots) {
     if (w.h_rots) cudaFreeHost(w.h_rots);
+    if (w.h_status) cudaFreeHost(w.h_status);
     cudaFree(w.d_rots);
     if (w.done) cudaEventDestroy(w.done);
   }

@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(256) k_top_build(int K, const float2* __restri
 // chunks, clamped to the jc chunks of the box) its rotations touch. Every column CTA of the tile
 // reads it with one load instead of rebuilding it.
 __global__ void __launch_bounds__(XS_R) k_tile_plan(WaveArgs a, int jc) {
-  __shared__ int s_jlo[KMAX], s_jhi[KMAX];
+  __shared__ int s_jlo[KMAX], s_jhi[KMAX], s_wmax;
   const int tid = threadIdx.x, lane = tid & 31;
   const int r0 = blockIdx.x * XS_R;
   const int nr = min(XS_R, a.nrot - r0);
@@ -217,9 +217,15 @@ __global__ void __launch_bounds__(XS_R) k_tile_plan(WaveArgs a, int jc) {
     s_jlo[tid] = XS_JMAX;
     s_jhi[tid] = -1;
   }
+  if (tid == 0) s_wmax = 0;
   __syncthreads();
   const RotRec* rec = a.rec + r0 + min(tid, nr - 1);
   const bool live = tid < nr && rec->valid;
+  {
+    // the largest window of the tile (x' rows any of its rotations keeps)
+    const int wm = __reduce_max_sync(0xffffffffu, live ? rec->W[0] : 0);
+    if (lane == 0 && wm > 0) atomicMax(&s_wmax, wm);
+  }
   for (int k = 0; k < K; ++k) {
     const int lo = live ? rec->xlo[k] : 1, hi = live ? rec->xhi[k] : 0;
     const int jl = lo <= hi ? min(lo >> 3, jc - 1) : 15;
@@ -247,7 +253,7 @@ __global__ void __launch_bounds__(XS_R) k_tile_plan(WaveArgs a, int jc) {
     tp[0] = pk;
     tp[1] = pl;
     tp[2] = ph;
-    tp[3] = ((unsigned long long)steps << 32) | n;
+    tp[3] = ((unsigned long long)steps << 32) | ((unsigned long long)min(s_wmax, 0xFFFF) << 16) | n;
   }
 }
 
@@ -300,7 +306,7 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS, F16>::MIN_BLOCKS)
   const uint64_t pk = ((uint64_t)t01.y << 32) | t01.x;
   const uint64_t pl = ((uint64_t)t01.w << 32) | t01.z;
   const uint64_t ph = ((uint64_t)t23.y << 32) | t23.x;
-  const int nact = (int)t23.z;
+  const int nact = (int)(t23.z & 0xFFFFu);
   const int NS = COLS * (int)t23.w;  // stages: one K-step of one (channel, column)
   // this thread's rotation: its window (epilogue) and, for the producers, its chunk range per
   // channel (8 bits each: jlo | jhi << 4, 0x0F when empty) from one vector load of the record
@@ -499,337 +505,6 @@ __global__ void __launch_bounds__(XS_THREADS, XsShape<COLS, F16>::MIN_BLOCKS)
 }
 
 
-// ---------------------------------------------------------------------------------------------
-// Ligand operand in tensor memory. The same contraction with the roles swapped: M = 128
-// rotations (TMEM lanes), N = 128 operator rows (x' real, x' imaginary), so the ligand rows are
-// the A operand and live in TMEM (written by the producer threads with tcgen05.st, one lane per
-// rotation) while only the operator tiles are read from shared memory by the MMAs -- half the
-// shared-memory traffic of the shared-memory kernel per MMA.
-//   TMEM: columns [0, 256) accumulators D[c][rotation][n] of the 2 columns, [256, 512) a ring of
-//   ligand stages (hi, lo x jc K-steps x 8 columns of bf16 pairs).
-//   Warps 0-3 and 4-7: two producer groups taking alternate stages (thread = rotation); each
-//   group's thread 0 also bulk-copies the stage's operator tiles. Warp 8: one elected lane
-//   issues the MMAs. Warps 9-12: the epilogue of a column as soon as its channels are done
-//   (stages are column-major), overlapping the next column's MMAs.
-// Measured at 64^3 (config 1): bit-identical to the shared-memory kernel and 1.27x slower
-// (512 TMEM columns allow one CTA per SM, so the prologue and the last column's epilogue are
-// exposed, and the producers wait on their global loads before each tcgen05.st). Opt-in
-// (cdk_opts.reserved[3] = 3).
-constexpr int TA_R = 128;
-constexpr int TA_COLS = 2;
-constexpr int TA_THREADS = 13 * 32;
-constexpr int TA_MMA_WARP = 8;
-constexpr int TA_EPI_WARP = 9;
-constexpr uint32_t TA_ACOL = TA_COLS * TA_R;  // first TMEM column of the ligand ring
-constexpr int TA_MAXSTAGES = 8;
-constexpr size_t TA_SMEM = (size_t)TA_MAXSTAGES * 2 * 2 * XS_STEP + 1024;  // <= 8 x 2 tiles x 2 steps
-
-__device__ __forceinline__ void umma_f16_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-      :
-      : "r"(d_tmem), "r"(a_tmem), "l"(b), "r"(XS_IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-      : "memory");
-}
-
-__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t* v) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr),
-      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
-      : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-__global__ void __launch_bounds__(TA_THREADS, 1) k_xpass_tmema64(WaveArgs a, const unsigned char* __restrict__ top,
-                                                                 int jc) {
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  unsigned char* ring = reinterpret_cast<unsigned char*>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  __shared__ __align__(8) uint64_t s_full[TA_MAXSTAGES];
-  __shared__ __align__(8) uint64_t s_empty[TA_MAXSTAGES];
-  __shared__ __align__(8) uint64_t s_colbar[TA_COLS];
-  __shared__ int s_fail;
-  __shared__ int s_issued[2];
-  __shared__ int s_consumed;
-  __shared__ uint32_t s_tmem;
-  __shared__ unsigned char s_jr[KMAX][TA_R];
-  __shared__ int s_jlo[KMAX], s_jhi[KMAX];
-  __shared__ int s_act[KMAX], s_nact;
-  __shared__ int s_W[TA_R];
-  const int K = a.K;
-  const uint32_t tile = (uint32_t)jc * XS_STEP;      // one hl of a stage's operator tiles
-  const uint32_t stage = 2 * tile;                   // operator tiles (hi, lo) of a stage
-  const uint32_t acols = 2u * 8u * (uint32_t)jc;     // TMEM columns of a stage's ligand (hi, lo)
-  const int nb = min(TA_MAXSTAGES, (int)((512u - TA_ACOL) / acols));
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int r0 = blockIdx.x * TA_R;
-  const int c0 = blockIdx.y * TA_COLS;
-  const int nr = min(TA_R, a.nrot - r0);
-  if (tid == 0) {
-    for (int b = 0; b < nb; ++b) {
-      // full: the producing group's 128 threads + the operator copies' expect_tx arrival
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_full[b])), "r"(129));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_empty[b])));
-    }
-    for (int c = 0; c < TA_COLS; ++c)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_colbar[c])));
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    s_fail = 0;
-    s_issued[0] = s_issued[1] = 0;
-    s_consumed = 0;
-  }
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                 "r"(512));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-  }
-  if (tid < KMAX) {
-    s_jlo[tid] = XS_JMAX;
-    s_jhi[tid] = -1;
-  }
-  __syncthreads();
-  if (tid < TA_R) {
-    const RotRec* rec = a.rec + r0 + min(tid, nr - 1);
-    const bool live = tid < nr && rec->valid;
-    s_W[tid] = live ? rec->W[0] : 0;
-    static_assert(KMAX == 16, "x ranges are two 32-byte vectors");
-    uint4 v[4];
-    const uint4* xr = reinterpret_cast<const uint4*>(rec->xlo);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) v[i] = xr[i];
-    const short* lo16 = reinterpret_cast<const short*>(&v[0]);
-    const short* hi16 = reinterpret_cast<const short*>(&v[2]);
-#pragma unroll
-    for (int k = 0; k < KMAX; ++k) {
-      if (k < K) {
-        const int lo = live ? lo16[k] : 1, hi = live ? hi16[k] : 0;
-        int jl = 15, jh = -1;
-        if (lo <= hi) {
-          jl = min(lo >> 3, jc - 1);
-          jh = min(hi >> 3, jc - 1);
-          s_jr[k][tid] = (unsigned char)(jl | (jh << 4));
-        } else {
-          s_jr[k][tid] = 0x0F;
-        }
-        const int wl = __reduce_min_sync(0xffffffffu, jl);
-        const int wh = __reduce_max_sync(0xffffffffu, jh);
-        if (lane == 0) {
-          if (wl < 15) atomicMin(&s_jlo[k], wl);
-          if (wh >= 0) atomicMax(&s_jhi[k], wh);
-        }
-      }
-    }
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (tid == 0) {
-    int n = 0;
-    for (int k = 0; k < K; ++k)
-      if (s_jlo[k] <= s_jhi[k]) s_act[n++] = k;
-    s_nact = n;
-  }
-  __syncthreads();
-  const uint32_t tmem = s_tmem;
-  const int nact = s_nact;
-  const int NS = nact * TA_COLS;  // stages: column-major (column, active channel)
-  const uint32_t ring_s = smem_u32(ring);
-  uint64_t pk = 0, pl = 0, ph = 0;
-  for (int i = 0; i < nact; ++i) {
-    const int k = s_act[i];
-    pk |= (uint64_t)k << (4 * i);
-    pl |= (uint64_t)s_jlo[k] << (4 * i);
-    ph |= (uint64_t)s_jhi[k] << (4 * i);
-  }
-
-  if (warp < 8) {
-    // ---- producers: group g takes stages g, g+2, ...; thread = rotation rr (its TMEM lane)
-    const int g = warp >> 2;
-    const int rr = (warp & 3) * 32 + lane;
-    const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
-    const int rg = r0 + (rr < nr ? rr : 0);
-    constexpr size_t RS = (size_t)(XS_NCOL / 4) * 32;
-    const size_t rot_rows = (size_t)(rg >> 3) * K * 16 * RS + (size_t)(c0 >> 2) * 32 + (rg & 7) * 4 + (c0 & 3);
-    uint64_t jr_lo = 0, jr_hi = 0;
-    for (int k = 0; k < K; ++k) {
-      const uint64_t v = s_jr[k][rr];
-      if (k < 8) jr_lo |= v << (8 * k);
-      else jr_hi |= v << (8 * (k - 8));
-    }
-    const bool leader = (tid & 127) == 0;
-    for (int s = g; s < NS; s += 2) {
-      const int b = s % nb;
-      const int c = s / nact, ai = s - c * nact;
-      const int k = (int)((pk >> (4 * ai)) & 15);
-      const int jlo = (int)((pl >> (4 * ai)) & 15), jhi = (int)((ph >> (4 * ai)) & 15);
-      const unsigned int jr = (unsigned int)(((k < 8 ? jr_lo : jr_hi) >> (8 * (k & 7))) & 255);
-      const int jl = (int)(jr & 15), jh = (int)(jr >> 4);
-      // this rotation's rows of the stage: [j][hl][re 4 words, im 4 words]
-      uint32_t rows[XS_JMAX][2][8];
-      const uint4* src0 = reinterpret_cast<const uint4*>(a.lop) + rot_rows + (size_t)k * 16 * RS + c;
-#pragma unroll
-      for (int jj = 0; jj < XS_JMAX; ++jj) {
-        const int j = jlo + jj;
-        const bool have = j <= jhi && jl <= j && j <= jh;
-#pragma unroll
-        for (int hl = 0; hl < 2; ++hl)
-#pragma unroll
-          for (int part = 0; part < 2; ++part) {
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (have) v = __ldg(src0 + (size_t)((hl * 4 + j) * 2 + part) * RS);
-            rows[jj][hl][part * 4 + 0] = v.x;
-            rows[jj][hl][part * 4 + 1] = v.y;
-            rows[jj][hl][part * 4 + 2] = v.z;
-            rows[jj][hl][part * 4 + 3] = v.w;
-          }
-      }
-      // the MMAs of stage s - nb must be done with this ring slot (TMEM columns and operator tiles);
-      // the decision is warp-uniform (tcgen05.st below is warp-collective)
-      if (s >= nb) {
-        const bool okw = __all_sync(0xffffffffu, mbar_wait(smem_u32(&s_empty[b]), (uint32_t)((s / nb) - 1) & 1u));
-        if (!okw) {
-          atomicOr(&s_fail, 1);
-          break;
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      }
-      const uint32_t full = smem_u32(&s_full[b]);
-      if (leader) {
-        const uint32_t bytes = (uint32_t)(jhi - jlo + 1) * XS_STEP;
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(2 * bytes), "r"(full)
-                     : "memory");
-#pragma unroll
-        for (int hl = 0; hl < 2; ++hl) {
-          const unsigned char* src = top + (((size_t)(c0 + c) * K + k) * 2 + hl) * XS_TILE + (size_t)jlo * XS_STEP;
-          const uint32_t dst = ring_s + (uint32_t)b * stage + (uint32_t)hl * tile + (uint32_t)jlo * XS_STEP;
-          asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                       "l"(src), "r"(bytes), "r"(full)
-                       : "memory");
-        }
-        s_issued[g] = s + 1;
-      }
-      const uint32_t acol = tmem + lane_base + TA_ACOL + (uint32_t)b * acols;
-#pragma unroll
-      for (int jj = 0; jj < XS_JMAX; ++jj) {
-        if (jlo + jj <= jhi) {
-#pragma unroll
-          for (int hl = 0; hl < 2; ++hl)
-            tmem_st8(acol + (uint32_t)hl * 8u * (uint32_t)jc + (uint32_t)(jlo + jj) * 8u, rows[jj][hl]);
-        }
-      }
-      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(full) : "memory");
-    }
-  } else if (warp == TA_MMA_WARP) {
-    {
-      // ---- MMA issuer: the whole warp runs the loop, one elected lane issues
-      const uint64_t desc0 = make_desc(ring_s, XS_GROUP, 128);
-      int s = 0;
-      for (; s < NS; ++s) {
-        const int b = s % nb;
-        if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_full[b]), (uint32_t)(s / nb) & 1u))) {
-          if (lane == 0) atomicOr(&s_fail, 1);
-          break;
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const int c = s / nact, ai = s - c * nact;
-        const int jlo = (int)((pl >> (4 * ai)) & 15), jhi = (int)((ph >> (4 * ai)) & 15);
-        const uint32_t acol = tmem + TA_ACOL + (uint32_t)b * acols + (uint32_t)jlo * 8u;
-        const uint32_t d = tmem + (uint32_t)(c * TA_R);
-        // descriptors by adding start-address units to one base (see the smem-ligand kernel)
-        const uint64_t th0 = desc0 + (uint64_t)((uint32_t)b * (stage >> 4) + (uint32_t)jlo * (XS_STEP >> 4));
-        const uint64_t tu = tile >> 4;
-        const uint32_t lo_off = 8u * (uint32_t)jc;
-#pragma unroll
-        for (int jj = 0; jj < XS_JMAX; ++jj) {
-          if (jlo + jj > jhi) break;
-          const uint64_t th = th0 + (uint64_t)jj * (XS_STEP >> 4), tl = th + tu;
-          const uint32_t lh = acol + (uint32_t)jj * 8u, ll = lh + lo_off;
-          const uint32_t acc = (ai > 0 || jj > 0) ? 1u : 0u;
-          if (elect_one()) umma_f16_ts(d, lh, th, acc);
-          if (elect_one()) umma_f16_ts(d, ll, th, 1u);
-          if (elect_one()) umma_f16_ts(d, lh, tl, 1u);
-        }
-        if (elect_one()) {
-          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                           smem_u32(&s_empty[b]))
-                       : "memory");
-          if (ai == nact - 1)  // column c complete: release its epilogue
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(&s_colbar[c]))
-                         : "memory");
-        }
-        __syncwarp();
-      }
-      if (lane == 0) {
-        s_consumed = s;
-        unsigned long long steps = 0;
-        for (int t = 0; t < s; ++t) {
-          const int at = t % nact;
-          steps += (unsigned long long)(((ph >> (4 * at)) & 15) - ((pl >> (4 * at)) & 15) + 1);
-        }
-        if (steps && a.work) atomicAdd(a.work + 2, steps);
-        if (s < NS) {  // a failed wait: let the columns' epilogue waits end
-          for (int c = 0; c < TA_COLS; ++c)
-            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&s_colbar[c])) : "memory");
-        }
-      }
-    }
-  } else if (NS > 0) {
-    // ---- epilogue: column c as soon as its accumulation is complete; thread = rotation
-    const int q = warp & 3;  // TMEM lane quarter of this warp
-    const int rr = q * 32 + lane;
-    const uint32_t lane_base = (uint32_t)(q * 32) << 16;
-    const int Wr = rr < nr ? s_W[rr] : 0;
-    for (int c = 0; c < TA_COLS; ++c) {
-      // warp-uniform decisions: tcgen05.ld below is warp-collective
-      if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_colbar[c]), 0u))) {
-        atomicOr(&s_fail, 1);
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      if (__any_sync(0xffffffffu, s_fail != 0)) break;
-      float2* dst = a.B + (size_t)(r0 + rr) * XS_N * XS_NCOL + c0 + c;
-      for (int x0 = 0; x0 < XS_N; x0 += 8) {
-        float v[16];  // operator columns 2x' (real), 2x' + 1 (imaginary) for x' = x0 .. x0 + 7
-        tmem_ld16(tmem + lane_base + (uint32_t)(c * TA_R + 2 * x0), v);
-#pragma unroll
-        for (int t = 0; t < 8; ++t)
-          if (x0 + t < Wr) dst[(size_t)(x0 + t) * XS_NCOL] = make_float2(v[2 * t], v[2 * t + 1]);
-      }
-    }
-  }
-  __syncthreads();
-  if (s_fail && tid == 0) {
-    // operator copies issued for stages the MMA thread never consumed: let them land
-    for (int g = 0; g < 2; ++g)
-      for (int t = s_consumed; t < s_issued[g]; ++t)
-        if ((t & 1) == g) mbar_wait(smem_u32(&s_full[t % nb]), (uint32_t)(t / nb) & 1u);
-    atomicOr(a.fault, 1);
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  if (warp == 0) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
-  }
-}
-
 }  // namespace
 
 int stream_bgroup() {
@@ -841,6 +516,12 @@ int stream_bgroup() {
   return g;
 }
 
+cudaError_t launch_tile_plan(const WaveArgs& a, int jc, cudaStream_t s) {
+  if (jc < 1 || jc > XS_JMAX) return cudaErrorInvalidValue;
+  k_tile_plan<<<(a.nrot + XS_R - 1) / XS_R, XS_R, 0, s>>>(a, jc);
+  return cudaGetLastError();
+}
+
 bool stream_supported(int n, int Lb) { return n == 64 && Lb >= 1 && Lb <= 8 * XS_JMAX; }
 
 size_t stream_top_bytes(int n, int K) {
@@ -848,7 +529,8 @@ size_t stream_top_bytes(int n, int K) {
 }
 
 size_t stream_lop_bytes_per_rotation(int n, int K, bool f16) {
-  return n == 64 ? (size_t)K * XS_NCOL * (f16 ? 128 : 256) : 0;
+  // per channel 16 split-BF16 rows or 8 FP16 rows of the half spectrum, 16 B per column
+  return (size_t)K * n * (n / 2 + 1) * (f16 ? 128 : 256);
 }
 
 cudaError_t launch_top_build(int n, int K, const float2* pt, void* top, const float* f16_scale,
@@ -876,19 +558,12 @@ cudaError_t launch_stream_cols(const WaveArgs& a, const void* top, int jc, cudaS
   return cudaGetLastError();
 }
 
-cudaError_t launch_xpass_stream(const WaveArgs& a, const void* top, bool tmem_ligand, cudaStream_t s) {
+cudaError_t launch_xpass_stream(const WaveArgs& a, const void* top, cudaStream_t s) {
   if (!stream_supported(a.n, a.Lb) || !a.lop || !top) return cudaErrorInvalidValue;
   const int jc = (a.Lb + 7) / 8;  // K-steps a valid rotation can touch
-  if (tmem_ligand) {
-    if (a.f16) return cudaErrorInvalidValue;  // the tensor-memory ligand kernel is split-BF16 only
-    cudaError_t e = cudaFuncSetAttribute(k_xpass_tmema64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TA_SMEM);
-    if (e != cudaSuccess) return e;
-    dim3 grid((a.nrot + TA_R - 1) / TA_R, XS_NCOL / TA_COLS);
-    k_xpass_tmema64<<<grid, TA_THREADS, TA_SMEM, s>>>(a, reinterpret_cast<const unsigned char*>(top), jc);
-    return cudaGetLastError();
-  }
   // ligand boxes of up to 24 planes: 2 columns, two CTAs per SM; larger boxes: 4 columns
-  k_tile_plan<<<(a.nrot + XS_R - 1) / XS_R, XS_R, 0, s>>>(a, jc);
+  cudaError_t e = launch_tile_plan(a, jc, s);
+  if (e != cudaSuccess) return e;
   if (a.f16) {
     return jc <= 3 ? launch_stream_cols<2, true>(a, top, jc, s) : launch_stream_cols<4, true>(a, top, jc, s);
   }

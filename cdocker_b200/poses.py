@@ -17,8 +17,14 @@ from . import _lib as L
 
 
 def sort_index(values) -> np.ndarray:
-    """Indices ordered by value, ascending; ties keep their original order."""
-    return np.argsort(np.asarray(values, np.float32), kind="stable")
+    """Indices ordered by value, ascending, through cdk_sort_index: the reference's std::sort
+    with strict < (include/GeneDiverseConformations.h:9-20), so equal energies rank in the same
+    order as in the reference driver."""
+    v = np.ascontiguousarray(values, np.float32).reshape(-1)
+    out = np.empty(v.shape[0], np.int64)
+    L.check(L.lib().cdk_sort_index(v.ctypes.data_as(C.POINTER(C.c_float)), v.shape[0],
+                                   out.ctypes.data_as(C.POINTER(C.c_long))))
+    return out
 
 
 def pose_coordinates(coor, quat, grid_min, spacing, idx) -> np.ndarray:

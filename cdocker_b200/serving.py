@@ -26,7 +26,7 @@ class Ticket:
 class Server:
     def __init__(self, receptor: Receptor, arena_bytes: int = 1 << 30, wave_rotations: int = 1024,
                  max_box: int = 0, max_atoms: int = 128, max_conformers: int = 1 << 16,
-                 max_waiting: int = 4096):
+                 max_waiting: int = 4096, inject_fault_wave: int = -1):
         lib = L.lib()
         o = L.CdkServerOpts()
         lib.cdk_server_opts_default(C.byref(o))
@@ -36,6 +36,8 @@ class Server:
         o.max_atoms = max_atoms
         o.max_conformers = max_conformers
         o.max_waiting = max_waiting
+        # test switch: the host sets the device-wait fault word of this wave (0-based)
+        o.reserved[0] = inject_fault_wave + 1 if inject_fault_wave >= 0 else 0
         h = C.c_void_p()
         L.check(lib.cdk_server_create(receptor.handle, C.byref(o), C.byref(h)))
         self._h = h

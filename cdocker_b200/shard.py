@@ -55,7 +55,8 @@ def gather_results(minE: np.ndarray, idx: np.ndarray, n_conf: int, n_q: int, gro
 
 
 def top_k(minE: np.ndarray, k: int) -> np.ndarray:
-    """Indices of the k lowest energies, ordered as std::sort with strict < orders them
-    (sort_index, include/GeneDiverseConformations.h:9-20; ties keep a stable order here)."""
-    order = np.argsort(minE, kind="stable")
-    return order[:k]
+    """Indices of the k lowest energies of the gathered job, ranked as the reference ranks a
+    conformer's rotations (sort_index: std::sort with strict <,
+    include/GeneDiverseConformations.h:9-20, through cdk_sort_index)."""
+    from .poses import sort_index
+    return sort_index(minE)[:k]

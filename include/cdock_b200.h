@@ -40,8 +40,9 @@ extern "C" {
 #define CDK_FORM_BF16X3 1 /* split-BF16 (hi*hi + hi*lo + lo*hi) DFT contractions, FP32 acc. */
 #define CDK_FORM_FP16X2 2 /* split-FP16 operator x FP16 ligand rows (two products), per-channel
                              power-of-two scaling, FP32 acc.: about 1e-4 relative error; half the
-                             ligand bytes and two thirds of the MMAs of BF16X3 (n = 64; other sizes
-                             and ligands above 96 atoms run the BF16X3 kernels) */
+                             ligand bytes and two thirds of the MMAs of BF16X3. Ligands of at most
+                             96 atoms with a box of at most 32 planes; a search outside that
+                             returns CDK_ERR_UNSUPPORTED (BF16X3 covers every ligand) */
 
 typedef struct cdk_ctx cdk_ctx;
 
@@ -56,13 +57,21 @@ typedef struct cdk_opts {
                           [1] = 1: spread planes through the radix FFT instead of the direct
                           separable evaluation; [2] = 1: autotune the x pass on the first wave
                           of each new ligand box; [3] precision-form x pass: 0 = tcgen05 with
-                          streamed operands in shared memory where it applies (n = 64, ligand
-                          box <= 32 planes, ligands <= 96 atoms), else the next one;
-                          1 = mma.sync; 2 = tcgen05 with operands built inside the kernel;
-                          3 = tcgen05 with streamed operands, the ligand in tensor memory;
+                          the Hankel operator resident in shared memory and streamed ligand
+                          rows where it applies (ligand box <= 32 planes, ligands <= 96 atoms,
+                          operator fits shared memory), else the next one; 1 = mma.sync;
+                          2 = tcgen05 with operands built inside the kernel (n = 64);
+                          3 = tcgen05 with streamed operator tiles (n = 64);
                           [4] = 1: keep the rotations in the given order in the streamed
                           tensor-core x pass (by default they are grouped by the ligand-box
-                          chunks their channels reach, which changes no result) */
+                          chunks their channels reach, which changes no result);
+                          [5] Hankel x pass columns per CTA: 0 = automatic, 1, or 2 (n <= 64);
+                          [6] precision forms: poses per wave re-scored in FP64
+                          (cdk_ctx_top_poses): 0 = 8 (none in the FP32 form), -1 = none,
+                          1..32; [7] = 1: no FP64 near-tie break of the argmin in the
+                          precision forms (by default, when a rotation's two best translations
+                          lie within 1e-3 (split-FP16) or 1e-4 (split-BF16) x max(|E|, 1) of
+                          each other, both are re-scored in FP64 and the lower is kept) */
 } cdk_opts;
 
 /* Library version string. */
@@ -99,15 +108,18 @@ int cdk_search_device(cdk_ctx* ctx, int nAtom, int nConf, const float* d_coor,
                       const float* d_quats, float* d_minE, int* d_idx, void* stream);
 
 /* cdk_search_device without any device allocation. It has no counterpart in the reference.
- * For callers that cannot call cudaMalloc when they search (recording into a CUDA graph,
- * real-time loops that must not hit the allocator, memory owned by a pool): the wave and
- * table scratch that cdk_search_device grows with cudaMalloc comes instead from one
- * file-scope device array of CDK_NOALLOC_SCRATCH_BYTES (64 MiB), held by every GPU that loads
- * the library until exit. Rotations run in waves that fit it; a search whose single rotation
- * does not fit returns CDK_ERR_UNSUPPORTED. The first call on each device looks up the
- * array's device address (cudaGetSymbolAddress) and must come before any stream capture.
- * Calls share the array: calls that overlap on the GPU race; serialise them. Same arguments,
- * results and errors as cdk_search_device. */
+ * For callers that cannot let the library call cudaMalloc when they search (real-time loops
+ * that must not hit the allocator's device-wide synchronisation, device memory owned by a
+ * pool that forbids outside allocations): the wave and table scratch that cdk_search_device
+ * grows with cudaMalloc comes instead from one file-scope device array of
+ * CDK_NOALLOC_SCRATCH_BYTES (64 MiB), held by every GPU that loads the library until exit.
+ * FP32-form contexts only: a context of another form returns CDK_ERR_UNSUPPORTED. Rotations
+ * run in waves that fit the array; a search whose single rotation does not fit returns
+ * CDK_ERR_UNSUPPORTED. The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress) and caches it; the cache does not survive cudaDeviceReset. The call
+ * synchronises its stream twice (ligand-box plan, overflow count). Calls share the array:
+ * calls that overlap on the GPU race; serialise them. Otherwise the same arguments, results
+ * and errors as cdk_search_device on an FP32 context. */
 #define CDK_NOALLOC_SCRATCH_BYTES (64u << 20)
 int cdk_search_device_noalloc(cdk_ctx* ctx, int nAtom, int nConf, const float* d_coor,
                               const float* d_charge, const float* d_eps, const int* d_slot,
@@ -159,6 +171,12 @@ int cdk_filter_quaternions(const float* coor, int nAtom, int nQ, const float* qu
  * grids, the used grid indices (ascending), and their count via *nUsed. */
 int cdk_vdw_slots(int nAtom, const float* radii, int nVdw, const float* gridRadii,
                   int* usedIdx, int* atomSlot, int* nUsed);
+
+/* sort_index (include/GeneDiverseConformations.h:9-20, used on the per-rotation minima at
+ * src/TranRotaConfSearchNoMini.cu:469): out[0..n) = indices of v in ascending order by
+ * std::sort with strict <, so equal values come out in the same (unstable) order as the
+ * reference's call. */
+int cdk_sort_index(const float* v, long n, long* out);
 
 /* Pose of one rotation at its best translation (src/TranRotaConfSearchNoMini.cu:473-487):
  * out[a] = Rotate(quat, coor[a]) + gridMin - mincoor + idx * spacing, in double.
@@ -232,7 +250,9 @@ typedef struct cdk_server_opts {
   int max_atoms;       /* largest ligand */
   int max_conformers;  /* conformer slots across admitted requests */
   int max_waiting;     /* queued (not yet admitted) requests before submit returns BUSY */
-  int reserved[4];
+  int reserved[4];     /* [0] = w > 0: test switch, the host sets the device-wait fault word of
+                          wave number w-1 after its kernels (every request in it then fails
+                          with CDK_ERR_CUDA); 0 in production */
 } cdk_server_opts;
 void cdk_server_opts_default(cdk_server_opts* opts);
 int cdk_server_create(cdk_ctx* ctx, const cdk_server_opts* opts, cdk_server** out);
@@ -242,13 +262,19 @@ int cdk_server_submit(cdk_server* s, int nAtom, int nConf, const float* coor,
                       const float* quats, uint64_t* ticket);
 /* Waits up to wait_ms (-1: forever, 0: no wait). CDK_OK: results copied (minE[nConf*nQ],
  * idx[nConf*nQ][3]) and timing[0..2] = queue, run, total ms; the ticket is then released.
- * CDK_ERR_BUSY: still running. */
+ * CDK_ERR_BUSY: still running. A finished request that failed returns its own status (results
+ * are still copied and the ticket released): CDK_ERR_OVERFLOW when a rotation of it left the
+ * planned ligand box, CDK_ERR_UNSUPPORTED when a scaled ligand value of it left the FP16 range
+ * of the split-FP16 form (those rotations read minE = NaN and idx = -2 or -3), CDK_ERR_CUDA when
+ * a wave that held its rotations failed to launch or a bounded device wait in it gave up.
+ * Errors are attributed per request: other requests of the same wave are unaffected by a
+ * per-rotation cause. */
 int cdk_server_poll(cdk_server* s, uint64_t ticket, int wait_ms, float* minE, int* idx,
                     double* timing);
 /* [0] waves, [1] rotations, [2] kernel launches, [3] completed requests, [4] p50 latency ms,
  * [5] p99 latency ms, [6] waiting requests, [7] admitted requests in flight, [8] waves run on
- * the streamed tensor-core x pass (precision-form contexts: waves whose ligand box is <= 32
- * planes at n = 64 and whose ligands have <= 96 atoms; the others run the FP32 x pass). */
+ * the tensor-core x pass (precision-form contexts: waves whose ligand box is <= 32 planes and
+ * whose ligands have <= 96 atoms, at any grid size; the others run the FP32 x pass). */
 int cdk_server_stats(cdk_server* s, double* out, int n);
 int cdk_server_destroy(cdk_server* s);
 
@@ -260,12 +286,23 @@ int cdk_server_destroy(cdk_server* s);
  * opts.reserved[0] = 1 (events around every launch), else 0; [13] x-pass column tile,
  * [14] x-pass rotations per CTA, [15] graph state (0 off, 1 shape seen, 2 replaying),
  * [16] x-pass kind (0 FP32 radix, 1 mma.sync, 2 tcgen05 with in-kernel operand builds,
- * 3 tcgen05 with streamed operands in shared memory, 4 tcgen05 with streamed operands, the
- * ligand in tensor memory, 5 tcgen05 with streamed operands, split-FP16 form),
- * [17] tensor-core K-steps the streamed x pass issued (one step = three 128 x 128 x 16 BF16
- * MMAs, 1,572,864 flops; in the split-FP16 form two FP16 MMAs, 1,048,576 flops). */
-#define CDK_NSTATS 18
+ * 3 tcgen05 with streamed operator tiles (64^3), 5 the same in the split-FP16 form,
+ * 6 tcgen05 with the resident Hankel operator, 7 the same in the split-FP16 form),
+ * [17] tensor-core K-steps the x pass issued per spectral column (one step = the MMAs of one
+ * 8-plane chunk of one channel for one column and 128 rotations), [18] Hankel x pass: issued
+ * MMA work in units of 128 x 8 x 16 multiply-adds (32,768 flops), [19] rotations whose two
+ * best translations lay within the near-tie tolerance and were re-scored in FP64, [20] of them,
+ * those whose translation the FP64 re-score changed. */
+#define CDK_NSTATS 21
 int cdk_ctx_stats(cdk_ctx* ctx, double* out, int n);
+
+/* The precision forms' FP64 re-score of each wave's lowest poses (the north star's top-k per
+ * rotation batch; opts.reserved[6] sets k): for the last search, *count = waves x k entries, wave
+ * by wave, each ascending in energy: rot[i] the rotation (c*nQ + q), minE[i] the search's
+ * energy, idx[i*3..] its translation, e64[i] the FP64 direct grid-energy sum of that pose
+ * (rot = -1 for slots of a wave with fewer valid rotations). Up to cap entries are copied. */
+int cdk_ctx_top_poses(cdk_ctx* ctx, int cap, int* rot, float* minE, int* idx, double* e64,
+                      int* count);
 
 #ifdef __cplusplus
 }

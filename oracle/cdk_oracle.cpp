@@ -164,6 +164,77 @@ void orc_sample_quaternions(unsigned long long seed, int nConf, int nQ, float* o
 
 void orc_srand(unsigned s) { srand(s); }
 
+// Synthetic receptor potential grids for the benchmark inputs of the reference arm (no
+// reference counterpart: the reference reads CHARMM-written grids, src/ReadGrids.cpp:6-68).
+// Same definition and operation order as the product's host generator, so the arm searches the
+// same grids without loading the product library:
+//   vdW_p(g) = min(sum_a sqrtEps_a [(Rmin/d)^12 - 2 (Rmin/d)^6], vdwCap), Rmin = r_a + r_p,
+//              d^2 clamped below at (Rmin/2)^2;
+//   elec(g)  = clamp(sum_a 332.0716 q_a / (4 max(d^2, 0.25)), +-elecCap);
+// atoms within `cutoff` of the point, visited cell by cell (cells of edge `cutoff`, the 27
+// around the point's cell in x, y, z order, atoms of a cell in index order).
+void orc_synth_receptor_grids(int n, float spacing, const float* origin, int nAtom,
+                              const float* xyz, const float* radius, const float* sqrtEps,
+                              const float* charge, int nVdw, const float* probe, float vdwCap,
+                              float elecCap, float cutoff, float* out) {
+  const size_t N = (size_t)n * n * n;
+  float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
+  for (int a = 0; a < nAtom; ++a)
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = std::min(lo[d], xyz[a * 3 + d]);
+      hi[d] = std::max(hi[d], xyz[a * 3 + d]);
+    }
+  int nc[3];
+  for (int d = 0; d < 3; ++d) nc[d] = nAtom ? std::max(1, (int)std::ceil((hi[d] - lo[d]) / cutoff) + 1) : 1;
+  std::vector<std::vector<int>> cells((size_t)nc[0] * nc[1] * nc[2]);
+  for (int a = 0; a < nAtom; ++a) {
+    int c[3];
+    for (int d = 0; d < 3; ++d) c[d] = std::min(nc[d] - 1, (int)((xyz[a * 3 + d] - lo[d]) / cutoff));
+    cells[((size_t)c[0] * nc[1] + c[1]) * nc[2] + c[2]].push_back(a);
+  }
+  const double cut2 = (double)cutoff * cutoff;
+  auto plane = [&](int i) {
+    std::vector<double> acc(nVdw + 1);
+    for (int j = 0; j < n; ++j)
+      for (int k = 0; k < n; ++k) {
+        const double p[3] = {origin[0] + (double)i * spacing, origin[1] + (double)j * spacing,
+                             origin[2] + (double)k * spacing};
+        std::fill(acc.begin(), acc.end(), 0.0);
+        int c[3];
+        for (int d = 0; d < 3; ++d)
+          c[d] = (int)std::floor(std::min(std::max((p[d] - lo[d]) / cutoff, -2.0), nc[d] + 1.0));
+        for (int cx = c[0] - 1; cx <= c[0] + 1; ++cx)
+          for (int cy = c[1] - 1; cy <= c[1] + 1; ++cy)
+            for (int cz = c[2] - 1; cz <= c[2] + 1; ++cz) {
+              if (cx < 0 || cy < 0 || cz < 0 || cx >= nc[0] || cy >= nc[1] || cz >= nc[2]) continue;
+              for (int a : cells[((size_t)cx * nc[1] + cy) * nc[2] + cz]) {
+                const double dx = p[0] - xyz[a * 3], dy = p[1] - xyz[a * 3 + 1], dz = p[2] - xyz[a * 3 + 2];
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 > cut2) continue;
+                for (int v = 0; v < nVdw; ++v) {
+                  const double rmin = (double)radius[a] + probe[v];
+                  const double dd2 = std::max(d2, 0.25 * rmin * rmin);
+                  const double s2 = rmin * rmin / dd2, s6 = s2 * s2 * s2;
+                  acc[v] += (double)sqrtEps[a] * (s6 * s6 - 2.0 * s6);
+                }
+                acc[nVdw] += 332.0716 * (double)charge[a] / (4.0 * std::max(d2, 0.25));
+              }
+            }
+        const size_t g = ((size_t)i * n + j) * n + k;
+        for (int v = 0; v < nVdw; ++v) out[v * N + g] = (float)std::min(acc[v], (double)vdwCap);
+        out[nVdw * N + g] = (float)std::max(-(double)elecCap, std::min(acc[nVdw], (double)elecCap));
+      }
+  };
+  const int nt = std::max(1, std::min(n, (int)std::thread::hardware_concurrency()));
+  std::atomic<int> next(0);
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t)
+    pool.emplace_back([&] {
+      for (int i = next++; i < n; i = next++) plane(i);
+    });
+  for (auto& th : pool) th.join();
+}
+
 // Keep q whose rotated bounding box is shorter than the grid on every axis; when more than
 // maxN pass, std::random_shuffle (rand()-driven) the kept indices and take the first maxN
 // (src/FilterQuaternions.cpp:11-83). Returns the count; out holds count*4 floats.

@@ -29,14 +29,12 @@ _dp = C.POINTER(C.c_double)
 _lp = C.POINTER(C.c_long)
 
 
-def build(ref: bool | None = None) -> None:
-    """Builds libcdk_oracle.so, and the reference libraries when the reference tree exists."""
-    targets = ["oracle"]
-    if ref is None:
-        ref = os.path.isdir("/root/reference/src")
+def build(ref: bool = True) -> None:
+    """Builds libcdk_oracle.so and, with ref, the reference libraries through build_ref.sh
+    (which does nothing where no reference checkout exists)."""
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
     if ref:
-        targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+        subprocess.run(["sh", os.path.join(HERE, "build_ref.sh")], check=True)
 
 
 def _f32(a):
@@ -81,6 +79,10 @@ def orc() -> C.CDLL:
         L.orc_rotate_bbox.argtypes = [C.c_int, _fp, C.c_int, _fp, _fp, _fp, _fp]
         L.orc_rotate.argtypes = [_fp, _fp, _fp]
         L.orc_srand.argtypes = [C.c_uint]
+        L.orc_synth_receptor_grids.argtypes = [C.c_int, C.c_float, _fp, C.c_int, _fp, _fp, _fp,
+                                               _fp, C.c_int, _fp, C.c_float, C.c_float, C.c_float,
+                                               _fp]
+        L.orc_synth_receptor_grids.restype = None
         L.orc_window.argtypes = [C.c_int, C.c_float, C.c_float]
         L.orc_window.restype = C.c_int
         L.orc_energy_map.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _fp, C.c_int,
@@ -114,6 +116,7 @@ def ref() -> C.CDLL:
         L.ref_min_max_coors.argtypes = [C.c_int, C.c_int, _fp, _fp, _fp]
         L.ref_rotate.argtypes = [_fp, _fp, _fp]
         L.ref_srand.argtypes = [C.c_uint]
+        L.ref_sort_index.argtypes = [C.c_int, _fp, _lp]
         L.ref_read_grids.argtypes = [C.c_char_p, _ip, _fp, _fp, C.c_long, _fp, C.c_long]
         L.ref_read_grids.restype = C.c_int
         _ref = L
@@ -128,6 +131,8 @@ def refcufft() -> C.CDLL:
                                       C.c_int, _fp, _fp, _fp, _fp, C.c_int, _fp, C.c_int, _fp,
                                       _ip, _dp]
         L.refcufft_search.restype = C.c_int
+        L.refcufft_kernels.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _fp, _fp, _fp, _fp]
+        L.refcufft_kernels.restype = C.c_int
         _refcufft = L
     return _refcufft
 
@@ -287,3 +292,75 @@ def kabsch_rmsd(a, b):
     lam = s[0] + s[1] + d * s[2]
     e = ((a * a).sum() + (b * b).sum() - 2.0 * lam) / len(a)
     return float(np.sqrt(max(e, 0.0)))
+
+
+# ------------------------------------------------------------------ inputs without the product
+def synth_receptor_grids(n, spacing, origin, xyz, radius, sqrt_eps, charge, probe_radii,
+                         vdw_cap=3.0, elec_cap=40.0, cutoff=12.0):
+    """Receptor potential grids [len(probe_radii)+1, n, n, n] (orc_synth_receptor_grids)."""
+    p = _f32(probe_radii)
+    xyz = _f32(xyz).reshape(-1, 3)
+    out = np.empty((p.shape[0] + 1, n, n, n), np.float32)
+    orc().orc_synth_receptor_grids(n, float(spacing), _pf(_f32(origin)), xyz.shape[0], _pf(xyz),
+                                   _pf(_f32(radius)), _pf(_f32(sqrt_eps)), _pf(_f32(charge)),
+                                   p.shape[0], _pf(p), float(vdw_cap), float(elec_cap),
+                                   float(cutoff), _pf(out))
+    return out
+
+
+def reference_inputs(name, seed=0, n_conf=None, n_q=None, n_atoms=None, ligand_radius=None):
+    """The benchmark workload built without the product library, for the reference arm: the
+    same seeds and shapes as cdocker_b200.synth.make_workload (its numpy ligand and conformer
+    generators are imported; they load no library), receptor grids from
+    orc_synth_receptor_grids, quaternion sampling and vdW slots from the reference's own helpers
+    (oracle/_ref) -- or their restatements here when _ref is absent -- and the filter check
+    from the restatement.
+    Returns a dict with grids [K,n,n,n], all_grids, coor, charge, eps, radii, slot, quats,
+    spacing, length, grid_radii."""
+    from cdocker_b200 import synth as S  # numpy only: make_ligand, make_conformers, constants
+    n, n_rec, box, n_lig, lig_r, conf_default, q_default = S.CONFIGS[name]
+    n_lig = n_lig if n_atoms is None else n_atoms
+    lig_r = lig_r if ligand_radius is None else ligand_radius
+    n_conf = conf_default if n_conf is None else n_conf
+    n_q = q_default if n_q is None else n_q
+    spacing = 0.5
+    rng = np.random.default_rng(seed)
+    xyz = rng.uniform(0.0, box, size=(n_rec, 3)).astype(np.float32)
+    radius = rng.uniform(1.5, 2.0, n_rec).astype(np.float32)
+    sqrt_eps = np.sqrt(rng.uniform(0.05, 0.2, n_rec)).astype(np.float32)
+    charge_r = rng.normal(0.0, 0.3, n_rec).astype(np.float32)
+    mid = np.full(3, box / 2, np.float32)
+    length = np.full(3, (n - 1) * spacing, np.float32)
+    origin = (mid - length / 2).astype(np.float32)
+    all_grids = synth_receptor_grids(n, spacing, origin, xyz, radius, sqrt_eps, charge_r,
+                                     S.PROBE_RADII)
+    lxyz, radii, eps, charge = S.make_ligand(n_lig, lig_r, seed + 1)
+    coor = S.make_conformers(lxyz, n_conf, seed + 2)
+    use_ref = ref_available()
+    g = _f32(S.PROBE_RADII)
+    r = _f32(radii)
+    used = np.empty(g.shape[0], np.int32)
+    slot = np.empty(r.shape[0], np.int32)
+    if use_ref:
+        nu = ref().ref_vdw_slots(r.shape[0], _pf(r), g.shape[0], _pf(g), _pi(used), _pi(slot))
+        quats = np.empty((n_conf, n_q, 4), np.float32)
+        ref().ref_quaternion_uniform_sampling(seed + 3, n_conf, n_q, _pf(quats))
+    else:
+        nu = orc().orc_vdw_slots(r.shape[0], _pf(r), g.shape[0], _pf(g), _pi(used), _pi(slot))
+        quats = sample_quaternions(seed + 3, n_conf, n_q)
+    used = used[:nu].copy()
+    for c in range(n_conf):
+        qc = _f32(quats[c])
+        out = np.empty_like(qc)
+        cc = _f32(coor[c])
+        # the restated filter (pinned bit-exact to the reference's in tests): the reference's
+        # own prints its count to stdout, which would interleave with the bench's JSON line
+        kept = orc().orc_filter_quaternions(_pf(cc), cc.shape[0], n_q, _pf(qc), float(length[0]),
+                                            float(length[1]), float(length[2]), n_q, _pf(out))
+        if kept != n_q:
+            raise RuntimeError(f"conformer {c}: only {kept} of {n_q} rotations fit")
+    grids = np.ascontiguousarray(np.concatenate([all_grids[used], all_grids[-1:]], axis=0))
+    return {"grids": grids, "all_grids": all_grids, "coor": coor, "charge": charge, "eps": eps,
+            "radii": radii, "slot": slot, "used": used, "quats": quats, "spacing": spacing,
+            "length": length, "grid_radii": S.PROBE_RADII.copy(), "n": n,
+            "source": "oracle/_ref (reference helpers)" if use_ref else "oracle restatement"}

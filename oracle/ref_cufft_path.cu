@@ -196,4 +196,51 @@ done:
 #undef RC_CHECK
 }
 
+// The reference's kernel.h pair on given spectra, launched as the driver launches them
+// (src/TranRotaConfSearchNoMini.cu:232-239, :423-426): ConjMult over the Q x K ligand spectra,
+// then SumGrids into Q summed spectra. Host arrays of interleaved complex floats in and out:
+// pot [K][odist], lig [Q][K][odist] (ConjMult's in-place result is written back to lig_out),
+// sum_out [Q][odist]. The device buffers are padded to the launches' extents (no bounds checks
+// in src/kernel.cu) and zero-filled beyond the data. Returns 0 or the failing line.
+#define RC_CHECK(x)      \
+  do {                   \
+    if ((x) != 0) {      \
+      status = __LINE__; \
+      goto done;         \
+    }                    \
+  } while (0)
+int refcufft_kernels(int odist, int K, int Q, int idist, const float* pot, const float* lig,
+                     float* lig_out, float* sum_out) {
+  const size_t launchConj = ((size_t)Q * K * odist / (1024 * 1024) + 1) * 1024 * 1024;
+  const size_t launchSum = ((size_t)Q * odist / (1024 * 1024) + 1) * 1024 * 1024;
+  const size_t sumReadQ = (launchSum - 1) / odist + 1;
+  size_t ligElems = launchConj;
+  if (sumReadQ * K * odist > ligElems) ligElems = sumReadQ * K * odist;
+  if ((size_t)Q * K * odist > ligElems) ligElems = (size_t)Q * K * odist;
+  cufftComplex *d_pot = nullptr, *d_lig = nullptr, *d_sum = nullptr;
+  int status = 0;
+  {
+    RC_CHECK(cudaMalloc((void**)&d_pot, sizeof(cufftComplex) * K * odist));
+    RC_CHECK(cudaMalloc((void**)&d_lig, sizeof(cufftComplex) * ligElems));
+    RC_CHECK(cudaMalloc((void**)&d_sum, sizeof(cufftComplex) * launchSum));
+    RC_CHECK(cudaMemset(d_lig, 0, sizeof(cufftComplex) * ligElems));
+    RC_CHECK(cudaMemcpy(d_pot, pot, sizeof(cufftComplex) * K * odist, cudaMemcpyHostToDevice));
+    RC_CHECK(cudaMemcpy(d_lig, lig, sizeof(cufftComplex) * (size_t)Q * K * odist, cudaMemcpyHostToDevice));
+    dim3 thrConj(1024, 1, 1), blkConj((unsigned)((size_t)Q * K * odist / (1024 * 1024) + 1), 1024, 1);
+    dim3 thrSum(1024, 1, 1), blkSum((unsigned)((size_t)Q * odist / (1024 * 1024) + 1), 1024, 1);
+    ConjMult<<<blkConj, thrConj>>>(d_pot, d_lig, odist, K);
+    RC_CHECK(cudaGetLastError());
+    RC_CHECK(cudaMemcpy(lig_out, d_lig, sizeof(cufftComplex) * (size_t)Q * K * odist, cudaMemcpyDeviceToHost));
+    SumGrids<<<blkSum, thrSum>>>(d_lig, d_sum, K, odist, idist);
+    RC_CHECK(cudaGetLastError());
+    RC_CHECK(cudaMemcpy(sum_out, d_sum, sizeof(cufftComplex) * (size_t)Q * odist, cudaMemcpyDeviceToHost));
+  }
+done:
+  cudaFree(d_pot);
+  cudaFree(d_lig);
+  cudaFree(d_sum);
+  return status;
+}
+#undef RC_CHECK
+
 }  // extern "C"

@@ -13,6 +13,13 @@
 #include <string>
 #include <vector>
 
+// GeneDiverseConformations.h declares the conformer generator on OpenBabel and OpenMM types
+// (absent here); declaring the two classes lets the header's own sort_index template compile
+namespace OpenBabel { class OBMol; }
+namespace OpenMM { class System; }
+#include <algorithm>
+using std::sort;  // the header calls sort unqualified, as its includers bring it in
+#include "GeneDiverseConformations.h"
 #include "FillLigandGrid.h"
 #include "FilterQuaternions.h"
 #include "GetIdxOfAtomsForVdwRadius.h"
@@ -25,6 +32,12 @@
 extern "C" {
 
 void ref_srand(unsigned s) { srand(s); }
+
+// the reference's sort_index<float> (include/GeneDiverseConformations.h:9-20)
+void ref_sort_index(int n, const float* v, long* out) {
+  const std::vector<size_t> id = sort_index<float>(std::vector<float>(v, v + n));
+  for (int i = 0; i < n; ++i) out[i] = (long)id[i];
+}
 
 void ref_rotate(const float* q, const float* v, float* out) { Rotate(q, v, out); }
 

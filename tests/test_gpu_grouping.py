@@ -1,4 +1,4 @@
-"""Rotation grouping of the streamed tensor-core x pass: the search sorts its rotation list so
+"""Rotation grouping of the tensor-core x pass: the search sorts its rotation list so
 that rotations whose channels reach the same 8-plane chunks of the ligand box share 128-rotation
 tiles. Chunks a rotation does not touch add exact zeros, so grouping must change no result --
 checked bit for bit against the ungrouped order -- while the tiles issue fewer K-steps."""
@@ -20,7 +20,7 @@ def test_grouping_changes_no_result(form, grids_cache):
                       group_rotations=grouped) as rec:
             e, i = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
             st = rec.stats()
-        assert st["xpass_kind"].startswith("tcgen05_streamed")
+        assert st["xpass_kind"].startswith("tcgen05_hankel")
         out[grouped] = (e, i, st["tensor_steps"])
     (eg, ig, sg), (eu, iu, su) = out[True], out[False]
     assert np.array_equal(eg.view(np.uint32), eu.view(np.uint32))

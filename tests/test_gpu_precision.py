@@ -15,16 +15,19 @@ pytestmark = pytest.mark.gpu
 TOL_TC = 1e-3
 
 
+HANKEL = {CDK_FORM_BF16X3: "tcgen05_hankel", CDK_FORM_FP16X2: "tcgen05_hankel_fp16"}
+
+
 @pytest.mark.parametrize("form", [CDK_FORM_BF16X3, CDK_FORM_FP16X2])
-@pytest.mark.parametrize("name,nconf,nq", [("c0_32", 1, 500), ("c1_64", 4, 25), ("c4_128", 1, 4)])
+@pytest.mark.parametrize("name,nconf,nq", [("c0_32", 1, 500), ("c1_64", 4, 25), ("c3_96", 2, 32),
+                                           ("c4_128", 2, 32)])
 def test_tc_form_vs_fp64(name, nconf, nq, form, grids_cache):
-    """Both tensor-core forms against FP64; the split-FP16 form runs its own kernel at 64^3 and
-    the split-BF16 kernels at the other grid sizes."""
+    """Both tensor-core forms against FP64 at every grid size, every rotation checked (64 at
+    96^3 and at 128^3); both run the tcgen05 x pass with the resident Hankel operator."""
     w = synth.make_workload(name, seed=5, n_conf=nconf, n_q=nq, grids_cache=grids_cache)
     with Receptor(w.grids, w.spacing, form=form) as rec:
         minE, idx = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
-        if form == CDK_FORM_FP16X2 and name == "c1_64":
-            assert rec.stats()["xpass_kind"] == "tcgen05_streamed_fp16"
+        assert rec.stats()["xpass_kind"] == HANKEL[form]
     _, ridx, r64 = O.search_direct(w.grids, w.spacing, w.coor, w.charge, w.eps, w.slot, w.quats,
                                    prec=1)
     qq = w.quats.reshape(-1, 4)
@@ -61,54 +64,69 @@ def test_fp64_rescore_of_top_poses(c0):
 
 @pytest.mark.parametrize("wave", [0, 200])
 def test_tensor_core_variants_agree(grids_cache, wave):
-    """tcgen05 with streamed operands (default at 64^3: both operands in shared memory; or the
-    ligand in tensor memory), tcgen05 with in-kernel operand builds and mma.sync apply the
-    same split-BF16 operator; ragged waves (200 rotations: a partial 128-rotation tile)
-    included."""
+    """tcgen05 with the resident Hankel operator (the default; one and two columns per CTA),
+    tcgen05 with streamed operator tiles, tcgen05 with in-kernel operand builds and mma.sync
+    apply the same split-BF16 operator; ragged waves (200 rotations: a partial 128-rotation
+    tile) included."""
     w = synth.make_workload("c1_64", seed=8, n_conf=2, n_q=150, grids_cache=grids_cache)
     out = {}
-    for name, kw in [("streamed", {}), ("streamed_tmem", {"tc_tmem_ligand": True}),
-                     ("build", {"tc_build": True}), ("mma_sync", {"tc_mma_sync": True})]:
+    kinds = {"hankel": "tcgen05_hankel", "hankel_1col": "tcgen05_hankel",
+             "hankel_2col": "tcgen05_hankel", "stream_tiles": "tcgen05_streamed",
+             "build": "tcgen05_build", "mma_sync": "mma_sync"}
+    for name, kw in [("hankel", {}), ("hankel_1col", {"tc_cols": 1}), ("hankel_2col", {"tc_cols": 2}),
+                     ("stream_tiles", {"tc_stream_tiles": True}), ("build", {"tc_build": True}),
+                     ("mma_sync", {"tc_mma_sync": True})]:
         with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3, wave_rotations=wave, **kw) as r:
             out[name] = r.search(w.coor, w.charge, w.eps, w.slot, w.quats)
-            kind = r.stats()["xpass_kind"]
-        assert kind == {"streamed": "tcgen05_streamed", "streamed_tmem": "tcgen05_streamed_tmem",
-                        "build": "tcgen05_build", "mma_sync": "mma_sync"}[name]
-    es, is_ = out["streamed"]
-    # the two streamed kernels run the same MMAs in the same order: bit-identical
-    assert np.array_equal(es, out["streamed_tmem"][0]) and np.array_equal(is_, out["streamed_tmem"][1])
-    for other in ("build", "mma_sync"):
+            st = r.stats()
+        assert st["xpass_kind"] == kinds[name]
+        if name.startswith("hankel_"):
+            assert st["col_tile"] == int(name[-4])
+    es, is_ = out["hankel"]
+    # one or two columns per CTA: the same MMAs per column, bit-identical
+    for v in ("hankel_1col", "hankel_2col"):
+        assert np.array_equal(es, out[v][0]) and np.array_equal(is_, out[v][1])
+    for other in ("stream_tiles", "build", "mma_sync"):
         eo, io = out[other]
         assert rel_err(es, eo).max() <= 1e-5
         assert np.mean(np.all(is_ == io, axis=1)) >= 0.99
 
 
 def test_streamed_falls_back_for_large_ligands(grids_cache):
-    """Ligands above 96 atoms take the FFT plane path, which writes no split rows: the context
-    picks the in-kernel-build tcgen05 x pass for them and stays correct."""
+    """Ligands above 96 atoms take the FFT plane path, which writes no split rows: a split-BF16
+    context picks the in-kernel-build tcgen05 x pass for them and stays correct; a split-FP16
+    context refuses them with CDK_ERR_UNSUPPORTED instead of switching form silently."""
     w = synth.make_workload("c1_64", seed=9, n_conf=1, n_q=20, grids_cache=grids_cache,
                             n_atoms=110)
     with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3) as rtc, \
             Receptor(w.grids, w.spacing) as r32:
         etc, itc = rtc.search(w.coor, w.charge, w.eps, w.slot, w.quats)
-        assert rtc.stats()["xpass_kind"] != "tcgen05_streamed"
+        assert rtc.stats()["xpass_kind"] == "tcgen05_build"
         e32, i32 = r32.search(w.coor, w.charge, w.eps, w.slot, w.quats)
     assert rel_err(etc, e32).max() <= TOL_TC
+    from cdocker_b200 import _lib as L
+    with Receptor(w.grids, w.spacing, form=CDK_FORM_FP16X2) as r16:
+        with pytest.raises(L.CdkError) as e:
+            r16.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+        assert e.value.code == L.CDK_ERR_UNSUPPORTED
 
 
 @pytest.mark.parametrize("form", [CDK_FORM_BF16X3, CDK_FORM_FP16X2])
-@pytest.mark.parametrize("n_atoms,radius,n_q,wave", [(6, 1.2, 40, 0),    # box 7 planes: one K-step, 6-stage ring
-                                                     (60, 6.8, 12, 0),   # box 30 planes: 4-column shape
-                                                     (40, 4.7, 37, 29)])  # ragged waves (not multiples of 8)
-def test_streamed_shapes_vs_fp64(grids_cache, n_atoms, radius, n_q, wave, form):
-    """The streamed tensor-core x pass of both forms across ligand boxes (1 to 4 K-steps, both
-    CTA shapes) and ragged waves, against the FP64 oracle."""
-    w = synth.make_workload("c1_64", seed=31, n_conf=1, n_q=n_q, grids_cache=grids_cache,
+@pytest.mark.parametrize("name,n_atoms,radius,n_q,wave",
+                         [("c1_64", 6, 1.2, 40, 0),     # box 7 planes: one K-step
+                          ("c1_64", 60, 6.8, 12, 0),    # box 30 planes: four K-steps
+                          ("c1_64", 40, 4.7, 37, 29),   # ragged waves (not multiples of 8)
+                          ("c4_128", 6, 1.2, 20, 0),    # 128^3: one K-step, windows near n
+                          ("c4_128", 60, 6.8, 12, 5),   # 128^3: four K-steps, 5-rotation waves
+                          ("c3_96", 30, 4.4, 21, 0)])   # 96^3
+def test_streamed_shapes_vs_fp64(grids_cache, name, n_atoms, radius, n_q, wave, form):
+    """The tensor-core x pass of both forms across ligand boxes (1 to 4 K-steps), grid sizes and
+    ragged waves, against the FP64 oracle."""
+    w = synth.make_workload(name, seed=31, n_conf=1, n_q=n_q, grids_cache=grids_cache,
                             n_atoms=n_atoms, ligand_radius=radius)
     with Receptor(w.grids, w.spacing, form=form, wave_rotations=wave) as rec:
         minE, idx = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
-        assert rec.stats()["xpass_kind"] == ("tcgen05_streamed_fp16" if form == CDK_FORM_FP16X2
-                                             else "tcgen05_streamed")
+        assert rec.stats()["xpass_kind"] == HANKEL[form]
     _, ridx, r64 = O.search_direct(w.grids, w.spacing, w.coor, w.charge, w.eps, w.slot, w.quats,
                                    prec=1)
     qq = w.quats.reshape(-1, 4)
@@ -135,3 +153,64 @@ def test_fp16_form_rejects_ligands_outside_its_range(grids_cache):
     with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3) as rec:
         minE, _ = rec.search(w.coor, big, w.eps, w.slot, w.quats)
         assert np.all(np.isfinite(minE))
+
+
+@pytest.mark.parametrize("form", [CDK_FORM_FP16X2, CDK_FORM_BF16X3])
+def test_fp64_near_tie_break(grids_cache, form):
+    """The precision forms re-score a rotation's two best translations in FP64 when they lie
+    within the near-tie tolerance and keep the lower: against the same search without the tie
+    break, every changed translation is at least as low in FP64, and agreement with the FP64
+    oracle's argmin does not drop."""
+    w = synth.make_workload("c1_64", seed=41, n_conf=3, n_q=200, grids_cache=grids_cache)
+    res = {}
+    for tb in (True, False):
+        with Receptor(w.grids, w.spacing, form=form, tie_break=tb) as rec:
+            e, i = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+            st = rec.stats()
+            res[tb] = (e, i, st)
+    (e1, i1, st1), (e0, i0, st0) = res[True], res[False]
+    assert st1["near_ties_rescored"] >= st1["near_ties_changed"] >= 0
+    assert st0["near_ties_rescored"] == 0
+    changed = np.nonzero(np.any(i1 != i0, axis=1))[0]
+    assert changed.size == st1["near_ties_changed"]
+    qq = w.quats.reshape(-1, 4)
+    if changed.size:
+        with Receptor(w.grids, w.spacing, form=form) as rec:
+            rc = (changed // 200).astype(np.int32)
+            f1 = rec.rescore_fp64(w.coor, w.charge, w.eps, w.slot, rc, qq[changed], i1[changed])
+            f0 = rec.rescore_fp64(w.coor, w.charge, w.eps, w.slot, rc, qq[changed], i0[changed])
+        assert np.all(f1 <= f0)
+    sel = np.arange(0, 600, 5)
+    _, ridx, r64 = O.search_direct(w.grids, w.spacing, w.coor, w.charge, w.eps, w.slot, w.quats,
+                                   prec=1)
+    agree1 = np.mean(np.all(i1[sel] == ridx[sel], axis=1))
+    agree0 = np.mean(np.all(i0[sel] == ridx[sel], axis=1))
+    assert agree1 >= agree0
+    assert rel_err(e1, r64).max() <= TOL_TC
+
+
+def test_top_poses_rescored_per_wave(grids_cache):
+    """Per wave, the k lowest-energy poses with their FP64 re-score (cdk_ctx_top_poses): the
+    rotations are the k smallest minima of their wave, the FP64 energies equal the oracle's
+    double energy map at those poses."""
+    w = synth.make_workload("c1_64", seed=42, n_conf=1, n_q=250, grids_cache=grids_cache)
+    k = 8
+    with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3, wave_rotations=100, top_k=k) as rec:
+        e, i = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+        rot, te, tidx, e64 = rec.top_poses()
+        st = rec.stats()
+    assert st["waves"] == 3 and rot.shape[0] == 3 * k
+    qq = w.quats.reshape(-1, 4)
+    for wv in range(3):
+        lo, hi = 100 * wv, min(250, 100 * (wv + 1))
+        want = np.sort(e[lo:hi])[:k]
+        got = rot[wv * k:(wv + 1) * k]
+        assert np.all((got >= lo) & (got < hi))
+        assert np.array_equal(np.sort(e[got]), want)
+        assert np.array_equal(te[wv * k:(wv + 1) * k], e[got])
+        assert np.array_equal(tidx[wv * k:(wv + 1) * k], i[got])
+    for j in range(0, 3 * k, 5):
+        r = int(rot[j])
+        emap = O.energy_map(w.grids, w.spacing, w.coor[0], w.charge, w.eps, w.slot, qq[r])
+        ref = emap[tuple(tidx[j])]
+        assert abs(e64[j] - ref) <= 1e-9 * max(1.0, abs(ref))
