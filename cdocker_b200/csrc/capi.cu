@@ -142,6 +142,8 @@ struct cdk_ctx {
   cudaGraphExec_t gexec = nullptr;
   // autotuned x-pass configuration (opts.reserved[2] = 1), per (Lb)
   int tuned_Lb = -1, tuned_col_tile = 0, tuned_chunk = 0;
+  // autotuned tensor-core x pass (Hankel operator), per (Lb, form): columns per CTA, ring cap
+  int tuned_hx_Lb = -1, tuned_hx_cols = 0, tuned_hx_nb = 0;
   double tune_ms[8] = {};
   double stats[CDK_NSTATS] = {};
 };
@@ -219,6 +221,60 @@ int autotune_xpass(cdk_ctx* c, WaveArgs a, const RotDesc* d_rots, long nRot, int
   return CDK_OK;
 }
 
+// Times the Hankel tensor-core x pass on the search's first wave (rotations in the order the
+// waves use) under each candidate shape -- one or two columns per CTA (n <= 64), ring caps of
+// 8, 16 and 32 stages -- and keeps the fastest for this ligand box. The candidates run the same
+// MMAs per column in the same order, so the results are identical whichever wins.
+int autotune_hankel(cdk_ctx* c, WaveArgs a, const RotDesc* order, long nRot, int wave, bool f16,
+                    const float* osc, cudaStream_t s) {
+  a.nrot = (int)std::min<long>(wave, nRot);
+  a.rots = order;
+  CDK_CUDA(launch_prep(a, s));
+  CDK_CUDA(launch_spread_yz(a, s));
+  struct Cand { int cols, nb; };
+  std::vector<Cand> cands;
+  for (int cols : {1, 2})
+    for (int nb : {8, 16, 32}) {
+      HankelPlan p{};
+      if (!hankel_plan(c->n, c->K, a.Lb, f16, cols, &p, nb) || p.cols != cols) continue;
+      bool dup = false;
+      for (const Cand& q : cands) dup |= (q.cols == cols && q.nb == p.nb);
+      if (!dup) cands.push_back({cols, p.nb});
+    }
+  if (cands.empty()) return CDK_OK;
+  cudaEvent_t e0, e1;
+  CDK_CUDA(cudaEventCreate(&e0));
+  CDK_CUDA(cudaEventCreate(&e1));
+  double best = 1e30;
+  Cand pick = cands[0];
+  int i = 0;
+  for (const Cand& cd : cands) {
+    HankelPlan p{};
+    hankel_plan(c->n, c->K, a.Lb, f16, cd.cols, &p, cd.nb);
+    float ms = 0.f, total = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {
+      CDK_CUDA(cudaEventRecord(e0, s));
+      CDK_CUDA(launch_xpass_hankel(a, c->d_ptilde, osc, p, s));
+      CDK_CUDA(cudaEventRecord(e1, s));
+      CDK_CUDA(cudaEventSynchronize(e1));
+      CDK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (rep == 1) total = ms;  // second run: warm caches
+    }
+    if (i < 8) c->tune_ms[i] = total;
+    ++i;
+    if (total < best) {
+      best = total;
+      pick = cd;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->tuned_hx_Lb = a.Lb;
+  c->tuned_hx_cols = pick.cols;
+  c->tuned_hx_nb = pick.nb;
+  return CDK_OK;
+}
+
 // the search proper on device tables; nRot rotations, outputs indexed by RotDesc.out
 int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const ConfDesc* d_confs,
               const RotDesc* d_rots, long nRot, int maxAtoms, int Lb, float* d_minE, int* d_idx,
@@ -231,7 +287,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   // Hankel-operator kernel at every n (box <= 32 planes, operator fits shared memory); the older
   // 64^3 kernel with streamed operator tiles on request (reserved[3] = 3)
   WaveArgs probe{};
-  probe.kyof = (c->opts.reserved[1] == 0) ? c->d_kyof : nullptr;
+  probe.kyof = (c->opts.reserved[1] & 1) ? nullptr : c->d_kyof;
   probe.max_atoms = maxAtoms;
   probe.atom_cap = maxAtoms;
   const int variant = c->opts.reserved[3];
@@ -322,7 +378,8 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   // the shared-memory streamed x pass writes B in plane groups (whole sectors per store)
   a.bgroup = rows ? stream_bgroup() : 1;
   a.col_tile = c->opts.col_tile > 0 ? c->opts.col_tile : pick_col_tile(n, K);
-  a.kyof = (c->opts.reserved[1] == 0) ? c->d_kyof : nullptr;  // reserved[1] = 1: FFT planes
+  a.kyof = (c->opts.reserved[1] & 1) ? nullptr : c->d_kyof;  // reserved[1] bit 0: FFT planes
+  a.yz_block_stages = (c->opts.reserved[1] & 2) ? 1 : 0;       // bit 1: block-stage yz kernel
   a.chunk = 0;
   if (c->tuned_Lb == Lb) {
     if (c->tuned_col_tile) a.col_tile = c->tuned_col_tile;
@@ -381,6 +438,12 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     order = sorted;
     launches += 4;
   }
+  if (hankel && c->opts.reserved[2] && c->tuned_hx_Lb != Lb) {
+    int rc = autotune_hankel(c, a, order, nRot, wave, f16form, osc.data(), s);
+    if (rc) return rc;
+  }
+  if (hankel && c->tuned_hx_Lb == Lb && c->tuned_hx_cols > 0)
+    hankel_plan(n, K, Lb, f16form, c->tuned_hx_cols, &hp, c->tuned_hx_nb);
   for (long r0 = 0; r0 < nRot; r0 += wave) {
     a.nrot = (int)std::min<long>(wave, nRot - r0);
     a.rots = order + r0;
@@ -488,7 +551,9 @@ int search_device_impl(cdk_ctx* c, int nAtom, int nConf, const float* d_coor,
   // CUDA graph: the first search of a shape runs plainly (growing the scratch), the second
   // captures build-tables + every wave into one graph, later ones replay it
   cdk_ctx::GraphKey key{{d_coor, d_charge, d_eps, d_slot, d_quats, d_minE, d_idx}, nAtom, nConf, nQ, Lb, s};
-  const bool graphs = c->opts.use_graphs != 0 && !(c->opts.reserved[2] && c->tuned_Lb != Lb);
+  // a search that autotunes (a new ligand box) runs plainly: timing runs do not go into graphs
+  const bool graphs = c->opts.use_graphs != 0 && !(c->opts.reserved[2] && c->tuned_Lb != Lb &&
+                                                   c->tuned_hx_Lb != Lb);
   if (graphs && c->gkey_seen == 2 && c->gkey == key) {
     CDK_CUDA(cudaGraphLaunch(c->gexec, s));
     CDK_CUDA(cudaEventRecord(c->ev1, s));
@@ -586,7 +651,7 @@ bool ctx_view(const cdk_ctx* c, CtxView* v) {
   v->max_atoms = c->opts.max_atoms;
   v->phat = c->d_phat;
   v->tw = c->d_tw;
-  v->kyof = (c->opts.reserved[1] == 0) ? c->d_kyof : nullptr;
+  v->kyof = (c->opts.reserved[1] & 1) ? nullptr : c->d_kyof;
   v->h_misc = c->h_misc;
   v->stream = c->stream;
   v->form = c->opts.form;

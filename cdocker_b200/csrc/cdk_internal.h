@@ -74,6 +74,7 @@ struct WaveArgs {
   float2* B;                 // [nrot][n][ncol], or with bgroup G > 1 [nrot][n/G][ncol/2][G][2]:
                              // the x planes grouped by G, 16 B (two columns) per (plane, pair)
   int bgroup;                // 0 or 1: plain B layout; 2, 4, 8: grouped (streamed x pass only)
+  int yz_block_stages;       // n = 64: 1 runs the block-stage yz kernel instead of the octet one
   unsigned long long* keys;  // [nrot]
   unsigned long long* keys2; // precision forms' near-tie break: [nrot][n][2] the two smallest
                              // keys of every window plane (null: not kept)
@@ -179,7 +180,8 @@ struct HankelPlan {
   size_t smem;      // dynamic shared memory per CTA
   int ctas_per_sm;  // 1 or 2
 };
-bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out);
+// nb_cap > 0: at most that many ring stages (the autotuner's candidates)
+bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out, int nb_cap = 0);
 cudaError_t launch_xpass_hankel(const WaveArgs& a, const float2* pt, const float* f16_scale,
                                 const HankelPlan& p, cudaStream_t s);
 // the stage plan of every 128-rotation tile of a wave into the tile's first RotRec

@@ -492,7 +492,9 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
   }
 }
 
-constexpr size_t kSmemCap = 227 * 1024;   // dynamic shared memory of one CTA
+// shared memory of one CTA: 227 KB in all, of which the kernel's static barriers and flags
+// take 1 KB (ptxas) -- the dynamic part's cap
+constexpr size_t kSmemCap = 227 * 1024 - 1024;
 constexpr size_t kSmemHalf = 110 * 1024;  // per CTA when two share an SM
 
 template <int N, int COLS, bool F16>
@@ -514,7 +516,7 @@ cudaError_t launch_hx(const WaveArgs& a, const float2* pt, const HxScale& sc, in
 // and dynamic shared memory. cols_pref: 0 = automatic, 1 or 2 = that many columns (2 only where
 // the operator of two columns fits). Returns false when the operator and a minimal ring do not
 // fit one CTA (large K at large n) or the box exceeds 32 planes.
-bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out) {
+bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out, int nb_cap) {
   if (!(n == 32 || n == 64 || n == 96 || n == 128) || K < 1 || K > KMAX || Lb < 1 || Lb > 8 * HX_JMAX)
     return false;
   const int jc = (Lb + 7) / 8;
@@ -529,8 +531,9 @@ bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out)
     for (int pass = two ? 0 : 1; pass < 2; ++pass) {
       const size_t cap = (pass == 0 ? kSmemHalf : kSmemCap) - 1024;
       if (cap <= L.op) continue;
-      const int nb = (int)std::min<size_t>(HX_MAXSTAGES, (cap - L.op) / L.stage);
+      int nb = (int)std::min<size_t>(HX_MAXSTAGES, (cap - L.op) / L.stage);
       if (nb < (pass == 0 ? 8 : 4) || (size_t)nb * L.stage < L.build) continue;
+      if (nb_cap > 0 && nb_cap < nb && (size_t)nb_cap * L.stage >= L.build) nb = nb_cap;
       out->cols = cols;
       out->G = G;
       out->jc = jc;

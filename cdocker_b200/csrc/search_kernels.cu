@@ -905,6 +905,143 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
   }
 }
 
+// Inverse (y,z) of one (rotation, x in window) plane + min / first argmin at n = 64 with warp-local
+// line transforms: an octet of 8 lanes owns one line (a kz column for y, a packed row pair for
+// z); lane t holds 8 values, the first radix-8 stage runs in its registers, the 8 x 8 exchange
+// between the two stages goes through the warp's own shared-memory slice (__syncwarp only),
+// and the second radix-8 stage (twiddles tw[t k]) yields natural index t + 8 j. The only
+// block-wide barriers: after the twiddle load, between the y and z passes, and in the final
+// reduction. Same radix stages, twiddles and packing as k_yz_inv_argmin<64>.
+template <bool TOP2>
+__global__ void __launch_bounds__(256, 4) k_yz_octet64(WaveArgs a) {
+  constexpr int N = 64, NZH = N / 2 + 1, NCOL = N * NZH;
+  constexpr int XS = 9;  // padded stride of the exchange slice (8 + 1 float2 per block)
+  __shared__ float2 s_tw[N];
+  __shared__ float2 s_y[N * NZH];         // y-transformed rows Y[y][kz]
+  __shared__ float2 s_x[8][4 * 8 * XS];   // per warp: 4 octets x 8 blocks x (8 + 1)
+  __shared__ unsigned long long s_best[8], s_best2[8];
+  const int x = blockIdx.x, r = blockIdx.y;
+  const RotRec* rec = a.rec + r;
+  if (!rec->valid) return;
+  const int Wx = rec->W[0], Wy = rec->W[1], Wz = rec->W[2];
+  if (x >= Wx) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int o = lane >> 3, t = lane & 7, g = warp * 4 + o;
+  if (tid < N) s_tw[tid] = a.tw[tid];
+  const int G = a.bgroup > 1 ? a.bgroup : 1;
+  const float2* src2 = reinterpret_cast<const float2*>(
+      reinterpret_cast<const float4*>(a.B + ((size_t)r * N + (x - x % G)) * NCOL) + x % G);
+  float2* S = &s_x[warp][o * 8 * XS];
+  __syncthreads();
+  // y: column l = g (warp 0's octet 0 also takes l = 32); positions t*8 + j in, natural y out
+  for (int it = 0; it < 2; ++it) {
+    if (it == 1 && warp != 0) break;
+    const int l = g + 32 * it;
+    const bool act = l < NZH;
+    float2 v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int f = (t * 8 + j) * NZH + l;
+      v[j] = act ? src2[(size_t)(f >> 1) * 2 * G + (f & 1)] : make_float2(0.f, 0.f);
+    }
+    Radix<8, +1>::run(v);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) S[t * XS + j] = v[j];
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = S[j * XS + t];
+    __syncwarp();
+#pragma unroll
+    for (int k = 1; k < 8; ++k) v[k] = c_mulc(v[k], s_tw[t * k]);
+    Radix<8, +1>::run(v);
+    if (act) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) s_y[(t + 8 * j) * NZH + l] = v[j];
+    }
+  }
+  __syncthreads();
+  // z: rows (2p, 2p + 1) packed as one complex line, Hermitian extension over z; natural z out
+  const int npairs = (Wy + 1) / 2;
+  const int p = g;
+  const bool act = p < npairs;
+  const float inv = 1.0f / (float)((double)N * N * N);
+  unsigned long long best = ~0ull, best2 = ~0ull;
+  {
+    const float2* A = s_y + (2 * min(p, N / 2 - 1)) * NZH;
+    const float2* Bv = A + NZH;
+    float2 v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int k = t + 8 * j;  // natural frequency at digit-reversed position t*8 + j
+      if (j < 4) {
+        const float2 ak = A[k], bk = Bv[k];
+        v[j] = make_float2(ak.x - bk.y, ak.y + bk.x);
+        if (j == 0 && t == 0) v[j] = make_float2(ak.x, bk.x);  // k = 0
+      } else {
+        const int m = N - k;
+        const float2 am = A[m], bm = Bv[m];
+        v[j] = make_float2(am.x + bm.y, -am.y + bm.x);
+        if (j == 4 && t == 0) v[j] = make_float2(am.x, bm.x);  // k = N/2
+      }
+    }
+    Radix<8, +1>::run(v);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) S[t * XS + j] = v[j];
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = S[j * XS + t];
+#pragma unroll
+    for (int k = 1; k < 8; ++k) v[k] = c_mulc(v[k], s_tw[t * k]);
+    Radix<8, +1>::run(v);
+    if (act) {
+      const int y0 = 2 * p;
+      const bool row0 = y0 < Wy, row1 = y0 + 1 < Wy;
+      const unsigned int lin0 = (unsigned int)((x * N + y0) * N + t);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (t + 8 * j < Wz) {
+          const unsigned long long k0 =
+              ((unsigned long long)order_key(v[j].x * inv) << 32) | (lin0 + (unsigned int)(8 * j));
+          const unsigned long long k1 =
+              ((unsigned long long)order_key(v[j].y * inv) << 32) | (lin0 + (unsigned int)(N + 8 * j));
+          if constexpr (TOP2) {
+            if (row0) top2_insert(k0, best, best2);
+            if (row1) top2_insert(k1, best, best2);
+          } else {
+            if (row0) best = k0 < best ? k0 : best;
+            if (row1) best = k1 < best ? k1 : best;
+          }
+        }
+      }
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, off);
+    if constexpr (TOP2) {
+      const unsigned long long other2 = __shfl_xor_sync(0xffffffffu, best2, off);
+      top2_merge(other, other2, best, best2);
+    } else {
+      best = other < best ? other : best;
+    }
+  }
+  if (lane == 0) {
+    s_best[warp] = best;
+    if constexpr (TOP2) s_best2[warp] = best2;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int w = 1; w < 8; ++w) {
+      if constexpr (TOP2) top2_merge(s_best[w], s_best2[w], best, best2);
+      else best = s_best[w] < best ? s_best[w] : best;
+    }
+    atomicMin(a.keys + r, best);
+    if constexpr (TOP2) {
+      a.keys2[((size_t)r * N + x) * 2] = best;
+      a.keys2[((size_t)r * N + x) * 2 + 1] = best2;
+    }
+  }
+}
+
 // FP64 energy of rotation r at translation (ti, tj, tk): the direct trilinear grid-energy sum
 // over its rotated atoms (k_prep's rot_xyz and min corner), cells and ratios in
 // FillLigandGrid's arithmetic, accumulated in double across the warp's lanes (atoms).
@@ -1192,6 +1329,14 @@ cudaError_t launch_spread_yz_t(const WaveArgs& a, cudaStream_t s) {
 
 template <int N>
 cudaError_t launch_yz_inv_t(const WaveArgs& a, cudaStream_t s) {
+  if constexpr (N == 64) {
+    if (!a.yz_block_stages) {
+      dim3 grid(N, a.nrot);
+      if (a.keys2) k_yz_octet64<true><<<grid, 256, 0, s>>>(a);
+      else k_yz_octet64<false><<<grid, 256, 0, s>>>(a);
+      return cudaGetLastError();
+    }
+  }
   // twiddles + one plane (n <= 64: the packed rows alias it) [+ the packed rows]
   const size_t sm = sizeof(float2) * (N + N * (N / 2 + 1) + (N <= 64 ? 0 : (N / 2) * (N + 1)));
   auto kern = a.keys2 ? k_yz_inv_argmin<N, true> : k_yz_inv_argmin<N, false>;

@@ -54,8 +54,9 @@ typedef struct cdk_opts {
   int col_tile;        /* spectral columns per CTA in the x pass; 0 = autotuned default */
   int use_graphs;      /* 1 = replay each wave through a captured CUDA graph */
   int reserved[8];     /* [0] = 1: time every kernel with events (cdk_ctx_stats [8..12]);
-                          [1] = 1: spread planes through the radix FFT instead of the direct
-                          separable evaluation; [2] = 1: autotune the x pass on the first wave
+                          [1] bit 0: spread planes through the radix FFT instead of the direct
+                          separable evaluation; bit 1: at n = 64, the inverse (y,z) kernel with
+                          block-wide radix stages instead of warp-local line transforms; [2] = 1: autotune the x pass on the first wave
                           of each new ligand box; [3] precision-form x pass: 0 = tcgen05 with
                           the Hankel operator resident in shared memory and streamed ligand
                           rows where it applies (ligand box <= 32 planes, ligands <= 96 atoms,

@@ -172,3 +172,51 @@ def test_autotune_same_results(c0):
     np.testing.assert_array_equal(e0, e1)
     np.testing.assert_array_equal(i0, i1)
     assert st["col_tile"] in (8, 16) and st["rotations_per_cta"] in (16, 32, 64)
+
+
+@pytest.mark.parametrize("form", [0, 2])
+def test_yz_octet_kernel_matches_block_stages(grids_cache, form):
+    """At 64^3 the inverse (y,z) transform runs warp-local line transforms (octets of lanes);
+    the block-stage kernel runs the same radix stages, twiddles and packing, so the minima and
+    translations agree (bit for bit where the compiler keeps the same operation order)."""
+    w = synth.make_workload("c1_64", seed=3, n_conf=2, n_q=120, grids_cache=grids_cache)
+    out = []
+    for block in (False, True):
+        with Receptor(w.grids, w.spacing, form=form, yz_block_stages=block) as rec:
+            out.append(rec.search(w.coor, w.charge, w.eps, w.slot, w.quats))
+    (e0, i0), (e1, i1) = out
+    assert np.abs(e0.astype(np.float64) - e1).max() <= 1e-6 * np.abs(e1).max()
+    assert np.mean(np.all(i0 == i1, axis=1)) >= 0.99
+
+
+def test_graph_replay_tensor_core_form(grids_cache):
+    """The split-FP16 search (rotation grouping, tile plans, the Hankel x pass, the FP64
+    near-tie break and the per-wave top-pose re-score) captured into one CUDA graph and replayed:
+    the same results as the plain search every time."""
+    import torch
+    w = synth.make_workload("c1_64", seed=12, n_conf=2, n_q=150, grids_cache=grids_cache)
+    with Receptor(w.grids, w.spacing, form=2) as plain:
+        ref = _device_search(plain, w, torch, 1)[0]
+    with Receptor(w.grids, w.spacing, form=2, use_graphs=1, wave_rotations=128) as rec:
+        outs = _device_search(rec, w, torch, 4)
+        assert rec.stats()["graph_state"] == 2
+    for e, i, _, _ in outs:
+        np.testing.assert_array_equal(e, ref[0])
+        np.testing.assert_array_equal(i, ref[1])
+
+
+@pytest.mark.parametrize("form", [1, 2])
+def test_autotune_tensor_core_same_results(grids_cache, form):
+    """The autotuner times the Hankel x pass under one and two columns per CTA and several ring
+    depths on the first wave and keeps the fastest; every candidate computes the same numbers."""
+    w = synth.make_workload("c1_64", seed=13, n_conf=2, n_q=200, grids_cache=grids_cache)
+    with Receptor(w.grids, w.spacing, form=form) as plain:
+        e0, i0 = plain.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+    with Receptor(w.grids, w.spacing, form=form, autotune=True) as rec:
+        e1, i1 = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+        st = rec.stats()
+        e2, i2 = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+    np.testing.assert_array_equal(e0, e1)
+    np.testing.assert_array_equal(i0, i1)
+    np.testing.assert_array_equal(e1, e2)
+    assert st["xpass_kind"].startswith("tcgen05_hankel") and st["col_tile"] in (1, 2)
