@@ -597,12 +597,12 @@ def run_ours(args, rank, world, local_rank):
         hbm, peak_kind = _peaks()
         nc = 64 * 64 * 33  # half-spectrum points of one grid
         b_rot = 8 * 9 * 64 ** 3 + 16 * 9 * nc + 16 * nc + 8 * 64 ** 3
-        dram_rot = sum(v for k, v in traffic.items() if isinstance(v, (int, float))) if traffic else None
         traffic = {}
         tp = os.path.join(ROOT, "profiles", "dram_bytes_per_rotation.json")
         if os.path.exists(tp):
             with open(tp) as f:
                 traffic = json.load(f).get(head, {})
+        dram_rot = sum(v for v in traffic.values() if isinstance(v, (int, float))) if traffic else None
         value = H["value"]
         rps = value / world
         line = {

@@ -195,7 +195,17 @@ def test_top_poses_rescored_per_wave(grids_cache):
     double energy map at those poses."""
     w = synth.make_workload("c1_64", seed=42, n_conf=1, n_q=250, grids_cache=grids_cache)
     k = 8
+    # with the grouping sort the waves hold rotations from anywhere in the list: every wave's
+    # k lowest still include each of the search's k lowest that it holds
     with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3, wave_rotations=100, top_k=k) as rec:
+        e, i = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+        rot, te, tidx, e64 = rec.top_poses()
+    assert rot.shape[0] == 3 * k and len(set(rot.tolist())) == 3 * k
+    assert set(np.argsort(e, kind="stable")[:k].tolist()) <= set(rot.tolist())
+    assert np.array_equal(te, e[rot]) and np.array_equal(tidx, i[rot])
+    # in the given order (no grouping) wave w holds rotations [100 w, 100 w + 100)
+    with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3, wave_rotations=100, top_k=k,
+                  group_rotations=False) as rec:
         e, i = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
         rot, te, tidx, e64 = rec.top_poses()
         st = rec.stats()
