@@ -905,20 +905,33 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
   }
 }
 
-// Inverse (y,z) of one (rotation, x in window) plane + min / first argmin at n = 64 with warp-local
-// line transforms: an octet of 8 lanes owns one line (a kz column for y, a packed row pair for
-// z); lane t holds 8 values, the first radix-8 stage runs in its registers, the 8 x 8 exchange
-// between the two stages goes through the warp's own shared-memory slice (__syncwarp only),
-// and the second radix-8 stage (twiddles tw[t k]) yields natural index t + 8 j. The only
-// block-wide barriers: after the twiddle load, between the y and z passes, and in the final
-// reduction. Same radix stages, twiddles and packing as k_yz_inv_argmin<64>.
-template <bool TOP2>
-__global__ void __launch_bounds__(256, 4) k_yz_octet64(WaveArgs a) {
-  constexpr int N = 64, NZH = N / 2 + 1, NCOL = N * NZH;
-  constexpr int XS = 9;  // padded stride of the exchange slice (8 + 1 float2 per block)
-  __shared__ float2 s_tw[N];
-  __shared__ float2 s_y[N * NZH];         // y-transformed rows Y[y][kz]
-  __shared__ float2 s_x[8][4 * 8 * XS];   // per warp: 4 octets x 8 blocks x (8 + 1)
+// Inverse (y,z) of one (rotation, x in window) plane + min / first argmin with warp-local line
+// transforms, for n = 8 R1 (R1 = 4, 8, 12, 16). An octet of 8 lanes owns one line (a kz column
+// for y, a packed row pair for z). The inverse runs the forward plan's two stages backwards:
+// stage 1, radix R1 over the 8 contiguous blocks of R1 digit-reversed positions (lane t holds
+// block t in registers); stage 2, radix 8 over the R1 groups {np + R1 j} with twiddles
+// tw[np k] (lane t takes groups np = t, t + 8, ...), giving natural index np + R1 j. The
+// exchange between the stages goes through the warp's own shared-memory slice (__syncwarp
+// only). Block-wide barriers: after the twiddle load, between the y and z passes (the y output
+// is the z input), and in the final reduction. Same radix stages, twiddles and packing as
+// k_yz_inv_argmin.
+template <int N>
+constexpr size_t octet_smem() {
+  // twiddles, Y[N][N/2+1], per warp 4 octets x 8 blocks x (R1 + 1)
+  return sizeof(float2) * (N + (size_t)N * (N / 2 + 1) + 8 * 4 * 8 * (N / 8 + 1));
+}
+
+template <int N, bool TOP2>
+__global__ void __launch_bounds__(256, (N <= 64 ? 4 : 2)) k_yz_octet(WaveArgs a) {
+  constexpr int NZH = N / 2 + 1, NCOL = N * NZH;
+  constexpr int R1 = N / 8;           // stage-1 radix; stage 2 is radix 8
+  constexpr int XS = R1 + 1;          // padded block stride of the exchange slice
+  constexpr int NG = (R1 + 7) / 8;    // stage-2 groups per lane
+  static_assert(N % 8 == 0 && (R1 == 4 || R1 == 8 || R1 == 12 || R1 == 16), "n = 8 R1");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* s_tw = reinterpret_cast<float2*>(smem_raw);
+  float2* s_y = s_tw + N;                    // y-transformed rows Y[y][kz]
+  float2* s_xall = s_y + (size_t)N * NZH;    // exchange slices
   __shared__ unsigned long long s_best[8], s_best2[8];
   const int x = blockIdx.x, r = blockIdx.y;
   const RotRec* rec = a.rec + r;
@@ -927,53 +940,70 @@ __global__ void __launch_bounds__(256, 4) k_yz_octet64(WaveArgs a) {
   if (x >= Wx) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int o = lane >> 3, t = lane & 7, g = warp * 4 + o;
-  if (tid < N) s_tw[tid] = a.tw[tid];
+  for (int i = tid; i < N; i += 256) s_tw[i] = a.tw[i];
   const int G = a.bgroup > 1 ? a.bgroup : 1;
   const float2* src2 = reinterpret_cast<const float2*>(
       reinterpret_cast<const float4*>(a.B + ((size_t)r * N + (x - x % G)) * NCOL) + x % G);
-  float2* S = &s_x[warp][o * 8 * XS];
+  float2* S = s_xall + (size_t)(warp * 4 + o) * 8 * XS;
   __syncthreads();
-  // y: column l = g (warp 0's octet 0 also takes l = 32); positions t*8 + j in, natural y out
-  for (int it = 0; it < 2; ++it) {
-    if (it == 1 && warp != 0) break;
+  // the second stage of one line from the exchange slice: groups np = t + 8 q, natural output
+  // index np + R1 j -> emit(np, j, value)
+  auto stage2 = [&](auto&& emit) {
+#pragma unroll
+    for (int q = 0; q < NG; ++q) {
+      const int np = t + 8 * q;
+      if (np < R1) {
+        float2 u[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) u[j] = S[j * XS + np];
+#pragma unroll
+        for (int k = 1; k < 8; ++k) u[k] = c_mulc(u[k], s_tw[np * k]);
+        Radix<8, +1>::run(u);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) emit(np, j, u[j]);
+      }
+    }
+  };
+  // y: columns l = g, g + 32, ...; every warp runs the same number of rounds (warp-uniform)
+  constexpr int YR = (NZH + 31) / 32;
+#pragma unroll 1
+  for (int it = 0; it < YR; ++it) {
+    if (warp * 4 + 32 * it >= NZH) break;  // no octet of this warp has a column left
     const int l = g + 32 * it;
     const bool act = l < NZH;
-    float2 v[8];
+    float2 v[R1];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int f = (t * 8 + j) * NZH + l;
+    for (int j = 0; j < R1; ++j) {
+      const int f = (t * R1 + j) * NZH + l;
       v[j] = act ? src2[(size_t)(f >> 1) * 2 * G + (f & 1)] : make_float2(0.f, 0.f);
     }
-    Radix<8, +1>::run(v);
+    Radix<R1, +1>::run(v);
 #pragma unroll
-    for (int j = 0; j < 8; ++j) S[t * XS + j] = v[j];
+    for (int j = 0; j < R1; ++j) S[t * XS + j] = v[j];
     __syncwarp();
-#pragma unroll
-    for (int j = 0; j < 8; ++j) v[j] = S[j * XS + t];
+    stage2([&](int np, int j, float2 val) {
+      if (act) s_y[(np + R1 * j) * NZH + l] = val;
+    });
     __syncwarp();
-#pragma unroll
-    for (int k = 1; k < 8; ++k) v[k] = c_mulc(v[k], s_tw[t * k]);
-    Radix<8, +1>::run(v);
-    if (act) {
-#pragma unroll
-      for (int j = 0; j < 8; ++j) s_y[(t + 8 * j) * NZH + l] = v[j];
-    }
   }
   __syncthreads();
-  // z: rows (2p, 2p + 1) packed as one complex line, Hermitian extension over z; natural z out
+  // z: rows (2p, 2p + 1) packed as one complex line, Hermitian extension over z
   const int npairs = (Wy + 1) / 2;
-  const int p = g;
-  const bool act = p < npairs;
   const float inv = 1.0f / (float)((double)N * N * N);
   unsigned long long best = ~0ull, best2 = ~0ull;
-  {
+  constexpr int ZR = (N / 2 + 31) / 32;
+#pragma unroll 1
+  for (int it = 0; it < ZR; ++it) {
+    if (warp * 4 + 32 * it >= npairs) break;  // warp-uniform
+    const int p = g + 32 * it;
+    const bool act = p < npairs;
     const float2* A = s_y + (2 * min(p, N / 2 - 1)) * NZH;
     const float2* Bv = A + NZH;
-    float2 v[8];
+    float2 v[R1];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int k = t + 8 * j;  // natural frequency at digit-reversed position t*8 + j
-      if (j < 4) {
+    for (int j = 0; j < R1; ++j) {
+      const int k = t + 8 * j;  // natural frequency at digit-reversed position t R1 + j
+      if (j < R1 / 2) {
         const float2 ak = A[k], bk = Bv[k];
         v[j] = make_float2(ak.x - bk.y, ak.y + bk.x);
         if (j == 0 && t == 0) v[j] = make_float2(ak.x, bk.x);  // k = 0
@@ -981,39 +1011,31 @@ __global__ void __launch_bounds__(256, 4) k_yz_octet64(WaveArgs a) {
         const int m = N - k;
         const float2 am = A[m], bm = Bv[m];
         v[j] = make_float2(am.x + bm.y, -am.y + bm.x);
-        if (j == 4 && t == 0) v[j] = make_float2(am.x, bm.x);  // k = N/2
+        if (j == R1 / 2 && t == 0) v[j] = make_float2(am.x, bm.x);  // k = N/2
       }
     }
-    Radix<8, +1>::run(v);
+    Radix<R1, +1>::run(v);
 #pragma unroll
-    for (int j = 0; j < 8; ++j) S[t * XS + j] = v[j];
+    for (int j = 0; j < R1; ++j) S[t * XS + j] = v[j];
     __syncwarp();
-#pragma unroll
-    for (int j = 0; j < 8; ++j) v[j] = S[j * XS + t];
-#pragma unroll
-    for (int k = 1; k < 8; ++k) v[k] = c_mulc(v[k], s_tw[t * k]);
-    Radix<8, +1>::run(v);
-    if (act) {
-      const int y0 = 2 * p;
-      const bool row0 = y0 < Wy, row1 = y0 + 1 < Wy;
-      const unsigned int lin0 = (unsigned int)((x * N + y0) * N + t);
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        if (t + 8 * j < Wz) {
-          const unsigned long long k0 =
-              ((unsigned long long)order_key(v[j].x * inv) << 32) | (lin0 + (unsigned int)(8 * j));
-          const unsigned long long k1 =
-              ((unsigned long long)order_key(v[j].y * inv) << 32) | (lin0 + (unsigned int)(N + 8 * j));
-          if constexpr (TOP2) {
-            if (row0) top2_insert(k0, best, best2);
-            if (row1) top2_insert(k1, best, best2);
-          } else {
-            if (row0) best = k0 < best ? k0 : best;
-            if (row1) best = k1 < best ? k1 : best;
-          }
+    const int y0 = 2 * p;
+    const bool row0 = act && y0 < Wy, row1 = act && y0 + 1 < Wy;
+    stage2([&](int np, int j, float2 val) {
+      const int z = np + R1 * j;
+      if (z < Wz) {
+        const unsigned int lin0 = (unsigned int)((x * N + y0) * N + z);
+        const unsigned long long k0 = ((unsigned long long)order_key(val.x * inv) << 32) | lin0;
+        const unsigned long long k1 = ((unsigned long long)order_key(val.y * inv) << 32) | (lin0 + N);
+        if constexpr (TOP2) {
+          if (row0) top2_insert(k0, best, best2);
+          if (row1) top2_insert(k1, best, best2);
+        } else {
+          if (row0) best = k0 < best ? k0 : best;
+          if (row1) best = k1 < best ? k1 : best;
         }
       }
-    }
+    });
+    __syncwarp();
   }
   for (int off = 16; off > 0; off >>= 1) {
     const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, off);
@@ -1329,13 +1351,14 @@ cudaError_t launch_spread_yz_t(const WaveArgs& a, cudaStream_t s) {
 
 template <int N>
 cudaError_t launch_yz_inv_t(const WaveArgs& a, cudaStream_t s) {
-  if constexpr (N == 64) {
-    if (!a.yz_block_stages) {
-      dim3 grid(N, a.nrot);
-      if (a.keys2) k_yz_octet64<true><<<grid, 256, 0, s>>>(a);
-      else k_yz_octet64<false><<<grid, 256, 0, s>>>(a);
-      return cudaGetLastError();
-    }
+  if (!a.yz_block_stages) {
+    constexpr size_t sm = octet_smem<N>();
+    auto kern = a.keys2 ? k_yz_octet<N, true> : k_yz_octet<N, false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    dim3 grid(N, a.nrot);
+    kern<<<grid, 256, sm, s>>>(a);
+    return cudaGetLastError();
   }
   // twiddles + one plane (n <= 64: the packed rows alias it) [+ the packed rows]
   const size_t sm = sizeof(float2) * (N + N * (N / 2 + 1) + (N <= 64 ? 0 : (N / 2) * (N + 1)));

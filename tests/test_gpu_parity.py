@@ -175,11 +175,12 @@ def test_autotune_same_results(c0):
 
 
 @pytest.mark.parametrize("form", [0, 2])
-def test_yz_octet_kernel_matches_block_stages(grids_cache, form):
-    """At 64^3 the inverse (y,z) transform runs warp-local line transforms (octets of lanes);
-    the block-stage kernel runs the same radix stages, twiddles and packing, so the minima and
+@pytest.mark.parametrize("name,nq", [("c0_32", 60), ("c1_64", 120), ("c3_96", 24), ("c4_128", 12)])
+def test_yz_octet_kernel_matches_block_stages(grids_cache, form, name, nq):
+    """The inverse (y,z) transform runs warp-local line transforms (octets of lanes); the
+    block-stage kernel runs the same radix stages, twiddles and packing, so the minima and
     translations agree (bit for bit where the compiler keeps the same operation order)."""
-    w = synth.make_workload("c1_64", seed=3, n_conf=2, n_q=120, grids_cache=grids_cache)
+    w = synth.make_workload(name, seed=3, n_conf=2, n_q=nq, grids_cache=grids_cache)
     out = []
     for block in (False, True):
         with Receptor(w.grids, w.spacing, form=form, yz_block_stages=block) as rec:
