@@ -483,8 +483,12 @@ def run_ours(args, rank, world, local_rank):
         return float(t.item())
 
     def timed_form(form):
+        # config 1 as specified: searches captured into a CUDA graph (the warm-up steps autotune
+        # the x pass, grow the scratch and capture; the timed steps replay) with the x-pass shape
+        # picked by the autotuner
         rec = Receptor(w.grids, w.spacing, device=local_rank, wave_rotations=args.wave,
-                       col_tile=args.col_tile, form=form, profile=True)
+                       col_tile=args.col_tile, form=form, profile=True,
+                       use_graphs=args.graphs, autotune=bool(args.autotune))
 
         def step():
             rec.search_device(n_atom, n_conf, d_coor.data_ptr(), d_charge.data_ptr(),
@@ -619,6 +623,9 @@ def run_ours(args, rank, world, local_rank):
                        "l2": "256 MiB written between timed steps (and every step's wave "
                              "scratch is GBs, far above L2)",
                        "wave_rotations": H["stats"]["wave_rotations"],
+                       "cuda_graph": H["stats"]["graph_state"] == 2,
+                       "autotuned_xpass": {"kind": H["stats"]["xpass_kind"],
+                                           "columns_per_cta": H["stats"]["col_tile"]},
                        "parallelism": f"rotation shards x{world}"},
             "gpu_launches": int(H["stats"]["launches"] * args.steps),
             "clocks": H["clocks"],
@@ -860,7 +867,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--wave", type=int, default=0)
     ap.add_argument("--col-tile", type=int, default=0)
-    ap.add_argument("--graphs", type=int, default=0)
+    ap.add_argument("--graphs", type=int, default=1,
+                    help="1: capture each search into a CUDA graph and replay it (default)")
+    ap.add_argument("--autotune", type=int, default=1,
+                    help="1: autotune the x pass on the first search (default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--ref-cufft", type=int, default=1)

@@ -415,6 +415,12 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     }
   }
   c->kev_used = 0;
+  // inside a stream capture the per-kernel events become external event-record nodes of the
+  // graph (a plain record there would only order the capture), so replays record them too
+  cudaStreamCaptureStatus cap_state = cudaStreamCaptureStatusNone;
+  CDK_CUDA(cudaStreamIsCapturing(s, &cap_state));
+  const unsigned int evflags = cap_state == cudaStreamCaptureStatusActive ? cudaEventRecordExternal
+                                                                          : cudaEventRecordDefault;
   if (c->opts.reserved[2] && c->tuned_Lb != Lb && !rows) {
     int rc = autotune_xpass(c, a, d_rots, nRot, wave, tc, s);
     if (rc) return rc;
@@ -448,24 +454,24 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     a.nrot = (int)std::min<long>(wave, nRot - r0);
     a.rots = order + r0;
     cudaEvent_t* ev = prof ? &c->kev[(size_t)waves * (kLaunchesPerWave + 1)] : nullptr;
-    if (prof) CDK_CUDA(cudaEventRecord(ev[0], s));
+    if (prof) CDK_CUDA(cudaEventRecordWithFlags(ev[0], s, evflags));
     CDK_CUDA(launch_prep(a, s));
-    if (prof) CDK_CUDA(cudaEventRecord(ev[1], s));
+    if (prof) CDK_CUDA(cudaEventRecordWithFlags(ev[1], s, evflags));
     CDK_CUDA(launch_spread_yz(a, s));
-    if (prof) CDK_CUDA(cudaEventRecord(ev[2], s));
+    if (prof) CDK_CUDA(cudaEventRecordWithFlags(ev[2], s, evflags));
     if (hankel) CDK_CUDA(launch_xpass_hankel(a, c->d_ptilde, osc.data(), hp, s));
     else if (streamed) CDK_CUDA(launch_xpass_stream(a, c->d_top, s));
     else if (umma) CDK_CUDA(launch_xpass_umma(a, c->d_ptilde, s));
     else if (tc) CDK_CUDA(launch_xpass_tc(a, c->d_ptilde, s));
     else CDK_CUDA(launch_xpass(a, s));
-    if (prof) CDK_CUDA(cudaEventRecord(ev[3], s));
+    if (prof) CDK_CUDA(cudaEventRecordWithFlags(ev[3], s, evflags));
     CDK_CUDA(launch_yz_inv_argmin(a, s));
     if (tiebreak) CDK_CUDA(launch_tiebreak(a, c->d_grids, f16form ? 1e-3f : 1e-4f, s));
     if (topk > 0)
       CDK_CUDA(launch_topk_rescore(a, c->d_grids, topk, static_cast<TopPose*>(c->topk.base) + (size_t)waves * topk, s));
-    if (prof) CDK_CUDA(cudaEventRecord(ev[4], s));
+    if (prof) CDK_CUDA(cudaEventRecordWithFlags(ev[4], s, evflags));
     CDK_CUDA(launch_finalize(a, s));
-    if (prof) CDK_CUDA(cudaEventRecord(ev[5], s));
+    if (prof) CDK_CUDA(cudaEventRecordWithFlags(ev[5], s, evflags));
     launches += kLaunchesPerWave + (rows ? 1 : 0) + (tiebreak ? 1 : 0) + (topk > 0 ? 1 : 0);  // + k_tile_plan
     ++waves;
   }
@@ -610,6 +616,7 @@ int check_errors_after(cdk_ctx* c, cudaStream_t s) {
   }
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, c->ev0, c->ev1) == cudaSuccess) c->stats[3] = ms;
+  (void)cudaGetLastError();
   CDK_CUDA(cudaMemcpy(c->h_work, c->d_work, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   c->stats[6] = (double)c->h_work[0];
   c->stats[7] = (double)c->h_work[1];
@@ -625,6 +632,9 @@ int check_errors_after(cdk_ctx* c, cudaStream_t s) {
       if (cudaEventElapsedTime(&t, ev[k], ev[k + 1]) == cudaSuccess) c->stats[8 + k] += t;
     }
   }
+  // a timing query that failed (an event never recorded) must not surface as the error of a
+  // later call
+  (void)cudaGetLastError();
   if (c->h_misc[2] != 0) {
     set_error(std::to_string(c->h_misc[2]) +
               " rotation(s) overflowed the planned ligand box; results for them are invalid");

@@ -193,8 +193,9 @@ __host__ __device__ inline HxLayout hx_layout(int n, int K, int cols, bool f16, 
   L.S = (uint32_t)G * HX_CORE;
   L.op = (uint32_t)cols * K * 2 * 3 * L.S;
   L.stage = (uint32_t)cols * (f16 ? 1 : 2) * HX_TILE;
-  // P~ of the CTA's columns (float2) + their four split arrays (re hi, re lo, im hi, im lo)
-  L.build = (uint32_t)cols * K * n * 8 + (uint32_t)cols * K * 4 * n * 2;
+  // P~ of the CTA's columns (float2) + their four split arrays (re hi, re lo, im hi, im lo),
+  // each n + 32 halves long (the first 32 repeated after the end: no wrap in the group build)
+  L.build = (uint32_t)cols * K * n * 8 + (uint32_t)cols * K * 4 * (n + 32) * 2;
   return L;
 }
 
@@ -243,48 +244,56 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
 
-  // ---- operator build: P~ of the CTA's columns -> split arrays -> Hankel rows
+  // ---- operator build: P~ of the CTA's columns -> split arrays -> Hankel groups
   {
-    float2* s_pt = reinterpret_cast<float2*>(ring);                           // [cols][K][N]
-    uint16_t* s_sp = reinterpret_cast<uint16_t*>(ring + (size_t)COLS * K * N * 8);  // [cols][K][4][N]
+    constexpr int NP = N + 32;  // split arrays repeat their first 32 halves after the end
+    float2* s_pt = reinterpret_cast<float2*>(ring);                               // [cols][K][N]
+    uint16_t* s_sp = reinterpret_cast<uint16_t*>(ring + (size_t)COLS * K * N * 8);  // [cols][K][4][NP]
     for (int i = tid; i < COLS * K * N; i += HX_THREADS) {
       const int cc = i / (K * N), rem = i - cc * K * N;
       s_pt[i] = pt[((size_t)(c0 + cc) * K) * N + rem];
     }
     __syncthreads();
-    for (int i = tid; i < COLS * K * N; i += HX_THREADS) {
-      const int k = (i / N) % K;
+    for (int i = tid; i < COLS * K * NP; i += HX_THREADS) {
+      const int ck = i / NP, m = i - ck * NP;
+      const int k = ck % K;
       const float scale = F16 ? sc.s[k] : 1.f;
-      const float2 v = s_pt[i];
+      const float2 v = s_pt[ck * N + (m < N ? m : m - N)];
       uint16_t h, l;
-      uint16_t* dst = s_sp + (size_t)(i / N) * 4 * N + (i % N);
+      uint16_t* dst = s_sp + (size_t)ck * 4 * NP + m;
       split16<F16>(F16 ? __fmul_rn(v.x, scale) : v.x, h, l);
       dst[0] = h;
-      dst[N] = l;
+      dst[NP] = l;
       split16<F16>(F16 ? __fmul_rn(v.y, scale) : v.y, h, l);
-      dst[2 * N] = h;
-      dst[3 * N] = l;
+      dst[2 * NP] = h;
+      dst[3 * NP] = l;
     }
     __syncthreads();
-    // rows: [cc][k][hl][buf (Re, Im, -Re)][g][r] x 16 B, H[g][r][d] = P~((8g + r + d) mod N);
-    // -Re is the negated Re split (negation is exact)
-    const int rows = COLS * K * 2 * 3 * G * 8;
-    for (int i = tid; i < rows; i += HX_THREADS) {
-      const int r = i & 7;
-      const int g = (i >> 3) % G;
-      const int t = (i >> 3) / G;  // ((cc * K + k) * 2 + hl) * 3 + buf
+    // one 128-byte group per item: [cc][k][hl][buf (Re, Im, -Re)][g] x 8 rows, row r holds
+    // P~(8g + r + d), d < 8 -- halves r .. r + 7 of the 16 at 8g: two aligned 16-byte loads,
+    // then per row four words picked (r even) or funnel-shifted by one half (r odd); -Re is the
+    // negated Re split (sign bits flipped: negation is exact)
+    const int groups = COLS * K * 2 * 3 * G;
+    for (int i = tid; i < groups; i += HX_THREADS) {
+      const int g = i % G;
+      const int t = i / G;  // ((cc * K + k) * 2 + hl) * 3 + buf
       const int buf = t % 3, hl = (t / 3) & 1, ck = t / 6;
-      const uint16_t* src = s_sp + (size_t)ck * 4 * N + (size_t)((buf == 1 ? 2 : 0) + hl) * N;
-      const uint16_t neg = buf == 2 ? 0x8000u : 0u;
-      uint32_t w[4];
+      const uint16_t* src = s_sp + (size_t)ck * 4 * NP + (size_t)((buf == 1 ? 2 : 0) + hl) * NP + 8 * g;
+      const uint4 c0v = *reinterpret_cast<const uint4*>(src);
+      const uint4 c1v = *reinterpret_cast<const uint4*>(src + 8);
+      const uint32_t W[8] = {c0v.x, c0v.y, c0v.z, c0v.w, c1v.x, c1v.y, c1v.z, c1v.w};
+      const uint32_t neg = buf == 2 ? 0x80008000u : 0u;
+      uint4* dst = reinterpret_cast<uint4*>(op) + (size_t)i * 8;
 #pragma unroll
-      for (int d = 0; d < 8; d += 2) {
-        const uint32_t e0 = src[(8 * g + r + d) % N] ^ neg, e1 = src[(8 * g + r + d + 1) % N] ^ neg;
-        w[d / 2] = e0 | (e1 << 16);
+      for (int r = 0; r < 8; ++r) {
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          w[q] = ((r & 1) ? __funnelshift_r(W[r / 2 + q], W[r / 2 + q + 1], 16) : W[r / 2 + q]) ^ neg;
+        dst[r] = make_uint4(w[0], w[1], w[2], w[3]);
       }
-      *reinterpret_cast<uint4*>(op + (size_t)i * 16) = make_uint4(w[0], w[1], w[2], w[3]);
     }
-    // the rows are read by the tensor cores (async proxy)
+    // the groups are read by the tensor cores (async proxy)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

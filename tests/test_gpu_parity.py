@@ -198,9 +198,14 @@ def test_graph_replay_tensor_core_form(grids_cache):
     w = synth.make_workload("c1_64", seed=12, n_conf=2, n_q=150, grids_cache=grids_cache)
     with Receptor(w.grids, w.spacing, form=2) as plain:
         ref = _device_search(plain, w, torch, 1)[0]
-    with Receptor(w.grids, w.spacing, form=2, use_graphs=1, wave_rotations=128) as rec:
+    with Receptor(w.grids, w.spacing, form=2, use_graphs=1, wave_rotations=128,
+                  profile=True) as rec:
         outs = _device_search(rec, w, torch, 4)
-        assert rec.stats()["graph_state"] == 2
+        st = rec.stats()
+        assert st["graph_state"] == 2
+        # the per-kernel events are recorded inside the graph too
+        assert st["kernel_ms"]["xpass"] > 0 and st["kernel_ms"]["yz_inv_argmin"] > 0
+        outs += _device_search(rec, w, torch, 1)  # and leave no error behind
     for e, i, _, _ in outs:
         np.testing.assert_array_equal(e, ref[0])
         np.testing.assert_array_equal(i, ref[1])

@@ -223,4 +223,6 @@ def test_top_poses_rescored_per_wave(grids_cache):
         r = int(rot[j])
         emap = O.energy_map(w.grids, w.spacing, w.coor[0], w.charge, w.eps, w.slot, qq[r])
         ref = emap[tuple(tidx[j])]
-        assert abs(e64[j] - ref) <= 1e-9 * max(1.0, abs(ref))
+        # the oracle's map sums FillLigandGrid's float-rounded cells; the re-score sums the
+        # exact trilinear weights in double: they agree to the float grid's rounding
+        assert abs(e64[j] - ref) <= 1e-7 * max(1.0, abs(ref))
