@@ -828,12 +828,19 @@ def config4_run(args):
 
 def profile_run(args):
     """One warm-up and one timed search of `--profile-run` rotations (first conformers of the
-    config-1 workload), per-kernel device times from events around every launch."""
+    config-1 workload, or of the config-4 workload with --profile-config c4_128), per-kernel
+    device times from events around every launch."""
     import torch
-    from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP16X2, CDK_FORM_FP32, Receptor
-    w = make_rank_workload(0, 1)
-    n_q = N_Q
-    n_conf = max(1, min(N_CONF, (args.profile_run + n_q - 1) // n_q))
+    from cdocker_b200 import CDK_FORM_BF16X3, CDK_FORM_FP16X2, CDK_FORM_FP32, Receptor, synth
+    if args.profile_config == "c4_128":
+        w = synth.make_workload("c4_128", seed=0, n_conf=max(1, (args.profile_run + 1999) // 2000),
+                                n_q=min(2000, args.profile_run))
+        n_q = w.quats.shape[1]
+        n_conf = w.quats.shape[0]
+    else:
+        w = make_rank_workload(0, 1)
+        n_q = N_Q
+        n_conf = max(1, min(N_CONF, (args.profile_run + n_q - 1) // n_q))
     if args.profile_run < n_q:
         n_q = args.profile_run
     dev = torch.device("cuda", 0)
@@ -881,6 +888,7 @@ def main():
     ap.add_argument("--serve-sweep", action="store_true",
                     help="config 3: 96^3 receptor, Poisson request streams at 5 rates; one JSON "
                          "line per rate (not the bench line)")
+    ap.add_argument("--profile-config", default="c1_64", choices=["c1_64", "c4_128"])
     ap.add_argument("--config4", action="store_true",
                     help="config 4: 128^3, 1e6 rotations, all forms, error vs FP64 on every "
                          "rotation; one JSON line (not the bench line)")

@@ -309,7 +309,8 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
     const uint32_t row_s = (uint32_t)(rr >> 3) * HX_CORE + (uint32_t)(rr & 7) * 16;
     constexpr size_t RS = (size_t)(NCOL / 4) * 32;  // one ligand row (16 B units)
     constexpr int ROWS = 8 * LPARTS;                // rows per (rotation, channel)
-    int s = 0;
+    int s = 0, b = 0;      // stages issued, ring slot of stage s
+    uint32_t round = 0;    // s / nb (the ring pass), kept as a counter: no division per stage
     for (int t = 0; t < ntiles; ++t) {
       const int r0 = t * HX_R;
       const int nr = min(HX_R, a.nrot - r0);
@@ -345,8 +346,7 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
         const int jl = (int)(jr & 15), jh = (int)(jr >> 4);
         const uint4* src0 = reinterpret_cast<const uint4*>(a.lop) + rot_rows + (size_t)k * ROWS * RS;
         for (int j = jlo; j <= jhi; ++j, ++s) {
-          const int b = s % nb;
-          if (s >= nb && !mbar_wait(smem_u32(&s_empty[b]), (uint32_t)((s / nb) - 1) & 1u, &s_fail)) {
+          if (s >= nb && !mbar_wait(smem_u32(&s_empty[b]), (round - 1) & 1u, &s_fail)) {
             s_fail = 1;
             ok = false;
             break;
@@ -365,6 +365,10 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
                              : "memory");
               }
           asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&s_full[b])) : "memory");
+          if (++b == nb) {
+            b = 0;
+            ++round;
+          }
         }
       }
       if (!ok) break;
@@ -372,7 +376,8 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
     asm volatile("cp.async.wait_all;" ::: "memory");
   } else if (warp == HX_MMA_WARP) {
     // ---- MMA issuer: the whole warp runs the loop (uniform descriptors), one lane issues
-    int s = 0, u = 0;
+    int s = 0, u = 0, b = 0;
+    uint32_t round = 0;
     bool good = true;
     for (int t = 0; t < ntiles && good; ++t) {
       const TilePlan p = load_plan(a.rec + t * HX_R);
@@ -392,8 +397,7 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
         const int k = (int)((p.pk >> (4 * ai)) & 15);
         const int jlo = (int)((p.pl >> (4 * ai)) & 15), jhi = (int)((p.ph >> (4 * ai)) & 15);
         for (int j = jlo; j <= jhi; ++j, ++s) {
-          const int b = s % nb;
-          if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_full[b]), (uint32_t)(s / nb) & 1u, &s_fail))) {
+          if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_full[b]), round & 1u, &s_fail))) {
             if (lane == 0) s_fail = 1;
             good = false;
             break;
@@ -425,6 +429,10 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
           if (elect_one()) umma_commit(smem_u32(&s_empty[b]));
           __syncwarp();
           first = false;
+          if (++b == nb) {
+            b = 0;
+            ++round;
+          }
         }
       }
       if (!good) break;
@@ -438,14 +446,20 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
       ++u;
     }
     // the newest commit completes after every earlier MMA of this warp
-    if (lane == 0 && s > 0 && !mbar_wait(smem_u32(&s_empty[(s - 1) % nb]), (uint32_t)((s - 1) / nb) & 1u, nullptr))
-      s_fail = 1;
+    if (lane == 0 && s > 0) {
+      // the slot and ring pass of stage s - 1 (one step back from the counters)
+      const int bl = b == 0 ? nb - 1 : b - 1;
+      const uint32_t rl = b == 0 ? round - 1 : round;
+      if (!mbar_wait(smem_u32(&s_empty[bl]), rl & 1u, nullptr)) s_fail = 1;
+    }
     __syncwarp();
   } else {
     // ---- epilogue: TMEM lane quarter q = rotations 32 q .. 32 q + 31
     const int q = warp & 3;
     const int rl = 32 * q + lane;
+    // plane groups of the B layout: 1, 2, 4 or 8 (a power of two: masks, no division)
     const int G2 = a.bgroup > 1 ? a.bgroup : 1;
+    const int gm = G2 - 1;
     int u = 0;
     for (int t = 0; t < ntiles; ++t) {
       const int r0 = t * HX_R;
@@ -477,7 +491,7 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
           if (xp < Wr) {
             // plane-group layout of B: float4 (re, im of column pair 2m, 2m + 1) at
             // (xp - xp % G) NCOL / 2 + m G + xp % G
-            const size_t f4 = (size_t)(xp - xp % G2) * (NCOL / 2) + (size_t)(c0 >> 1) * G2 + xp % G2;
+            const size_t f4 = (size_t)(xp & ~gm) * (NCOL / 2) + (size_t)(c0 >> 1) * G2 + (xp & gm);
             if constexpr (COLS == 2) {
               rowp[f4] = make_float4(re[0][i], im[0][i], re[1][i], im[1][i]);
             } else {

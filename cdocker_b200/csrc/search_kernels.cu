@@ -915,14 +915,19 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
 // only). Block-wide barriers: after the twiddle load, between the y and z passes (the y output
 // is the z input), and in the final reduction. Same radix stages, twiddles and packing as
 // k_yz_inv_argmin.
+// 288 threads = 36 octets: the 33 kz columns (and at most 32 row pairs) of a 64^3 plane in one
+// round each, 49 / 65 columns at 96^3 / 128^3 in two
+constexpr int kOctWarps = 9;
+constexpr int kOctets = 4 * kOctWarps;
+
 template <int N>
 constexpr size_t octet_smem() {
   // twiddles, Y[N][N/2+1], per warp 4 octets x 8 blocks x (R1 + 1)
-  return sizeof(float2) * (N + (size_t)N * (N / 2 + 1) + 8 * 4 * 8 * (N / 8 + 1));
+  return sizeof(float2) * (N + (size_t)N * (N / 2 + 1) + kOctWarps * 4 * 8 * (N / 8 + 1));
 }
 
 template <int N, bool TOP2>
-__global__ void __launch_bounds__(256, (N <= 64 ? 4 : 2)) k_yz_octet(WaveArgs a) {
+__global__ void __launch_bounds__(32 * kOctWarps, (N <= 64 ? 4 : 2)) k_yz_octet(WaveArgs a) {
   constexpr int NZH = N / 2 + 1, NCOL = N * NZH;
   constexpr int R1 = N / 8;           // stage-1 radix; stage 2 is radix 8
   constexpr int XS = R1 + 1;          // padded block stride of the exchange slice
@@ -932,7 +937,7 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 4 : 2)) k_yz_octet(WaveArgs a)
   float2* s_tw = reinterpret_cast<float2*>(smem_raw);
   float2* s_y = s_tw + N;                    // y-transformed rows Y[y][kz]
   float2* s_xall = s_y + (size_t)N * NZH;    // exchange slices
-  __shared__ unsigned long long s_best[8], s_best2[8];
+  __shared__ unsigned long long s_best[kOctWarps], s_best2[kOctWarps];
   const int x = blockIdx.x, r = blockIdx.y;
   const RotRec* rec = a.rec + r;
   if (!rec->valid) return;
@@ -940,7 +945,7 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 4 : 2)) k_yz_octet(WaveArgs a)
   if (x >= Wx) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int o = lane >> 3, t = lane & 7, g = warp * 4 + o;
-  for (int i = tid; i < N; i += 256) s_tw[i] = a.tw[i];
+  for (int i = tid; i < N; i += 32 * kOctWarps) s_tw[i] = a.tw[i];
   const int G = a.bgroup > 1 ? a.bgroup : 1;
   const float2* src2 = reinterpret_cast<const float2*>(
       reinterpret_cast<const float4*>(a.B + ((size_t)r * N + (x - x % G)) * NCOL) + x % G);
@@ -964,12 +969,12 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 4 : 2)) k_yz_octet(WaveArgs a)
       }
     }
   };
-  // y: columns l = g, g + 32, ...; every warp runs the same number of rounds (warp-uniform)
-  constexpr int YR = (NZH + 31) / 32;
+  // y: columns l = g, g + 36, ...; a warp stops when none of its octets has a column left
+  constexpr int YR = (NZH + kOctets - 1) / kOctets;
 #pragma unroll 1
   for (int it = 0; it < YR; ++it) {
-    if (warp * 4 + 32 * it >= NZH) break;  // no octet of this warp has a column left
-    const int l = g + 32 * it;
+    if (warp * 4 + kOctets * it >= NZH) break;
+    const int l = g + kOctets * it;
     const bool act = l < NZH;
     float2 v[R1];
 #pragma unroll
@@ -991,11 +996,11 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 4 : 2)) k_yz_octet(WaveArgs a)
   const int npairs = (Wy + 1) / 2;
   const float inv = 1.0f / (float)((double)N * N * N);
   unsigned long long best = ~0ull, best2 = ~0ull;
-  constexpr int ZR = (N / 2 + 31) / 32;
+  constexpr int ZR = (N / 2 + kOctets - 1) / kOctets;
 #pragma unroll 1
   for (int it = 0; it < ZR; ++it) {
-    if (warp * 4 + 32 * it >= npairs) break;  // warp-uniform
-    const int p = g + 32 * it;
+    if (warp * 4 + kOctets * it >= npairs) break;  // warp-uniform
+    const int p = g + kOctets * it;
     const bool act = p < npairs;
     const float2* A = s_y + (2 * min(p, N / 2 - 1)) * NZH;
     const float2* Bv = A + NZH;
@@ -1052,7 +1057,7 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 4 : 2)) k_yz_octet(WaveArgs a)
   }
   __syncthreads();
   if (tid == 0) {
-    for (int w = 1; w < 8; ++w) {
+    for (int w = 1; w < kOctWarps; ++w) {
       if constexpr (TOP2) top2_merge(s_best[w], s_best2[w], best, best2);
       else best = s_best[w] < best ? s_best[w] : best;
     }
@@ -1357,7 +1362,7 @@ cudaError_t launch_yz_inv_t(const WaveArgs& a, cudaStream_t s) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     dim3 grid(N, a.nrot);
-    kern<<<grid, 256, sm, s>>>(a);
+    kern<<<grid, 32 * kOctWarps, sm, s>>>(a);
     return cudaGetLastError();
   }
   // twiddles + one plane (n <= 64: the packed rows alias it) [+ the packed rows]
