@@ -135,8 +135,9 @@ class Receptor:
                  use_graphs: int = 0, profile: bool = False, fft_planes: bool = False,
                  autotune: bool = False, tc_mma_sync: bool = False, tc_build: bool = False,
                  group_rotations: bool = True, tc_stream_tiles: bool = False,
+                 tc_hankel: bool = False,
                  tc_cols: int = 0, top_k: int = 0, tie_break: bool = True,
-                 yz_block_stages: bool = False):
+                 yz_block_stages: bool = False, yz_octets: bool = False):
         g = _f32(grids)
         if g.ndim != 4:
             raise ValueError("grids must be [K, n, n, n]")
@@ -152,9 +153,11 @@ class Receptor:
         opts.col_tile = col_tile
         opts.use_graphs = use_graphs
         opts.reserved[0] = 1 if profile else 0
-        opts.reserved[1] = (1 if fft_planes else 0) | (2 if yz_block_stages else 0)
+        opts.reserved[1] = ((1 if fft_planes else 0) | (2 if yz_block_stages else 0) |
+                            (4 if yz_octets else 0))
         opts.reserved[2] = 1 if autotune else 0
-        opts.reserved[3] = 1 if tc_mma_sync else (2 if tc_build else (3 if tc_stream_tiles else 0))
+        opts.reserved[3] = (1 if tc_mma_sync else 2 if tc_build else 3 if tc_stream_tiles
+                            else 4 if tc_hankel else 0)
         opts.reserved[5] = tc_cols
         opts.reserved[6] = top_k
         opts.reserved[7] = 0 if tie_break else 1

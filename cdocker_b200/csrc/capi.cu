@@ -290,11 +290,15 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   probe.kyof = (c->opts.reserved[1] & 1) ? nullptr : c->d_kyof;
   probe.max_atoms = maxAtoms;
   probe.atom_cap = maxAtoms;
+  // automatic choice (reserved[3] = 0): at 64^3 the streamed-tile kernel where it applies (box
+  // <= 32 planes; measured 1.4x faster there than the Hankel kernel), the Hankel kernel at the
+  // other sizes; 3 forces streamed tiles, 4 the Hankel kernel
   const int variant = c->opts.reserved[3];
+  const bool can_stream = tc && stream_supported(n, Lb) && direct_planes(probe);
+  const bool streamed = can_stream && (variant == 3 || variant == 0);
   HankelPlan hp{};
-  const bool hankel = tc && (variant == 0) && direct_planes(probe) &&
+  const bool hankel = tc && !streamed && (variant == 0 || variant == 4) && direct_planes(probe) &&
                       hankel_plan(n, K, Lb, f16form, c->opts.reserved[5], &hp);
-  const bool streamed = tc && (variant == 3) && stream_supported(n, Lb) && direct_planes(probe);
   if (streamed && !c->d_top) {
     const size_t tb = stream_top_bytes(n, K);
     if (cudaMalloc(&c->d_top, tb) != cudaSuccess) {
@@ -379,7 +383,8 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   a.bgroup = rows ? stream_bgroup() : 1;
   a.col_tile = c->opts.col_tile > 0 ? c->opts.col_tile : pick_col_tile(n, K);
   a.kyof = (c->opts.reserved[1] & 1) ? nullptr : c->d_kyof;  // reserved[1] bit 0: FFT planes
-  a.yz_block_stages = (c->opts.reserved[1] & 2) ? 1 : 0;       // bit 1: block-stage yz kernel
+  // bit 1: block-stage yz kernel at every n; bit 2: octet yz kernel at every n
+  a.yz_block_stages = (c->opts.reserved[1] & 2) ? 1 : (c->opts.reserved[1] & 4) ? 2 : 0;
   a.chunk = 0;
   if (c->tuned_Lb == Lb) {
     if (c->tuned_col_tile) a.col_tile = c->tuned_col_tile;

@@ -74,7 +74,8 @@ struct WaveArgs {
   float2* B;                 // [nrot][n][ncol], or with bgroup G > 1 [nrot][n/G][ncol/2][G][2]:
                              // the x planes grouped by G, 16 B (two columns) per (plane, pair)
   int bgroup;                // 0 or 1: plain B layout; 2, 4, 8: grouped (streamed x pass only)
-  int yz_block_stages;       // n = 64: 1 runs the block-stage yz kernel instead of the octet one
+  int yz_block_stages;       // inverse (y,z) kernel: 0 by grid size (block stages at n <= 64,
+                             // octets at n >= 96), 1 block stages, 2 octets
   unsigned long long* keys;  // [nrot]
   unsigned long long* keys2; // precision forms' near-tie break: [nrot][n][2] the two smallest
                              // keys of every window plane (null: not kept)

@@ -1356,7 +1356,11 @@ cudaError_t launch_spread_yz_t(const WaveArgs& a, cudaStream_t s) {
 
 template <int N>
 cudaError_t launch_yz_inv_t(const WaveArgs& a, cudaStream_t s) {
-  if (!a.yz_block_stages) {
+  // octet kernel at n >= 96 (measured 1.9x faster at 128^3); block stages at n <= 64 (the
+  // packed rows alias the plane there, 8 CTAs per SM: 1.6x faster than the octets at 64^3);
+  // yz_block_stages: 1 forces block stages, 2 forces octets
+  const bool octet = a.yz_block_stages == 2 || (a.yz_block_stages == 0 && N >= 96);
+  if (octet) {
     constexpr size_t sm = octet_smem<N>();
     auto kern = a.keys2 ? k_yz_octet<N, true> : k_yz_octet<N, false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

@@ -397,15 +397,21 @@ void worker_loop(cdk_server* s) {
     a.Lb = lb;
     a.atom_cap = cap;
     a.rots = w.d_rots;
+    // the same x-pass choice as a plain search on the context (results alone and in the mix
+    // stay identical): streamed tiles at 64^3 where they apply, the Hankel kernel elsewhere
     HankelPlan hp{};
-    const bool tc_wave = s->streamed && direct_planes(a) && hankel_plan(n, K, lb, f16, 0, &hp);
+    const bool tile_wave = s->streamed && s->v.top != nullptr && stream_supported(n, lb) && direct_planes(a);
+    const bool tc_wave = tile_wave || (s->streamed && s->v.tc_variant != 3 && direct_planes(a) &&
+                                       hankel_plan(n, K, lb, f16, 0, &hp));
     a.lop = tc_wave ? lop_base : nullptr;
     a.f16 = (tc_wave && f16) ? 1 : 0;
     a.bgroup = tc_wave ? stream_bgroup() : 1;
     if (le == cudaSuccess) {
       note(launch_prep(a, s->stream));
       note(launch_spread_yz(a, s->stream));
-      note(tc_wave ? launch_xpass_hankel(a, s->v.ptilde, s->osc, hp, s->stream) : launch_xpass(a, s->stream));
+      note(tile_wave ? launch_xpass_stream(a, s->v.top, s->stream)
+                     : tc_wave ? launch_xpass_hankel(a, s->v.ptilde, s->osc, hp, s->stream)
+                               : launch_xpass(a, s->stream));
       note(launch_yz_inv_argmin(a, s->stream));
       if (a.keys2)
         note(launch_tiebreak(a, s->v.grids, s->v.form == CDK_FORM_FP16X2 ? 1e-3f : 1e-4f, s->stream));
@@ -478,10 +484,20 @@ int cdk_server_create(cdk_ctx* ctx, const cdk_server_opts* opts, cdk_server** ou
   // ligand rows) on waves it applies to (ligand box <= 32 planes, ligands <= 96 atoms on the
   // direct plane path); other waves and FP32 contexts run the FP32 radix x pass
   HankelPlan probe{};
-  s->streamed = ((s->v.form == CDK_FORM_BF16X3 && s->v.tc_variant == 0) ||
-                 s->v.form == CDK_FORM_FP16X2) &&
+  const bool tcv = s->v.tc_variant == 0 || s->v.tc_variant == 3 || s->v.tc_variant == 4;
+  s->streamed = ((s->v.form == CDK_FORM_BF16X3 && tcv) || s->v.form == CDK_FORM_FP16X2) &&
                 s->v.kyof != nullptr && s->v.ptilde != nullptr &&
-                hankel_plan(n, K, std::min(s->opts.max_box, 32), s->v.form == CDK_FORM_FP16X2, 0, &probe);
+                (stream_supported(n, std::min(s->opts.max_box, 32)) ||
+                 hankel_plan(n, K, std::min(s->opts.max_box, 32), s->v.form == CDK_FORM_FP16X2, 0, &probe));
+  if (s->streamed && s->v.tc_variant != 4 && stream_top_bytes(n, K) > 0) {
+    // 64^3: the streamed-tile kernel's operator image, built once per context
+    const int rc = ctx_ensure_top(ctx);
+    if (rc != CDK_OK) {
+      delete s;
+      return rc;
+    }
+    ctx_view(ctx, &s->v);
+  }
   for (int k = 0; k < KMAX; ++k) s->osc[k] = s->v.lscale[k] != 0.f ? 1.f / s->v.lscale[k] : 1.f;
   const size_t planes = (size_t)W * K * s->opts.max_box * ncol * sizeof(float2);
   const size_t rows = s->streamed ? (size_t)((W + 7) & ~7) *

@@ -55,14 +55,16 @@ typedef struct cdk_opts {
   int use_graphs;      /* 1 = replay each wave through a captured CUDA graph */
   int reserved[8];     /* [0] = 1: time every kernel with events (cdk_ctx_stats [8..12]);
                           [1] bit 0: spread planes through the radix FFT instead of the direct
-                          separable evaluation; bit 1: at n = 64, the inverse (y,z) kernel with
-                          block-wide radix stages instead of warp-local line transforms; [2] = 1: autotune the x pass on the first wave
-                          of each new ligand box; [3] precision-form x pass: 0 = tcgen05 with
-                          the Hankel operator resident in shared memory and streamed ligand
-                          rows where it applies (ligand box <= 32 planes, ligands <= 96 atoms,
-                          operator fits shared memory), else the next one; 1 = mma.sync;
+                          separable evaluation; bit 1: the inverse (y,z) kernel with
+                          block-wide radix stages at every n; bit 2: the one with warp-local
+                          line transforms at every n (default: block stages at n <= 64,
+                          warp-local lines at n >= 96); [2] = 1: autotune the x pass on the first wave
+                          of each new ligand box; [3] precision-form x pass: 0 = automatic
+                          (ligands <= 96 atoms, box <= 32 planes: tcgen05 with streamed operator
+                          tiles at n = 64, tcgen05 with the Hankel operator resident in shared
+                          memory at the other sizes; else the next one); 1 = mma.sync;
                           2 = tcgen05 with operands built inside the kernel (n = 64);
-                          3 = tcgen05 with streamed operator tiles (n = 64);
+                          3 = streamed operator tiles (n = 64); 4 = the Hankel kernel;
                           [4] = 1: keep the rotations in the given order in the streamed
                           tensor-core x pass (by default they are grouped by the ligand-box
                           chunks their channels reach, which changes no result);

@@ -183,7 +183,8 @@ def test_yz_octet_kernel_matches_block_stages(grids_cache, form, name, nq):
     w = synth.make_workload(name, seed=3, n_conf=2, n_q=nq, grids_cache=grids_cache)
     out = []
     for block in (False, True):
-        with Receptor(w.grids, w.spacing, form=form, yz_block_stages=block) as rec:
+        with Receptor(w.grids, w.spacing, form=form, yz_block_stages=block,
+                      yz_octets=not block) as rec:
             out.append(rec.search(w.coor, w.charge, w.eps, w.slot, w.quats))
     (e0, i0), (e1, i1) = out
     assert np.abs(e0.astype(np.float64) - e1).max() <= 1e-6 * np.abs(e1).max()
@@ -216,9 +217,9 @@ def test_autotune_tensor_core_same_results(grids_cache, form):
     """The autotuner times the Hankel x pass under one and two columns per CTA and several ring
     depths on the first wave and keeps the fastest; every candidate computes the same numbers."""
     w = synth.make_workload("c1_64", seed=13, n_conf=2, n_q=200, grids_cache=grids_cache)
-    with Receptor(w.grids, w.spacing, form=form) as plain:
+    with Receptor(w.grids, w.spacing, form=form, tc_hankel=True) as plain:
         e0, i0 = plain.search(w.coor, w.charge, w.eps, w.slot, w.quats)
-    with Receptor(w.grids, w.spacing, form=form, autotune=True) as rec:
+    with Receptor(w.grids, w.spacing, form=form, autotune=True, tc_hankel=True) as rec:
         e1, i1 = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
         st = rec.stats()
         e2, i2 = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)

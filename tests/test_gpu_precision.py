@@ -16,6 +16,13 @@ TOL_TC = 1e-3
 
 
 HANKEL = {CDK_FORM_BF16X3: "tcgen05_hankel", CDK_FORM_FP16X2: "tcgen05_hankel_fp16"}
+TILES = {CDK_FORM_BF16X3: "tcgen05_streamed", CDK_FORM_FP16X2: "tcgen05_streamed_fp16"}
+
+
+def auto_kind(n, form):
+    """The automatic tensor-core x pass: streamed operator tiles at 64^3, the Hankel kernel at
+    the other grid sizes."""
+    return TILES[form] if n == 64 else HANKEL[form]
 
 
 @pytest.mark.parametrize("form", [CDK_FORM_BF16X3, CDK_FORM_FP16X2])
@@ -23,11 +30,16 @@ HANKEL = {CDK_FORM_BF16X3: "tcgen05_hankel", CDK_FORM_FP16X2: "tcgen05_hankel_fp
                                            ("c4_128", 2, 32)])
 def test_tc_form_vs_fp64(name, nconf, nq, form, grids_cache):
     """Both tensor-core forms against FP64 at every grid size, every rotation checked (64 at
-    96^3 and at 128^3); both run the tcgen05 x pass with the resident Hankel operator."""
+    96^3 and at 128^3), with the automatic x pass and, at 64^3, the Hankel kernel as well."""
     w = synth.make_workload(name, seed=5, n_conf=nconf, n_q=nq, grids_cache=grids_cache)
-    with Receptor(w.grids, w.spacing, form=form) as rec:
-        minE, idx = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
-        assert rec.stats()["xpass_kind"] == HANKEL[form]
+    for hankel in ((False, True) if w.n == 64 else (False,)):
+        with Receptor(w.grids, w.spacing, form=form, tc_hankel=hankel) as rec:
+            minE, idx = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+            assert rec.stats()["xpass_kind"] == (HANKEL[form] if hankel else auto_kind(w.n, form))
+        _check_fp64(w, nq, minE, idx)
+
+
+def _check_fp64(w, nq, minE, idx):
     _, ridx, r64 = O.search_direct(w.grids, w.spacing, w.coor, w.charge, w.eps, w.slot, w.quats,
                                    prec=1)
     qq = w.quats.reshape(-1, 4)
@@ -73,8 +85,9 @@ def test_tensor_core_variants_agree(grids_cache, wave):
     kinds = {"hankel": "tcgen05_hankel", "hankel_1col": "tcgen05_hankel",
              "hankel_2col": "tcgen05_hankel", "stream_tiles": "tcgen05_streamed",
              "build": "tcgen05_build", "mma_sync": "mma_sync"}
-    for name, kw in [("hankel", {}), ("hankel_1col", {"tc_cols": 1}), ("hankel_2col", {"tc_cols": 2}),
-                     ("stream_tiles", {"tc_stream_tiles": True}), ("build", {"tc_build": True}),
+    for name, kw in [("hankel", {"tc_hankel": True}), ("hankel_1col", {"tc_hankel": True, "tc_cols": 1}),
+                     ("hankel_2col", {"tc_hankel": True, "tc_cols": 2}),
+                     ("stream_tiles", {}), ("build", {"tc_build": True}),
                      ("mma_sync", {"tc_mma_sync": True})]:
         with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3, wave_rotations=wave, **kw) as r:
             out[name] = r.search(w.coor, w.charge, w.eps, w.slot, w.quats)
@@ -112,6 +125,7 @@ def test_streamed_falls_back_for_large_ligands(grids_cache):
 
 
 @pytest.mark.parametrize("form", [CDK_FORM_BF16X3, CDK_FORM_FP16X2])
+@pytest.mark.parametrize("hankel", [False, True])
 @pytest.mark.parametrize("name,n_atoms,radius,n_q,wave",
                          [("c1_64", 6, 1.2, 40, 0),     # box 7 planes: one K-step
                           ("c1_64", 60, 6.8, 12, 0),    # box 30 planes: four K-steps
@@ -119,14 +133,16 @@ def test_streamed_falls_back_for_large_ligands(grids_cache):
                           ("c4_128", 6, 1.2, 20, 0),    # 128^3: one K-step, windows near n
                           ("c4_128", 60, 6.8, 12, 5),   # 128^3: four K-steps, 5-rotation waves
                           ("c3_96", 30, 4.4, 21, 0)])   # 96^3
-def test_streamed_shapes_vs_fp64(grids_cache, name, n_atoms, radius, n_q, wave, form):
-    """The tensor-core x pass of both forms across ligand boxes (1 to 4 K-steps), grid sizes and
-    ragged waves, against the FP64 oracle."""
+def test_streamed_shapes_vs_fp64(grids_cache, name, n_atoms, radius, n_q, wave, form, hankel):
+    """The tensor-core x passes of both forms across ligand boxes (1 to 4 K-steps), grid sizes
+    and ragged waves, against the FP64 oracle (the automatic choice, and the Hankel kernel)."""
     w = synth.make_workload(name, seed=31, n_conf=1, n_q=n_q, grids_cache=grids_cache,
                             n_atoms=n_atoms, ligand_radius=radius)
-    with Receptor(w.grids, w.spacing, form=form, wave_rotations=wave) as rec:
+    if hankel and w.n != 64:
+        pytest.skip("the automatic choice is the Hankel kernel at this size")
+    with Receptor(w.grids, w.spacing, form=form, wave_rotations=wave, tc_hankel=hankel) as rec:
         minE, idx = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
-        assert rec.stats()["xpass_kind"] == HANKEL[form]
+        assert rec.stats()["xpass_kind"] == (HANKEL[form] if hankel else auto_kind(w.n, form))
     _, ridx, r64 = O.search_direct(w.grids, w.spacing, w.coor, w.charge, w.eps, w.slot, w.quats,
                                    prec=1)
     qq = w.quats.reshape(-1, 4)
