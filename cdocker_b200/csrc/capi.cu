@@ -144,6 +144,9 @@ struct cdk_ctx {
   int tuned_Lb = -1, tuned_col_tile = 0, tuned_chunk = 0;
   // autotuned tensor-core x pass (Hankel operator), per (Lb, form): columns per CTA, ring cap
   int tuned_hx_Lb = -1, tuned_hx_cols = 0, tuned_hx_nb = 0;
+  // the ligand box whose x pass the autotuner has settled (whatever kernel it runs, including
+  // those with nothing to tune); searches of that box may be captured into graphs
+  int tuned_any_Lb = -1;
   double tune_ms[8] = {};
   double stats[CDK_NSTATS] = {};
 };
@@ -455,6 +458,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   }
   if (hankel && c->tuned_hx_Lb == Lb && c->tuned_hx_cols > 0)
     hankel_plan(n, K, Lb, f16form, c->tuned_hx_cols, &hp, c->tuned_hx_nb);
+  if (c->opts.reserved[2]) c->tuned_any_Lb = Lb;
   for (long r0 = 0; r0 < nRot; r0 += wave) {
     a.nrot = (int)std::min<long>(wave, nRot - r0);
     a.rots = order + r0;
@@ -563,8 +567,7 @@ int search_device_impl(cdk_ctx* c, int nAtom, int nConf, const float* d_coor,
   // captures build-tables + every wave into one graph, later ones replay it
   cdk_ctx::GraphKey key{{d_coor, d_charge, d_eps, d_slot, d_quats, d_minE, d_idx}, nAtom, nConf, nQ, Lb, s};
   // a search that autotunes (a new ligand box) runs plainly: timing runs do not go into graphs
-  const bool graphs = c->opts.use_graphs != 0 && !(c->opts.reserved[2] && c->tuned_Lb != Lb &&
-                                                   c->tuned_hx_Lb != Lb);
+  const bool graphs = c->opts.use_graphs != 0 && !(c->opts.reserved[2] && c->tuned_any_Lb != Lb);
   if (graphs && c->gkey_seen == 2 && c->gkey == key) {
     CDK_CUDA(cudaGraphLaunch(c->gexec, s));
     CDK_CUDA(cudaEventRecord(c->ev1, s));
