@@ -254,6 +254,7 @@ int autotune_hankel(cdk_ctx* c, WaveArgs a, const RotDesc* order, long nRot, int
   for (const Cand& cd : cands) {
     HankelPlan p{};
     hankel_plan(c->n, c->K, a.Lb, f16, cd.cols, &p, cd.nb);
+    hankel_b_layout(p, a);
     float ms = 0.f, total = 0.f;
     for (int rep = 0; rep < 2; ++rep) {
       CDK_CUDA(cudaEventRecord(e0, s));
@@ -458,6 +459,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   }
   if (hankel && c->tuned_hx_Lb == Lb && c->tuned_hx_cols > 0)
     hankel_plan(n, K, Lb, f16form, c->tuned_hx_cols, &hp, c->tuned_hx_nb);
+  if (hankel) hankel_b_layout(hp, a);
   if (c->opts.reserved[2]) c->tuned_any_Lb = Lb;
   for (long r0 = 0; r0 < nRot; r0 += wave) {
     a.nrot = (int)std::min<long>(wave, nRot - r0);

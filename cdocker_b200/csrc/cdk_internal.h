@@ -72,8 +72,11 @@ struct WaveArgs {
   RotRec* rec;               // [nrot]
   float2* A;                 // [nrot][K][Lb][ncol]
   float2* B;                 // [nrot][n][ncol], or with bgroup G > 1 [nrot][n/G][ncol/2][G][2]:
-                             // the x planes grouped by G, 16 B (two columns) per (plane, pair)
-  int bgroup;                // 0 or 1: plain B layout; 2, 4, 8: grouped (streamed x pass only)
+                             // the x planes grouped by G, 16 B (two columns) per (plane, pair);
+                             // or with bcol [nrot][n/G][ncol][G]: G planes of one column
+  int bgroup;                // 0 or 1: plain B layout; 2, 4, 8: grouped (tensor-core x passes)
+  int bcol;                  // 1: the grouped layout keeps single columns (G x 8 B runs), for
+                             // x passes that own one column per CTA
   int yz_block_stages;       // inverse (y,z) kernel: 0 by grid size (block stages at n <= 64,
                              // octets at n >= 96), 1 block stages, 2 octets
   unsigned long long* keys;  // [nrot]
@@ -185,6 +188,9 @@ struct HankelPlan {
 bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out, int nb_cap = 0);
 cudaError_t launch_xpass_hankel(const WaveArgs& a, const float2* pt, const float* f16_scale,
                                 const HankelPlan& p, cudaStream_t s);
+// the B layout the plan's x pass writes (and the inverse (y,z) kernels then read): one column per
+// CTA writes single-column groups of 4 planes, two columns column-pair groups
+void hankel_b_layout(const HankelPlan& p, WaveArgs& a);
 // the stage plan of every 128-rotation tile of a wave into the tile's first RotRec
 cudaError_t launch_tile_plan(const WaveArgs& a, int jc, cudaStream_t s);
 

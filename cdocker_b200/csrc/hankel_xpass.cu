@@ -128,6 +128,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// one 32-byte store (eight floats; p 32-byte aligned)
+__device__ __forceinline__ void st_v8(void* p, float a0, float a1, float a2, float a3, float a4, float a5,
+                                      float a6, float a7) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(a0), "f"(a1), "f"(a2),
+               "f"(a3), "f"(a4), "f"(a5), "f"(a6), "f"(a7)
+               : "memory");
+}
+
 // hi/lo parts of a value (16-bit patterns): split BF16, or split FP16 of a pre-scaled value
 template <bool F16>
 __device__ __forceinline__ void split16(float v, uint16_t& hi, uint16_t& lo) {
@@ -454,12 +462,16 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
     }
     __syncwarp();
   } else {
-    // ---- epilogue: TMEM lane quarter q = rotations 32 q .. 32 q + 31
+    // ---- epilogue: TMEM lane quarter q = rotations 32 q .. 32 q + 31. A thread holds 16
+    // consecutive output planes of its rotation per TMEM load and writes them as runs: with two
+    // columns, 32 bytes per plane pair (column-pair groups of G >= 2 planes); with one column
+    // and single-column groups (G = 4), 32 bytes per 4 planes. Each store fills whole sectors.
     const int q = warp & 3;
     const int rl = 32 * q + lane;
     // plane groups of the B layout: 1, 2, 4 or 8 (a power of two: masks, no division)
     const int G2 = a.bgroup > 1 ? a.bgroup : 1;
     const int gm = G2 - 1;
+    const bool bcol = COLS == 1 && a.bcol != 0;
     int u = 0;
     for (int t = 0; t < ntiles; ++t) {
       const int r0 = t * HX_R;
@@ -485,17 +497,48 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
           tmem_ld16(tbase + (uint32_t)(cc * 2 * NMAX + NMAX + x0), im[cc]);
         }
         tmem_wait_ld();
+        // rows at or past the rotation's window are garbage the inverse (y,z) pass never reads;
+        // a run that starts inside the window is written whole (every row < N is in bounds)
+        if constexpr (COLS == 2) {
+          // column-pair groups: float4 (re, im of columns 2m, 2m + 1) of plane xp at
+          // (xp - xp % G) NCOL / 2 + m G + xp % G; planes xp, xp + 1 (xp even) adjacent when G >= 2
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const int xp = x0 + i;
-          if (xp < Wr) {
-            // plane-group layout of B: float4 (re, im of column pair 2m, 2m + 1) at
-            // (xp - xp % G) NCOL / 2 + m G + xp % G
-            const size_t f4 = (size_t)(xp & ~gm) * (NCOL / 2) + (size_t)(c0 >> 1) * G2 + (xp & gm);
-            if constexpr (COLS == 2) {
-              rowp[f4] = make_float4(re[0][i], im[0][i], re[1][i], im[1][i]);
-            } else {
-              reinterpret_cast<float2*>(rowp + f4)[c0 & 1] = make_float2(re[0][i], im[0][i]);
+          for (int i = 0; i < 16; i += 2) {
+            const int xp = x0 + i;
+            if (xp < Wr) {
+              const size_t f4 = (size_t)(xp & ~gm) * (NCOL / 2) + (size_t)(c0 >> 1) * G2 + (xp & gm);
+              if (G2 >= 2) {
+                st_v8(rowp + f4, re[0][i], im[0][i], re[1][i], im[1][i], re[0][i + 1], im[0][i + 1],
+                      re[1][i + 1], im[1][i + 1]);
+              } else {
+                rowp[f4] = make_float4(re[0][i], im[0][i], re[1][i], im[1][i]);
+                rowp[f4 + NCOL / 2] = make_float4(re[0][i + 1], im[0][i + 1], re[1][i + 1], im[1][i + 1]);
+              }
+            }
+          }
+        } else if (bcol && G2 >= 4) {
+          // single-column groups: float2 of plane xp at (xp - xp % G) NCOL + c G + xp % G; four
+          // planes from xp (a multiple of 4) are one 32-byte run
+          float2* row2 = reinterpret_cast<float2*>(rowp);
+#pragma unroll
+          for (int i = 0; i < 16; i += 4) {
+            const int xp = x0 + i;
+            if (xp < Wr)
+              st_v8(row2 + (size_t)(xp & ~gm) * NCOL + (size_t)c0 * G2 + (xp & gm), re[0][i], im[0][i],
+                    re[0][i + 1], im[0][i + 1], re[0][i + 2], im[0][i + 2], re[0][i + 3], im[0][i + 3]);
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int xp = x0 + i;
+            if (xp < Wr) {
+              if (bcol) {
+                reinterpret_cast<float2*>(rowp)[(size_t)(xp & ~gm) * NCOL + (size_t)c0 * G2 + (xp & gm)] =
+                    make_float2(re[0][i], im[0][i]);
+              } else {
+                const size_t f4 = (size_t)(xp & ~gm) * (NCOL / 2) + (size_t)(c0 >> 1) * G2 + (xp & gm);
+                reinterpret_cast<float2*>(rowp + f4)[c0 & 1] = make_float2(re[0][i], im[0][i]);
+              }
             }
           }
         }
@@ -572,9 +615,16 @@ bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out,
   return false;
 }
 
+void hankel_b_layout(const HankelPlan& p, WaveArgs& a) {
+  a.bcol = p.cols == 1 ? 1 : 0;
+  a.bgroup = p.cols == 1 ? 4 : stream_bgroup();
+}
+
 cudaError_t launch_xpass_hankel(const WaveArgs& a, const float2* pt, const float* f16_scale,
                                 const HankelPlan& p, cudaStream_t s) {
   if (!a.lop || !pt || a.K > KMAX) return cudaErrorInvalidValue;
+  // the B layout must be the plan's (the inverse (y,z) pass reads what this pass writes)
+  if ((a.bcol != 0) != (p.cols == 1) || (a.bcol && a.bgroup != 4)) return cudaErrorInvalidValue;
   HxScale sc{};
   for (int k = 0; k < a.K; ++k) sc.s[k] = (a.f16 && f16_scale) ? f16_scale[k] : 1.f;
   // the stage plan of every 128-rotation tile (channels, K-steps, largest window)

@@ -685,7 +685,25 @@ __global__ void __launch_bounds__(256, 2) k_xpass2(WaveArgs a, int rot_per_cta) 
 
 // ---------------------------------------------------------------------------------------
 // keep the two smallest keys (b1 < b2) of a stream of distinct keys
+// Plane x of rotation r read from B in any of its layouts; at(f) is column f of the plane.
+// Column-pair groups (cs = 1): float2 (f >> 1) 2G + (f & 1) past the plane's first pair; single-
+// column groups (cs = 0): float2 f G past the plane's first column. The plain layout is G = 1.
+struct BPlane {
+  const float2* p;
+  int cs, gs;
+  __device__ __forceinline__ BPlane(const WaveArgs& a, int r, int x, int n, int ncol) {
+    const int G = a.bgroup > 1 ? a.bgroup : 1;
+    cs = a.bcol ? 0 : 1;
+    gs = G << cs;
+    p = a.B + ((size_t)r * n + (x - x % G)) * ncol + ((x % G) << cs);
+  }
+  __device__ __forceinline__ float2 at(int f) const { return p[(size_t)(f >> cs) * gs + (f & cs)]; }
+};
+
 __device__ __forceinline__ void top2_insert(unsigned long long k, unsigned long long& b1, unsigned long long& b2) {
+  // most candidates lose to the current second-smallest on the energy bits alone (one 32-bit
+  // compare); the 64-bit order decides the rest
+  if ((unsigned int)(k >> 32) > (unsigned int)(b2 >> 32)) return;
   if (k < b1) {
     b2 = b1;
     b1 = k;
@@ -727,9 +745,9 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
   const int tid = threadIdx.x, nthr = blockDim.x;
   for (int i = tid; i < N; i += nthr) tw[i] = a.tw[i];
   // plane x: NCOL / 2 column pairs, 16 B each, contiguous (plain layout) or every G-th of the
-  // plane group (grouped layout, G planes per 16 B x column-pair block)
-  const int G = a.bgroup > 1 ? a.bgroup : 1;
-  const float4* src = reinterpret_cast<const float4*>(a.B + ((size_t)r * N + (x - x % G)) * NCOL) + x % G;
+  // plane group (grouped layout, G planes per 16 B x column-pair block); or, single-column
+  // groups, one float2 of every G
+  const BPlane bp(a, r, x, N, NCOL);
   if constexpr (ALIAS) {
     // y: positions -> natural rows, the first (R1-point, twiddle-free) stage reading its rows
     // straight from B: item (column l, block b) takes positions b R1 + j of column l, plane
@@ -737,15 +755,11 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
     using PL = FFTPlan<N>;
     constexpr int R0 = PL::R0, R1 = PL::R1;
     static_assert(PL::NS == 2 && StageM<N, 2>::value == 1, "two-stage plan");
-    const float2* src2 = reinterpret_cast<const float2*>(src);
     for (int w = tid; w < NZH * R0; w += nthr) {
       const int b = w / NZH, l = w - b * NZH;
       float2 v[R1];
 #pragma unroll
-      for (int j = 0; j < R1; ++j) {
-        const int f = (b * R1 + j) * NZH + l;
-        v[j] = src2[(size_t)(f >> 1) * 2 * G + (f & 1)];
-      }
+      for (int j = 0; j < R1; ++j) v[j] = bp.at((b * R1 + j) * NZH + l);
       Radix<R1, +1>::run(v);
       float2* p = O + l + b * R1 * NZH;
 #pragma unroll
@@ -755,8 +769,7 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
     fft_stage<N, R0, StageM<N, 1>::value, true>(O, NZH, 1, NZH, tw, tid, nthr);
     __syncthreads();
   } else {
-    float4* dst = reinterpret_cast<float4*>(O);
-    for (int i = tid; i < NCOL / 2; i += nthr) dst[i] = src[(size_t)i * G];
+    for (int i = tid; i < NCOL; i += nthr) O[i] = bp.at(i);
     __syncthreads();
     fft_lines<N, true>(O, NZH, 1, NZH, tw, tid, nthr);  // y: positions -> natural rows
   }
@@ -946,9 +959,7 @@ __global__ void __launch_bounds__(32 * kOctWarps, (N <= 64 ? 4 : 2)) k_yz_octet(
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int o = lane >> 3, t = lane & 7, g = warp * 4 + o;
   for (int i = tid; i < N; i += 32 * kOctWarps) s_tw[i] = a.tw[i];
-  const int G = a.bgroup > 1 ? a.bgroup : 1;
-  const float2* src2 = reinterpret_cast<const float2*>(
-      reinterpret_cast<const float4*>(a.B + ((size_t)r * N + (x - x % G)) * NCOL) + x % G);
+  const BPlane bp(a, r, x, N, NCOL);
   float2* S = s_xall + (size_t)(warp * 4 + o) * 8 * XS;
   __syncthreads();
   // the second stage of one line from the exchange slice: groups np = t + 8 q, natural output
@@ -979,8 +990,7 @@ __global__ void __launch_bounds__(32 * kOctWarps, (N <= 64 ? 4 : 2)) k_yz_octet(
     float2 v[R1];
 #pragma unroll
     for (int j = 0; j < R1; ++j) {
-      const int f = (t * R1 + j) * NZH + l;
-      v[j] = act ? src2[(size_t)(f >> 1) * 2 * G + (f & 1)] : make_float2(0.f, 0.f);
+      v[j] = act ? bp.at((t * R1 + j) * NZH + l) : make_float2(0.f, 0.f);
     }
     Radix<R1, +1>::run(v);
 #pragma unroll

@@ -406,6 +406,8 @@ void worker_loop(cdk_server* s) {
     a.lop = tc_wave ? lop_base : nullptr;
     a.f16 = (tc_wave && f16) ? 1 : 0;
     a.bgroup = tc_wave ? stream_bgroup() : 1;
+    a.bcol = 0;
+    if (tc_wave && !tile_wave) hankel_b_layout(hp, a);
     if (le == cudaSuccess) {
       note(launch_prep(a, s->stream));
       note(launch_spread_yz(a, s->stream));
