@@ -143,7 +143,7 @@ struct cdk_ctx {
   // autotuned x-pass configuration (opts.reserved[2] = 1), per (Lb)
   int tuned_Lb = -1, tuned_col_tile = 0, tuned_chunk = 0;
   // autotuned tensor-core x pass (Hankel operator), per (Lb, form): columns per CTA, ring cap
-  int tuned_hx_Lb = -1, tuned_hx_cols = 0, tuned_hx_nb = 0;
+  int tuned_hx_Lb = -1, tuned_hx_cols = 0, tuned_hx_nb = 0, tuned_hx_ks = 0;
   // the ligand box whose x pass the autotuner has settled (whatever kernel it runs, including
   // those with nothing to tune); searches of that box may be captured into graphs
   int tuned_any_Lb = -1;
@@ -234,16 +234,17 @@ int autotune_hankel(cdk_ctx* c, WaveArgs a, const RotDesc* order, long nRot, int
   a.rots = order;
   CDK_CUDA(launch_prep(a, s));
   CDK_CUDA(launch_spread_yz(a, s));
-  struct Cand { int cols, nb; };
+  struct Cand { int cols, nb, ks; };
   std::vector<Cand> cands;
   for (int cols : {1, 2})
-    for (int nb : {8, 16, 32}) {
-      HankelPlan p{};
-      if (!hankel_plan(c->n, c->K, a.Lb, f16, cols, &p, nb) || p.cols != cols) continue;
-      bool dup = false;
-      for (const Cand& q : cands) dup |= (q.cols == cols && q.nb == p.nb);
-      if (!dup) cands.push_back({cols, p.nb});
-    }
+    for (int ks : {1, 2})
+      for (int nb : {4, 8, 16, 32}) {
+        HankelPlan p{};
+        if (!hankel_plan(c->n, c->K, a.Lb, f16, cols, &p, nb, ks) || p.cols != cols || p.ks != ks) continue;
+        bool dup = false;
+        for (const Cand& q : cands) dup |= (q.cols == cols && q.nb == p.nb && q.ks == ks);
+        if (!dup) cands.push_back({cols, p.nb, ks});
+      }
   if (cands.empty()) return CDK_OK;
   cudaEvent_t e0, e1;
   CDK_CUDA(cudaEventCreate(&e0));
@@ -253,7 +254,7 @@ int autotune_hankel(cdk_ctx* c, WaveArgs a, const RotDesc* order, long nRot, int
   int i = 0;
   for (const Cand& cd : cands) {
     HankelPlan p{};
-    hankel_plan(c->n, c->K, a.Lb, f16, cd.cols, &p, cd.nb);
+    hankel_plan(c->n, c->K, a.Lb, f16, cd.cols, &p, cd.nb, cd.ks);
     hankel_b_layout(p, a);
     float ms = 0.f, total = 0.f;
     for (int rep = 0; rep < 2; ++rep) {
@@ -276,6 +277,7 @@ int autotune_hankel(cdk_ctx* c, WaveArgs a, const RotDesc* order, long nRot, int
   c->tuned_hx_Lb = a.Lb;
   c->tuned_hx_cols = pick.cols;
   c->tuned_hx_nb = pick.nb;
+  c->tuned_hx_ks = pick.ks;
   return CDK_OK;
 }
 
@@ -302,7 +304,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   const bool streamed = can_stream && (variant == 3 || variant == 0);
   HankelPlan hp{};
   const bool hankel = tc && !streamed && (variant == 0 || variant == 4) && direct_planes(probe) &&
-                      hankel_plan(n, K, Lb, f16form, c->opts.reserved[5], &hp);
+                      hankel_plan(n, K, Lb, f16form, c->opts.reserved[5] & 3, &hp, 0, (c->opts.reserved[5] >> 2) & 3);
   if (streamed && !c->d_top) {
     const size_t tb = stream_top_bytes(n, K);
     if (cudaMalloc(&c->d_top, tb) != cudaSuccess) {
@@ -458,7 +460,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     if (rc) return rc;
   }
   if (hankel && c->tuned_hx_Lb == Lb && c->tuned_hx_cols > 0)
-    hankel_plan(n, K, Lb, f16form, c->tuned_hx_cols, &hp, c->tuned_hx_nb);
+    hankel_plan(n, K, Lb, f16form, c->tuned_hx_cols, &hp, c->tuned_hx_nb, c->tuned_hx_ks);
   if (hankel) hankel_b_layout(hp, a);
   if (c->opts.reserved[2]) c->tuned_any_Lb = Lb;
   for (long r0 = 0; r0 < nRot; r0 += wave) {

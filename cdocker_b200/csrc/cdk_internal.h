@@ -181,11 +181,14 @@ struct HankelPlan {
   int G;            // 128-byte groups of one Hankel buffer
   int jc;           // 8-plane K-steps of the ligand box
   int nb;           // ring stages
+  int ks;           // K-steps per ring stage (1 or 2)
   size_t smem;      // dynamic shared memory per CTA
   int ctas_per_sm;  // 1 or 2
 };
-// nb_cap > 0: at most that many ring stages (the autotuner's candidates)
-bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out, int nb_cap = 0);
+// nb_cap > 0: at most that many ring stages (the autotuner's candidates); ks_pref > 0: that many
+// K-steps per stage
+bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out, int nb_cap = 0,
+                 int ks_pref = 0);
 cudaError_t launch_xpass_hankel(const WaveArgs& a, const float2* pt, const float* f16_scale,
                                 const HankelPlan& p, cudaStream_t s);
 // the B layout the plan's x pass writes (and the inverse (y,z) kernels then read): one column per

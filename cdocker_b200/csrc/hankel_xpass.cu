@@ -22,14 +22,14 @@
 // P~ and stays resident: no operator bytes are streamed per tile.
 //
 // CTA = COLS columns, persistent over the wave's 128-rotation tiles; 288 threads:
-//   warps 0-3  producers: thread = rotation of the tile; per stage (one K-step of one channel,
-//              all COLS columns) 16-byte cp.async copies of its ligand rows (rows of chunks the
+//   warps 0-3  producers: thread = rotation of the tile; per stage (one or two K-steps of one
+//              channel, all COLS columns) 16-byte cp.async copies of its ligand rows (rows of chunks the
 //              rotation does not touch are zero-filled by the copy itself), then one
 //              cp.async-completion arrival on the stage's "full" mbarrier;
-//   warp 4     MMA issuer: one elected lane issues per stage and column 2 (real, imaginary) x
-//              2 (split-FP16: operator hi, lo) or x 3 (split-BF16: hi*hi, lo*hi, hi*lo) MMAs,
-//              commits each stage to its "empty" mbarrier and each tile to a TMEM "full"
-//              mbarrier;
+//   warp 4     MMA issuer (one elected lane issues): per K-step and column 2 (real, imaginary) x 2
+//              (split-FP16: operator hi, lo) or x 3 (split-BF16: hi*hi, lo*hi, hi*lo) MMAs;
+//              commits each stage (1 or 2 K-steps) to its "empty" mbarrier and each tile to a
+//              TMEM "full" mbarrier;
 //   warps 5-8  epilogue: TMEM -> B of tile t while the MMAs of tile t+1 accumulate into the
 //              other of two TMEM accumulator sets (TMEM "empty" mbarrier per set).
 // Every wait is bounded; a wait that gives up sets the fault flag, the other roles stop at their
@@ -40,6 +40,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "cdk_internal.h"
 
@@ -192,15 +193,17 @@ __device__ __forceinline__ uint32_t make_idesc(int n) {
 struct HxLayout {
   uint32_t S;         // one Hankel buffer: G groups x 128 B
   uint32_t op;        // the column operator: COLS x K x (hi, lo) x 3 buffers
-  uint32_t stage;     // one ring stage: COLS x LPARTS x 4 KB
+  uint32_t ksub;      // one K-step of a stage: COLS x LPARTS x 4 KB
+  uint32_t stage;     // one ring stage: ks K-steps
   uint32_t build;     // scratch of the operator build (inside the ring area)
 };
 
-__host__ __device__ inline HxLayout hx_layout(int n, int K, int cols, bool f16, int G) {
+__host__ __device__ inline HxLayout hx_layout(int n, int K, int cols, bool f16, int G, int ks) {
   HxLayout L;
   L.S = (uint32_t)G * HX_CORE;
   L.op = (uint32_t)cols * K * 2 * 3 * L.S;
-  L.stage = (uint32_t)cols * (f16 ? 1 : 2) * HX_TILE;
+  L.ksub = (uint32_t)cols * (f16 ? 1 : 2) * HX_TILE;
+  L.stage = (uint32_t)ks * L.ksub;
   // P~ of the CTA's columns (float2) + their four split arrays (re hi, re lo, im hi, im lo),
   // each n + 32 halves long (the first 32 repeated after the end: no wrap in the group build)
   L.build = (uint32_t)cols * K * n * 8 + (uint32_t)cols * K * 4 * (n + 32) * 2;
@@ -209,7 +212,7 @@ __host__ __device__ inline HxLayout hx_layout(int n, int K, int cols, bool f16, 
 
 template <int N, int COLS, bool F16>
 __global__ void __launch_bounds__(HX_THREADS, 2)
-    k_xpass_hankel(WaveArgs a, const float2* __restrict__ pt, HxScale sc, int jc, int G, int nb) {
+    k_xpass_hankel(WaveArgs a, const float2* __restrict__ pt, HxScale sc, int jc, int G, int nb, int ks) {
   constexpr int NCOL = N * (N / 2 + 1);
   constexpr int LPARTS = F16 ? 1 : 2;
   constexpr int NMAX = N;                          // TMEM columns of one output block (re or im)
@@ -227,7 +230,7 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
   __shared__ volatile int s_fail;
   __shared__ uint32_t s_tmem;
   const int K = a.K;
-  const HxLayout L = hx_layout(N, K, COLS, F16, G);
+  const HxLayout L = hx_layout(N, K, COLS, F16, G, ks);
   unsigned char* op = base;              // resident operator
   unsigned char* ring = base + L.op;     // ring stages (the operator build uses it first)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -353,25 +356,31 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
         const unsigned int jr = (unsigned int)(((k < 8 ? jr_lo : jr_hi) >> (8 * (k & 7))) & 255);
         const int jl = (int)(jr & 15), jh = (int)(jr >> 4);
         const uint4* src0 = reinterpret_cast<const uint4*>(a.lop) + rot_rows + (size_t)k * ROWS * RS;
-        for (int j = jlo; j <= jhi; ++j, ++s) {
+        // a stage: K-steps j0 .. min(j0 + ks, jhi + 1) - 1 of this channel
+        for (int j0 = jlo; j0 <= jhi; j0 += ks, ++s) {
           if (s >= nb && !mbar_wait(smem_u32(&s_empty[b]), (round - 1) & 1u, &s_fail)) {
             s_fail = 1;
             ok = false;
             break;
           }
           const uint32_t st = ring_s + (uint32_t)b * L.stage;
-          const bool have = jl <= j && j <= jh;
+          const int jn = min(ks, jhi + 1 - j0);
+          for (int jj = 0; jj < jn; ++jj) {
+            const int j = j0 + jj;
+            const bool have = jl <= j && j <= jh;
 #pragma unroll
-          for (int cc = 0; cc < COLS; ++cc)
+            for (int cc = 0; cc < COLS; ++cc)
 #pragma unroll
-            for (int hl = 0; hl < LPARTS; ++hl)
+              for (int hl = 0; hl < LPARTS; ++hl)
 #pragma unroll
-              for (int part = 0; part < 2; ++part) {
-                const uint4* src = src0 + (size_t)((hl * 4 + j) * 2 + part) * RS + cc;
-                const uint32_t dst = st + (uint32_t)(cc * LPARTS + hl) * HX_TILE + (uint32_t)part * (HX_TILE / 2) + row_s;
-                asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(have ? 16 : 0)
-                             : "memory");
-              }
+                for (int part = 0; part < 2; ++part) {
+                  const uint4* src = src0 + (size_t)((hl * 4 + j) * 2 + part) * RS + cc;
+                  const uint32_t dst = st + (uint32_t)jj * L.ksub + (uint32_t)(cc * LPARTS + hl) * HX_TILE +
+                                       (uint32_t)part * (HX_TILE / 2) + row_s;
+                  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(have ? 16 : 0)
+                               : "memory");
+                }
+          }
           asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&s_full[b])) : "memory");
           if (++b == nb) {
             b = 0;
@@ -383,7 +392,14 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
   } else if (warp == HX_MMA_WARP) {
-    // ---- MMA issuer: the whole warp runs the loop (uniform descriptors), one lane issues
+    // ---- MMA issuer: the whole warp runs the loop (uniform control flow), one elected lane
+    // issues each stage's MMAs and its commit. Shared-memory descriptors are built once; the
+    // start-address field (bits 0-13) holds the byte address >> 4, so moving a descriptor by a
+    // 16-byte aligned byte offset adds offset >> 4 (shared addresses stay below 256 KB: no carry
+    // out of the field).
+    const uint64_t dring = make_desc(ring_s, HX_TILE / 2, HX_CORE);  // ligand rows, slot 0
+    const uint64_t dop = make_desc(op_s, L.S, HX_CORE);              // operator, group 0
+    const uint64_t sS = L.S >> 4;
     int s = 0, u = 0, b = 0;
     uint32_t round = 0;
     bool good = true;
@@ -400,11 +416,12 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
       const int nt = tile_n(p.wmax);
       const uint32_t idesc = make_idesc<F16>(nt);
       const uint32_t dset = tmem + (uint32_t)d * DSET;
-      bool first = true;
+      uint32_t acc0 = 0u;  // the tile's first K-step starts its accumulators
       for (int ai = 0; ai < p.nact && good; ++ai) {
         const int k = (int)((p.pk >> (4 * ai)) & 15);
         const int jlo = (int)((p.pl >> (4 * ai)) & 15), jhi = (int)((p.ph >> (4 * ai)) & 15);
-        for (int j = jlo; j <= jhi; ++j, ++s) {
+        const uint64_t dopk = dop + (uint64_t)((k * 2 * 3) * L.S >> 4);
+        for (int j0 = jlo; j0 <= jhi; j0 += ks, ++s) {
           if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_full[b]), round & 1u, &s_fail))) {
             if (lane == 0) s_fail = 1;
             good = false;
@@ -413,30 +430,32 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
           // the producers' cp.async writes (generic proxy) reach the tensor core (async proxy)
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const uint32_t acc0 = first ? 0u : 1u;
+          const int jn = min(ks, jhi + 1 - j0);
+          const uint64_t aslot = dring + (uint64_t)((b * L.stage) >> 4);
+          if (elect_one()) {
+            for (int jj = 0; jj < jn; ++jj) {
 #pragma unroll
-          for (int cc = 0; cc < COLS; ++cc) {
-            const uint32_t st = ring_s + (uint32_t)b * L.stage + (uint32_t)(cc * LPARTS) * HX_TILE;
-            const uint64_t ahi = make_desc(st, HX_TILE / 2, HX_CORE);
-            const uint32_t obase = op_s + (uint32_t)(((cc * K + k) * 2) * 3) * L.S + (uint32_t)j * HX_CORE;
-            const uint64_t bre_hi = make_desc(obase, L.S, HX_CORE);          // Re | Im
-            const uint64_t bim_hi = make_desc(obase + L.S, L.S, HX_CORE);    // Im | -Re
-            const uint64_t bre_lo = make_desc(obase + 3 * L.S, L.S, HX_CORE);
-            const uint64_t bim_lo = make_desc(obase + 4 * L.S, L.S, HX_CORE);
-            const uint32_t dre = dset + (uint32_t)(cc * 2 * NMAX), dim = dre + NMAX;
-            if (elect_one()) umma(dre, ahi, bre_hi, idesc, acc0);
-            if (elect_one()) umma(dim, ahi, bim_hi, idesc, acc0);
-            if constexpr (!F16) {
-              const uint64_t alo = make_desc(st + HX_TILE, HX_TILE / 2, HX_CORE);
-              if (elect_one()) umma(dre, alo, bre_hi, idesc, 1u);
-              if (elect_one()) umma(dim, alo, bim_hi, idesc, 1u);
+              for (int cc = 0; cc < COLS; ++cc) {
+                const uint64_t ahi = aslot + (uint64_t)((jj * L.ksub + cc * LPARTS * HX_TILE) >> 4);
+                // Re | Im and Im | -Re operands (one buffer apart), hi then lo part (3 buffers on)
+                const uint64_t bre_hi = dopk + (uint64_t)(cc * K * 2 * 3) * sS + (uint64_t)((j0 + jj) * (HX_CORE >> 4));
+                const uint32_t dre = dset + (uint32_t)(cc * 2 * NMAX), dim = dre + NMAX;
+                umma(dre, ahi, bre_hi, idesc, acc0);
+                umma(dim, ahi, bre_hi + sS, idesc, acc0);
+                if constexpr (!F16) {
+                  const uint64_t alo = ahi + (HX_TILE >> 4);
+                  umma(dre, alo, bre_hi, idesc, 1u);
+                  umma(dim, alo, bre_hi + sS, idesc, 1u);
+                }
+                umma(dre, ahi, bre_hi + 3 * sS, idesc, 1u);
+                umma(dim, ahi, bre_hi + 4 * sS, idesc, 1u);
+              }
+              acc0 = 1u;
             }
-            if (elect_one()) umma(dre, ahi, bre_lo, idesc, 1u);
-            if (elect_one()) umma(dim, ahi, bim_lo, idesc, 1u);
+            umma_commit(smem_u32(&s_empty[b]));
           }
-          if (elect_one()) umma_commit(smem_u32(&s_empty[b]));
           __syncwarp();
-          first = false;
+          acc0 = 1u;
           if (++b == nb) {
             b = 0;
             ++round;
@@ -527,6 +546,16 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
               st_v8(row2 + (size_t)(xp & ~gm) * NCOL + (size_t)c0 * G2 + (xp & gm), re[0][i], im[0][i],
                     re[0][i + 1], im[0][i + 1], re[0][i + 2], im[0][i + 2], re[0][i + 3], im[0][i + 3]);
           }
+        } else if (bcol && G2 == 2) {
+          // single-column groups of 2 planes: one 16-byte run per plane pair
+          float2* row2 = reinterpret_cast<float2*>(rowp);
+#pragma unroll
+          for (int i = 0; i < 16; i += 2) {
+            const int xp = x0 + i;
+            if (xp < Wr)
+              *reinterpret_cast<float4*>(row2 + (size_t)xp * NCOL + (size_t)c0 * 2) =
+                  make_float4(re[0][i], im[0][i], re[0][i + 1], im[0][i + 1]);
+          }
         } else {
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
@@ -564,7 +593,7 @@ constexpr size_t kSmemCap = 227 * 1024 - 1024;
 constexpr size_t kSmemHalf = 110 * 1024;  // per CTA when two share an SM
 
 template <int N, int COLS, bool F16>
-cudaError_t launch_hx(const WaveArgs& a, const float2* pt, const HxScale& sc, int jc, int G, int nb,
+cudaError_t launch_hx(const WaveArgs& a, const float2* pt, const HxScale& sc, int jc, int G, int nb, int ks,
                       size_t smem, cudaStream_t s) {
   constexpr int NCOL = N * (N / 2 + 1);
   auto kern = k_xpass_hankel<N, COLS, F16>;
@@ -572,17 +601,19 @@ cudaError_t launch_hx(const WaveArgs& a, const float2* pt, const HxScale& sc, in
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  kern<<<NCOL / COLS, HX_THREADS, smem, s>>>(a, pt, sc, jc, G, nb);
+  kern<<<NCOL / COLS, HX_THREADS, smem, s>>>(a, pt, sc, jc, G, nb, ks);
   return cudaGetLastError();
 }
 
 }  // namespace
 
 // Shape of the x pass for (n, K, ligand box, form): columns per CTA, Hankel groups, ring stages
-// and dynamic shared memory. cols_pref: 0 = automatic, 1 or 2 = that many columns (2 only where
-// the operator of two columns fits). Returns false when the operator and a minimal ring do not
-// fit one CTA (large K at large n) or the box exceeds 32 planes.
-bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out, int nb_cap) {
+// (each of ks K-steps) and dynamic shared memory. cols_pref: 0 = automatic, 1 or 2 = that many
+// columns (2 only where the operator of two columns fits); ks_pref: 0 = automatic (2 K-steps per
+// stage where the ligand box has several and the ring keeps as many K-steps in flight), 1 or 2.
+// Returns false when the operator and a minimal ring do not fit one CTA (large K at large n) or
+// the box exceeds 32 planes.
+bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out, int nb_cap, int ks_pref) {
   if (!(n == 32 || n == 64 || n == 96 || n == 128) || K < 1 || K > KMAX || Lb < 1 || Lb > 8 * HX_JMAX)
     return false;
   const int jc = (Lb + 7) / 8;
@@ -590,41 +621,57 @@ bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out,
   for (int cols : {2, 1}) {
     if (cols_pref && cols != cols_pref) continue;
     if (cols == 2 && n > 64) continue;  // the tensor memory of two double-buffered columns
-    const HxLayout L = hx_layout(n, K, cols, f16, G);
     // two CTAs per SM when the tensor memory allows (<= 256 columns each) and the operator
-    // leaves room for a ring of at least 8 stages; else one CTA with the largest ring
+    // leaves room for a ring of at least 8 K-steps; else one CTA with the largest ring
     const bool two = 2 * 2 * cols * n <= 256;
     for (int pass = two ? 0 : 1; pass < 2; ++pass) {
       const size_t cap = (pass == 0 ? kSmemHalf : kSmemCap) - 1024;
-      if (cap <= L.op) continue;
-      int nb = (int)std::min<size_t>(HX_MAXSTAGES, (cap - L.op) / L.stage);
-      if (nb < (pass == 0 ? 8 : 4) || (size_t)nb * L.stage < L.build) continue;
-      if (nb_cap > 0 && nb_cap < nb && (size_t)nb_cap * L.stage >= L.build) nb = nb_cap;
-      out->cols = cols;
-      out->G = G;
-      out->jc = jc;
-      out->nb = nb;
-      out->smem = (size_t)L.op + (size_t)nb * L.stage + 1024;
-      // a CTA that takes all 512 tensor-memory columns must have its SM alone: its shared
-      // memory then keeps a second CTA out (tcgen05.alloc would otherwise stall it)
-      if (pass == 1) out->smem = std::max(out->smem, (size_t)120 * 1024);
-      out->ctas_per_sm = pass == 0 ? 2 : 1;
-      return true;
+      for (int ks : {2, 1}) {
+        if (ks_pref && ks != ks_pref) continue;
+        if (ks == 2 && jc < 2 && !ks_pref) continue;
+        const HxLayout L = hx_layout(n, K, cols, f16, G, ks);
+        if (cap <= L.op) continue;
+        int nb = (int)std::min<size_t>(HX_MAXSTAGES, (cap - L.op) / L.stage);
+        if (nb < 2 || nb * ks < (pass == 0 ? 8 : 4) || (size_t)nb * L.stage < L.build) continue;
+        if (nb_cap > 0 && nb_cap < nb && (size_t)nb_cap * L.stage >= L.build && nb_cap >= 2) nb = nb_cap;
+        out->cols = cols;
+        out->G = G;
+        out->jc = jc;
+        out->nb = nb;
+        out->ks = ks;
+        out->smem = (size_t)L.op + (size_t)nb * L.stage + 1024;
+        // a CTA that takes all 512 tensor-memory columns must have its SM alone: its shared
+        // memory then keeps a second CTA out (tcgen05.alloc would otherwise stall it)
+        if (pass == 1) out->smem = std::max(out->smem, (size_t)120 * 1024);
+        out->ctas_per_sm = pass == 0 ? 2 : 1;
+        return true;
+      }
     }
   }
   return false;
 }
 
+// planes per single-column group: 4 (32-byte runs, the default) or 2 (16-byte runs); the
+// environment variable CDK_B_COLGROUP overrides it, for measurement
+static int hankel_colgroup() {
+  static const int g = [] {
+    const char* e = std::getenv("CDK_B_COLGROUP");
+    const int v = e ? std::atoi(e) : 4;
+    return (v == 2 || v == 4) ? v : 4;
+  }();
+  return g;
+}
+
 void hankel_b_layout(const HankelPlan& p, WaveArgs& a) {
   a.bcol = p.cols == 1 ? 1 : 0;
-  a.bgroup = p.cols == 1 ? 4 : stream_bgroup();
+  a.bgroup = p.cols == 1 ? hankel_colgroup() : stream_bgroup();
 }
 
 cudaError_t launch_xpass_hankel(const WaveArgs& a, const float2* pt, const float* f16_scale,
                                 const HankelPlan& p, cudaStream_t s) {
   if (!a.lop || !pt || a.K > KMAX) return cudaErrorInvalidValue;
   // the B layout must be the plan's (the inverse (y,z) pass reads what this pass writes)
-  if ((a.bcol != 0) != (p.cols == 1) || (a.bcol && a.bgroup != 4)) return cudaErrorInvalidValue;
+  if ((a.bcol != 0) != (p.cols == 1) || (a.bcol && a.bgroup != 2 && a.bgroup != 4)) return cudaErrorInvalidValue;
   HxScale sc{};
   for (int k = 0; k < a.K; ++k) sc.s[k] = (a.f16 && f16_scale) ? f16_scale[k] : 1.f;
   // the stage plan of every 128-rotation tile (channels, K-steps, largest window)
@@ -632,10 +679,10 @@ cudaError_t launch_xpass_hankel(const WaveArgs& a, const float2* pt, const float
   if (e != cudaSuccess) return e;
 #define CDK_HX(NN)                                                                               \
   case NN:                                                                                       \
-    if (a.f16) return p.cols == 2 ? launch_hx<NN, (NN <= 64 ? 2 : 1), true>(a, pt, sc, p.jc, p.G, p.nb, p.smem, s) \
-                                  : launch_hx<NN, 1, true>(a, pt, sc, p.jc, p.G, p.nb, p.smem, s);             \
-    return p.cols == 2 ? launch_hx<NN, (NN <= 64 ? 2 : 1), false>(a, pt, sc, p.jc, p.G, p.nb, p.smem, s)       \
-                       : launch_hx<NN, 1, false>(a, pt, sc, p.jc, p.G, p.nb, p.smem, s);
+    if (a.f16) return p.cols == 2 ? launch_hx<NN, (NN <= 64 ? 2 : 1), true>(a, pt, sc, p.jc, p.G, p.nb, p.ks, p.smem, s) \
+                                  : launch_hx<NN, 1, true>(a, pt, sc, p.jc, p.G, p.nb, p.ks, p.smem, s);             \
+    return p.cols == 2 ? launch_hx<NN, (NN <= 64 ? 2 : 1), false>(a, pt, sc, p.jc, p.G, p.nb, p.ks, p.smem, s)       \
+                       : launch_hx<NN, 1, false>(a, pt, sc, p.jc, p.G, p.nb, p.ks, p.smem, s);
   switch (a.n) {
     CDK_HX(32)
     CDK_HX(64)
