@@ -158,7 +158,7 @@ class Receptor:
         opts.reserved[2] = 1 if autotune else 0
         opts.reserved[3] = (1 if tc_mma_sync else 2 if tc_build else 3 if tc_stream_tiles
                             else 4 if tc_hankel else 0)
-        opts.reserved[5] = (tc_cols & 3) | ((tc_ksteps & 3) << 2)
+        opts.reserved[5] = (tc_cols & 3) | ((tc_ksteps & 7) << 2)
         opts.reserved[6] = top_k
         opts.reserved[7] = 0 if tie_break else 1
         opts.reserved[4] = 0 if group_rotations else 1

@@ -304,7 +304,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   const bool streamed = can_stream && (variant == 3 || variant == 0);
   HankelPlan hp{};
   const bool hankel = tc && !streamed && (variant == 0 || variant == 4) && direct_planes(probe) &&
-                      hankel_plan(n, K, Lb, f16form, c->opts.reserved[5] & 3, &hp, 0, (c->opts.reserved[5] >> 2) & 3);
+                      hankel_plan(n, K, Lb, f16form, c->opts.reserved[5] & 3, &hp, 0, (c->opts.reserved[5] >> 2) & 7);
   if (streamed && !c->d_top) {
     const size_t tb = stream_top_bytes(n, K);
     if (cudaMalloc(&c->d_top, tb) != cudaSuccess) {

@@ -181,7 +181,7 @@ struct HankelPlan {
   int G;            // 128-byte groups of one Hankel buffer
   int jc;           // 8-plane K-steps of the ligand box
   int nb;           // ring stages
-  int ks;           // K-steps per ring stage (1 or 2)
+  int ks;           // K-steps per ring stage (1 to 4)
   size_t smem;      // dynamic shared memory per CTA
   int ctas_per_sm;  // 1 or 2
 };

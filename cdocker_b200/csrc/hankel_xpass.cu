@@ -322,20 +322,37 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
     constexpr int ROWS = 8 * LPARTS;                // rows per (rotation, channel)
     int s = 0, b = 0;      // stages issued, ring slot of stage s
     uint32_t round = 0;    // s / nb (the ring pass), kept as a counter: no division per stage
-    for (int t = 0; t < ntiles; ++t) {
+    // the next tile's plan and this thread's rotation record are loaded one tile ahead, so
+    // their latency hides behind the current tile's copies
+    struct Ahead {
+      TilePlan p;
+      uint4 x[4];  // xlo[16] then xhi[16]
+      int valid;
+    };
+    auto fetch = [&](int t, Ahead& f) {
       const int r0 = t * HX_R;
       const int nr = min(HX_R, a.nrot - r0);
-      const TilePlan p = load_plan(a.rec + r0);
-      if (p.steps == 0) continue;
+      f.p = load_plan(a.rec + r0);
       const RotRec* rec = a.rec + r0 + min(rr, nr - 1);
-      const bool live = rr < nr && rec->valid;
+      f.valid = rec->valid;
+      const uint4* xr = reinterpret_cast<const uint4*>(rec->xlo);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) f.x[i] = xr[i];
+    };
+    Ahead nxt;
+    if (ntiles > 0) fetch(0, nxt);
+    for (int t = 0; t < ntiles; ++t) {
+      const Ahead cur = nxt;
+      if (t + 1 < ntiles) fetch(t + 1, nxt);
+      const int r0 = t * HX_R;
+      const int nr = min(HX_R, a.nrot - r0);
+      const TilePlan p = cur.p;
+      if (p.steps == 0) continue;
+      const bool live = rr < nr && cur.valid;
       // this rotation's chunk range per channel, 8 bits each (0x0F: none)
       uint64_t jr_lo = 0, jr_hi = 0;
       {
-        uint4 v[4];
-        const uint4* xr = reinterpret_cast<const uint4*>(rec->xlo);  // xlo[16] then xhi[16]
-#pragma unroll
-        for (int i = 0; i < 4; ++i) v[i] = xr[i];
+        const uint4* v = cur.x;
         const short* lo16 = reinterpret_cast<const short*>(&v[0]);
         const short* hi16 = reinterpret_cast<const short*>(&v[2]);
 #pragma unroll
@@ -403,8 +420,11 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
     int s = 0, u = 0, b = 0;
     uint32_t round = 0;
     bool good = true;
+    TilePlan pn{};  // the next tile's plan, loaded one tile ahead
+    if (ntiles > 0) pn = load_plan(a.rec);
     for (int t = 0; t < ntiles && good; ++t) {
-      const TilePlan p = load_plan(a.rec + t * HX_R);
+      const TilePlan p = pn;
+      if (t + 1 < ntiles) pn = load_plan(a.rec + (t + 1) * HX_R);
       if (p.steps == 0) continue;
       const int d = u & 1;
       if (u >= 2 && !__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_tempty[d]), (uint32_t)((u >> 1) - 1) & 1u, &s_fail))) {
@@ -497,6 +517,9 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
       const int nr = min(HX_R, a.nrot - r0);
       const TilePlan p = load_plan(a.rec + r0);
       if (p.steps == 0) continue;
+      // the rotation's window, loaded before the wait for the accumulators
+      const RotRec* rec = a.rec + r0 + min(rl, nr - 1);
+      const int Wr = (rl < nr && rec->valid) ? rec->W[0] : 0;
       const int d = u & 1;
       if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_tfull[d]), (uint32_t)(u >> 1) & 1u, &s_fail))) {
         if (lane == 0) s_fail = 1;
@@ -504,8 +527,6 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int nt = tile_n(p.wmax);
-      const RotRec* rec = a.rec + r0 + min(rl, nr - 1);
-      const int Wr = (rl < nr && rec->valid) ? rec->W[0] : 0;
       float4* rowp = reinterpret_cast<float4*>(a.B + (size_t)(r0 + min(rl, nr - 1)) * N * NCOL);
       const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)d * DSET;
       for (int x0 = 0; x0 < nt; x0 += 16) {
@@ -626,9 +647,9 @@ bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out,
     const bool two = 2 * 2 * cols * n <= 256;
     for (int pass = two ? 0 : 1; pass < 2; ++pass) {
       const size_t cap = (pass == 0 ? kSmemHalf : kSmemCap) - 1024;
-      for (int ks : {2, 1}) {
-        if (ks_pref && ks != ks_pref) continue;
-        if (ks == 2 && jc < 2 && !ks_pref) continue;
+      // automatic: 2 K-steps per stage where the box has several (else 1)
+      for (int ks : {4, 3, 2, 1}) {
+        if (ks_pref ? ks != ks_pref : (ks > 2 || (ks == 2 && jc < 2))) continue;
         const HxLayout L = hx_layout(n, K, cols, f16, G, ks);
         if (cap <= L.op) continue;
         int nb = (int)std::min<size_t>(HX_MAXSTAGES, (cap - L.op) / L.stage);

@@ -69,8 +69,8 @@ typedef struct cdk_opts {
                           tensor-core x pass (by default they are grouped by the ligand-box
                           chunks their channels reach, which changes no result);
                           [5] Hankel x pass shape: bits 0-1 columns per CTA (0 = automatic,
-                          1, or 2 at n <= 64), bits 2-3 K-steps per ring stage (0 = automatic,
-                          1 or 2);
+                          1, or 2 at n <= 64), bits 2-4 K-steps per ring stage (0 = automatic,
+                          1 to 4);
                           [6] precision forms: poses per wave re-scored in FP64
                           (cdk_ctx_top_poses): 0 = 8 (none in the FP32 form), -1 = none,
                           1..32; [7] = 1: no FP64 near-tie break of the argmin in the
