@@ -924,10 +924,16 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
 // stage 1, radix R1 over the 8 contiguous blocks of R1 digit-reversed positions (lane t holds
 // block t in registers); stage 2, radix 8 over the R1 groups {np + R1 j} with twiddles
 // tw[np k] (lane t takes groups np = t, t + 8, ...), giving natural index np + R1 j. The
-// exchange between the stages goes through the warp's own shared-memory slice (__syncwarp
-// only). Block-wide barriers: after the twiddle load, between the y and z passes (the y output
-// is the z input), and in the final reduction. Same radix stages, twiddles and packing as
-// k_yz_inv_argmin.
+// exchange between the two stages goes through the line's own storage in the plane buffer
+// (y: its kz column, rows at stride N/2+1; z: the two rows of its row pair, N + 2 slots), with
+// __syncwarp only. Stage-1 output m of block t sits at line position t R1 + (m + t) mod R1 --
+// block t rotated by t -- so the 8 lanes' stores of one m, and the 8 lanes' loads of one block
+// in stage 2, fall in 8 different banks (odd row stride). In the y pass stage 2 gathers both
+// of its groups before any lane writes the natural outputs back into the column. Block-wide
+// barriers: after the twiddle load, between the y and z passes (the y output is the z input),
+// and in the final reduction. Shared memory is the twiddles and the plane only (68 KB at
+// 128^3), so three CTAs of 288 threads (72 registers) fit an SM. Same radix stages, twiddles
+// and packing as k_yz_inv_argmin.
 // 288 threads = 36 octets: the 33 kz columns (and at most 32 row pairs) of a 64^3 plane in one
 // round each, 49 / 65 columns at 96^3 / 128^3 in two
 constexpr int kOctWarps = 9;
@@ -935,21 +941,19 @@ constexpr int kOctets = 4 * kOctWarps;
 
 template <int N>
 constexpr size_t octet_smem() {
-  // twiddles, Y[N][N/2+1], per warp 4 octets x 8 blocks x (R1 + 1)
-  return sizeof(float2) * (N + (size_t)N * (N / 2 + 1) + kOctWarps * 4 * 8 * (N / 8 + 1));
+  return sizeof(float2) * (N + (size_t)N * (N / 2 + 1));
 }
 
 template <int N, bool TOP2>
-__global__ void __launch_bounds__(32 * kOctWarps, (N <= 64 ? 4 : 2)) k_yz_octet(WaveArgs a) {
+__global__ void __launch_bounds__(32 * kOctWarps, 3) k_yz_octet(WaveArgs a) {
   constexpr int NZH = N / 2 + 1, NCOL = N * NZH;
   constexpr int R1 = N / 8;           // stage-1 radix; stage 2 is radix 8
-  constexpr int XS = R1 + 1;          // padded block stride of the exchange slice
   constexpr int NG = (R1 + 7) / 8;    // stage-2 groups per lane
   static_assert(N % 8 == 0 && (R1 == 4 || R1 == 8 || R1 == 12 || R1 == 16), "n = 8 R1");
+  static_assert(NZH % 2 == 1, "odd row stride");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* s_tw = reinterpret_cast<float2*>(smem_raw);
-  float2* s_y = s_tw + N;                    // y-transformed rows Y[y][kz]
-  float2* s_xall = s_y + (size_t)N * NZH;    // exchange slices
+  float2* s_y = s_tw + N;  // y-transformed rows Y[y][kz]
   __shared__ unsigned long long s_best[kOctWarps], s_best2[kOctWarps];
   const int x = blockIdx.x, r = blockIdx.y;
   const RotRec* rec = a.rec + r;
@@ -960,46 +964,45 @@ __global__ void __launch_bounds__(32 * kOctWarps, (N <= 64 ? 4 : 2)) k_yz_octet(
   const int o = lane >> 3, t = lane & 7, g = warp * 4 + o;
   for (int i = tid; i < N; i += 32 * kOctWarps) s_tw[i] = a.tw[i];
   const BPlane bp(a, r, x, N, NCOL);
-  float2* S = s_xall + (size_t)(warp * 4 + o) * 8 * XS;
   __syncthreads();
-  // the second stage of one line from the exchange slice: groups np = t + 8 q, natural output
-  // index np + R1 j -> emit(np, j, value)
-  auto stage2 = [&](auto&& emit) {
-#pragma unroll
-    for (int q = 0; q < NG; ++q) {
-      const int np = t + 8 * q;
-      if (np < R1) {
-        float2 u[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) u[j] = S[j * XS + np];
-#pragma unroll
-        for (int k = 1; k < 8; ++k) u[k] = c_mulc(u[k], s_tw[np * k]);
-        Radix<8, +1>::run(u);
-#pragma unroll
-        for (int j = 0; j < 8; ++j) emit(np, j, u[j]);
-      }
-    }
-  };
+  // line position of stage-1 output m of block blk
+  auto xpos = [](int blk, int m) { return blk * R1 + (m + blk) % R1; };
   // y: columns l = g, g + 36, ...; a warp stops when none of its octets has a column left
   constexpr int YR = (NZH + kOctets - 1) / kOctets;
 #pragma unroll 1
   for (int it = 0; it < YR; ++it) {
-    if (warp * 4 + kOctets * it >= NZH) break;
+    if (warp * 4 + kOctets * it >= NZH) break;  // warp-uniform
     const int l = g + kOctets * it;
     const bool act = l < NZH;
+    float2* col = s_y + (act ? l : 0);
     float2 v[R1];
 #pragma unroll
-    for (int j = 0; j < R1; ++j) {
-      v[j] = act ? bp.at((t * R1 + j) * NZH + l) : make_float2(0.f, 0.f);
-    }
+    for (int j = 0; j < R1; ++j) v[j] = act ? bp.at((t * R1 + j) * NZH + l) : make_float2(0.f, 0.f);
     Radix<R1, +1>::run(v);
+    if (act) {
 #pragma unroll
-    for (int j = 0; j < R1; ++j) S[t * XS + j] = v[j];
+      for (int j = 0; j < R1; ++j) col[xpos(t, j) * NZH] = v[j];
+    }
     __syncwarp();
-    stage2([&](int np, int j, float2 val) {
-      if (act) s_y[(np + R1 * j) * NZH + l] = val;
-    });
-    __syncwarp();
+    float2 u[NG][8];
+#pragma unroll
+    for (int q = 0; q < NG; ++q) {
+      const int np = t + 8 * q;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) u[q][j] = (act && np < R1) ? col[xpos(j, np) * NZH] : make_float2(0.f, 0.f);
+    }
+    __syncwarp();  // every group of the line gathered before any natural output is written
+#pragma unroll
+    for (int q = 0; q < NG; ++q) {
+      const int np = t + 8 * q;
+      if (act && np < R1) {
+#pragma unroll
+        for (int k = 1; k < 8; ++k) u[q][k] = c_mulc(u[q][k], s_tw[np * k]);
+        Radix<8, +1>::run(u[q]);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) col[(np + R1 * j) * NZH] = u[q][j];
+      }
+    }
   }
   __syncthreads();
   // z: rows (2p, 2p + 1) packed as one complex line, Hermitian extension over z
@@ -1012,13 +1015,16 @@ __global__ void __launch_bounds__(32 * kOctWarps, (N <= 64 ? 4 : 2)) k_yz_octet(
     if (warp * 4 + kOctets * it >= npairs) break;  // warp-uniform
     const int p = g + kOctets * it;
     const bool act = p < npairs;
-    const float2* A = s_y + (2 * min(p, N / 2 - 1)) * NZH;
-    const float2* Bv = A + NZH;
+    float2* rows = s_y + (size_t)(2 * (act ? p : 0)) * NZH;  // rows 2p, 2p + 1: N + 2 slots
+    const float2* A = rows;
+    const float2* Bv = rows + NZH;
     float2 v[R1];
 #pragma unroll
     for (int j = 0; j < R1; ++j) {
       const int k = t + 8 * j;  // natural frequency at digit-reversed position t R1 + j
-      if (j < R1 / 2) {
+      if (!act) {
+        v[j] = make_float2(0.f, 0.f);
+      } else if (j < R1 / 2) {
         const float2 ak = A[k], bk = Bv[k];
         v[j] = make_float2(ak.x - bk.y, ak.y + bk.x);
         if (j == 0 && t == 0) v[j] = make_float2(ak.x, bk.x);  // k = 0
@@ -1029,28 +1035,43 @@ __global__ void __launch_bounds__(32 * kOctWarps, (N <= 64 ? 4 : 2)) k_yz_octet(
         if (j == R1 / 2 && t == 0) v[j] = make_float2(am.x, bm.x);  // k = N/2
       }
     }
+    __syncwarp();  // the octet has read its rows: their slots become the exchange
     Radix<R1, +1>::run(v);
+    if (act) {
 #pragma unroll
-    for (int j = 0; j < R1; ++j) S[t * XS + j] = v[j];
+      for (int j = 0; j < R1; ++j) rows[xpos(t, j)] = v[j];
+    }
     __syncwarp();
     const int y0 = 2 * p;
     const bool row0 = act && y0 < Wy, row1 = act && y0 + 1 < Wy;
-    stage2([&](int np, int j, float2 val) {
-      const int z = np + R1 * j;
-      if (z < Wz) {
-        const unsigned int lin0 = (unsigned int)((x * N + y0) * N + z);
-        const unsigned long long k0 = ((unsigned long long)order_key(val.x * inv) << 32) | lin0;
-        const unsigned long long k1 = ((unsigned long long)order_key(val.y * inv) << 32) | (lin0 + N);
-        if constexpr (TOP2) {
-          if (row0) top2_insert(k0, best, best2);
-          if (row1) top2_insert(k1, best, best2);
-        } else {
-          if (row0) best = k0 < best ? k0 : best;
-          if (row1) best = k1 < best ? k1 : best;
+#pragma unroll
+    for (int q = 0; q < NG; ++q) {
+      const int np = t + 8 * q;
+      if (act && np < R1) {
+        float2 u[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) u[j] = rows[xpos(j, np)];
+#pragma unroll
+        for (int k = 1; k < 8; ++k) u[k] = c_mulc(u[k], s_tw[np * k]);
+        Radix<8, +1>::run(u);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int z = np + R1 * j;
+          if (z < Wz) {
+            const unsigned int lin0 = (unsigned int)((x * N + y0) * N + z);
+            const unsigned long long k0 = ((unsigned long long)order_key(u[j].x * inv) << 32) | lin0;
+            const unsigned long long k1 = ((unsigned long long)order_key(u[j].y * inv) << 32) | (lin0 + N);
+            if constexpr (TOP2) {
+              if (row0) top2_insert(k0, best, best2);
+              if (row1) top2_insert(k1, best, best2);
+            } else {
+              if (row0) best = k0 < best ? k0 : best;
+              if (row1) best = k1 < best ? k1 : best;
+            }
+          }
         }
       }
-    });
-    __syncwarp();
+    }
   }
   for (int off = 16; off > 0; off >>= 1) {
     const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, off);
@@ -1366,9 +1387,9 @@ cudaError_t launch_spread_yz_t(const WaveArgs& a, cudaStream_t s) {
 
 template <int N>
 cudaError_t launch_yz_inv_t(const WaveArgs& a, cudaStream_t s) {
-  // octet kernel at n >= 96 (measured 1.9x faster at 128^3); block stages at n <= 64 (the
-  // packed rows alias the plane there, 8 CTAs per SM: 1.6x faster than the octets at 64^3);
-  // yz_block_stages: 1 forces block stages, 2 forces octets
+  // octet kernel at n >= 96 (measured 2.1x faster than block stages at 128^3, 1.05x at 96^3);
+  // block stages at n <= 64 (the packed rows alias the plane there, 8 CTAs per SM: 1.6x faster
+  // than the octets at 64^3); yz_block_stages: 1 forces block stages, 2 forces octets
   const bool octet = a.yz_block_stages == 2 || (a.yz_block_stages == 0 && N >= 96);
   if (octet) {
     constexpr size_t sm = octet_smem<N>();

@@ -182,9 +182,8 @@ def test_yz_octet_kernel_matches_block_stages(grids_cache, form, name, nq):
     translations agree (bit for bit where the compiler keeps the same operation order)."""
     w = synth.make_workload(name, seed=3, n_conf=2, n_q=nq, grids_cache=grids_cache)
     out = []
-    for block in (False, True):
-        with Receptor(w.grids, w.spacing, form=form, yz_block_stages=block,
-                      yz_octets=not block) as rec:
+    for kw in ({"yz_octets": True}, {"yz_block_stages": True}):
+        with Receptor(w.grids, w.spacing, form=form, **kw) as rec:
             out.append(rec.search(w.coor, w.charge, w.eps, w.slot, w.quats))
     (e0, i0), (e1, i1) = out
     assert np.abs(e0.astype(np.float64) - e1).max() <= 1e-6 * np.abs(e1).max()
