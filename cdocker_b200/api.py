@@ -137,7 +137,8 @@ class Receptor:
                  group_rotations: bool = True, tc_stream_tiles: bool = False,
                  tc_hankel: bool = False,
                  tc_cols: int = 0, top_k: int = 0, tie_break: bool = True,
-                 yz_block_stages: bool = False, yz_octets: bool = False, tc_ksteps: int = 0):
+                 yz_block_stages: bool = False, yz_octets: bool = False, tc_ksteps: int = 0,
+                 tc_thread_copies: bool = False, tc_tiled_rows: bool = False):
         g = _f32(grids)
         if g.ndim != 4:
             raise ValueError("grids must be [K, n, n, n]")
@@ -158,7 +159,8 @@ class Receptor:
         opts.reserved[2] = 1 if autotune else 0
         opts.reserved[3] = (1 if tc_mma_sync else 2 if tc_build else 3 if tc_stream_tiles
                             else 4 if tc_hankel else 0)
-        opts.reserved[5] = (tc_cols & 3) | ((tc_ksteps & 7) << 2)
+        opts.reserved[5] = ((tc_cols & 3) | ((tc_ksteps & 7) << 2) |
+                            (32 if tc_thread_copies else 0) | (64 if tc_tiled_rows else 0))
         opts.reserved[6] = top_k
         opts.reserved[7] = 0 if tie_break else 1
         opts.reserved[4] = 0 if group_rotations else 1

@@ -301,7 +301,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   // other sizes; 3 forces streamed tiles, 4 the Hankel kernel
   const int variant = c->opts.reserved[3];
   const bool can_stream = tc && stream_supported(n, Lb) && direct_planes(probe);
-  const bool streamed = can_stream && (variant == 3 || variant == 0);
+  const bool streamed = can_stream && use_stream_tiles(variant, f16form);
   HankelPlan hp{};
   const bool hankel = tc && !streamed && (variant == 0 || variant == 4) && direct_planes(probe) &&
                       hankel_plan(n, K, Lb, f16form, c->opts.reserved[5] & 3, &hp, 0, (c->opts.reserved[5] >> 2) & 7);
@@ -327,6 +327,8 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     return CDK_ERR_UNSUPPORTED;
   }
   const bool f16 = f16form && rows;
+  // the Hankel x pass loads tiled ligand rows by bulk copies, or untiled rows by per-thread copies
+  const bool tiled = hankel && hankel_tiled(c->opts.reserved[5], f16form);
   const size_t lop_per = rows ? stream_lop_bytes_per_rotation(n, K, f16) : 0;
   int wave = c->opts.wave_rotations;
   if (wave <= 0) {
@@ -350,7 +352,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   const int topk = c->opts.reserved[6] < 0 ? 0 : c->opts.reserved[6] > 0 ? std::min(c->opts.reserved[6], (int)kTopMax)
                                                                         : (tc ? 8 : 0);
   const size_t b_keys2 = tiebreak ? align_up((size_t)wave * n * 2 * sizeof(unsigned long long)) : 0;
-  const size_t b_A = align_up(rows ? (size_t)((wave + 7) & ~7) * lop_per
+  const size_t b_A = align_up(rows ? lop_wave_bytes(wave, tiled, lop_per)
                                    : (size_t)wave * K * Lb * ncol * sizeof(float2));
   const size_t b_B = align_up((size_t)wave * n * ncol * sizeof(float2));
   if (!grow(c->wave, b_rotxyz + b_rec + b_keys + b_A + b_B + b_keys2)) {
@@ -374,6 +376,8 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   a.keys = reinterpret_cast<unsigned long long*>(base + b_rotxyz + b_rec);
   a.A = rows ? nullptr : reinterpret_cast<float2*>(base + b_rotxyz + b_rec + b_keys);
   a.lop = rows ? reinterpret_cast<unsigned char*>(base + b_rotxyz + b_rec + b_keys) : nullptr;
+  a.lop_tiled = tiled ? 1 : 0;
+  a.lop_bstride = lop_block_stride();
   a.B = reinterpret_cast<float2*>(base + b_rotxyz + b_rec + b_keys + b_A);
   a.keys2 = tiebreak ? reinterpret_cast<unsigned long long*>(base + b_rotxyz + b_rec + b_keys + b_A + b_B) : nullptr;
   a.phat = c->d_phat;
@@ -678,6 +682,7 @@ bool ctx_view(const cdk_ctx* c, CtxView* v) {
   v->stream = c->stream;
   v->form = c->opts.form;
   v->tc_variant = c->opts.reserved[3];
+  v->hx_shape = c->opts.reserved[5];
   v->top = c->d_top;
   v->ptilde = c->d_ptilde;
   v->grids = c->d_grids;

@@ -99,11 +99,47 @@ struct WaveArgs {
                              // and channel: [chunk][re, im]) of the planes times lscale[k]
   float lscale[KMAX];        // split-FP16 form: 2^sigma_k per channel (a power of two, exact)
   int* range_err;            // split-FP16 form: set when a scaled ligand value left the FP16 range
-  unsigned char* lop;        // when set (n = 64, direct planes): the plane kernel writes the
-                             // ligand as split-BF16 x-chunk rows here instead of A:
-                             // [nrot/8][K][hi/lo][chunk j < 4][re/im][ncol/4][nrot%8][ncol%4]
-                             // x 16 B (8 planes; nrot rounded up to a multiple of 8)
+  unsigned char* lop;        // when set (direct planes): the plane kernel writes the ligand as
+                             // split-BF16 or FP16 x-chunk rows here instead of A, in one of
+                             // two layouts (lop_tiled)
+  int lop_tiled;             // 0: [nrot/8][K][hi/lo][chunk j < 4][re/im][ncol/4][nrot%8][ncol%4]
+                             //    x 16 B of 8 planes (nrot rounded up to a multiple of 8), the
+                             //    streamed-tile x pass's rows;
+                             // 1: 128-rotation tiles [nrot/128][K][chunk j < 4][ncol][hi/lo]
+                             //    of 4 KB blocks (lop_bstride bytes apart) in the tensor cores'
+                             //    K-major layout with 32-byte
+                             //    swizzle (rotation m of the tile at 32 m: its re and im planes,
+                             //    16 B each, the halves exchanged where m & 4), one bulk copy
+                             //    per K-step for the Hankel x pass; chunks of the tile's stage
+                             //    plan that a valid rotation does not touch hold zeros (the
+                             //    plane kernel runs after k_tile_plan)
+  int plane_rot_major;       // set by the plane kernel's launcher: grid (nrot, K) instead of
+                             // (K, nrot)
+  int lop_bstride;           // tiled rows: bytes from one 4 KB block to the next (>= 4096)
 };
+// rotations per tensor-core tile (the MMA's M), and the 4 KB block of one (tile, channel, chunk,
+// part, column) in the tiled ligand-row layout
+constexpr int kTileRot = 128;
+constexpr size_t kLopBlock = 4096;
+// rotations a wave's ligand rows are allocated for
+inline size_t lop_rotations(long nrot, bool tiled) {
+  return tiled ? (size_t)((nrot + kTileRot - 1) / kTileRot) * kTileRot : (size_t)((nrot + 7) & ~7L);
+}
+// The automatic tensor-core x pass at n = 64 (variant: opts.reserved[3]): streamed operator tiles
+// in the split-BF16 form, the Hankel kernel (over tiled rows) in the split-FP16 form
+inline bool use_stream_tiles(int variant, bool f16form) { return variant == 3 || (variant == 0 && !f16form); }
+// The Hankel x pass loads tiled rows by bulk copies in the split-FP16 form (opts.reserved[5] bit 6:
+// in the split-BF16 form too, whose plane kernel then writes its two parts as 32-byte pieces more
+// slowly than the untiled rows; bit 5: never)
+inline bool hankel_tiled(int reserved5, bool f16form) { return !(reserved5 & 32) && (f16form || (reserved5 & 64)); }
+// tiled rows: the stride of their 4 KB blocks (a pad after each block spreads the plane
+// kernel's 32-byte stores of neighbouring columns over more DRAM banks)
+int lop_block_stride();
+// bytes of a wave's ligand rows: per-rotation bytes scaled by the block stride when tiled
+inline size_t lop_wave_bytes(long nrot, bool tiled, size_t per_rotation) {
+  return tiled ? lop_rotations(nrot, true) * (per_rotation / kLopBlock) * (size_t)lop_block_stride()
+               : lop_rotations(nrot, false) * per_rotation;
+}
 
 // Launchers (stream-ordered, no synchronisation). Return cudaError_t of the launch.
 cudaError_t launch_prep(const WaveArgs& a, cudaStream_t s);
@@ -217,6 +253,7 @@ struct CtxView {
   cudaStream_t stream;
   int form;              // CDK_FORM_*
   int tc_variant;        // opts.reserved[3]
+  int hx_shape;          // opts.reserved[5]
   const void* top;       // operator image of the streamed tensor-core x pass (or null)
   const float2* ptilde;  // precision forms: P~ [ncol][K][n], the Hankel x pass's operator source
   const float* grids;    // receptor grids [K][n][n][n] (FP64 re-scores)

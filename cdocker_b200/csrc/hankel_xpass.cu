@@ -70,6 +70,17 @@ __device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint
   return d;
 }
 
+// shared-memory matrix descriptor: K-major with 32-byte swizzle (rows of 32 bytes = one K-step
+// of 16 values, 8-row atoms of 256 bytes; SBO: M/N stride of the atoms; LBO unused: 1)
+__device__ __forceinline__ uint64_t make_desc_sw32(uint32_t saddr, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)6 << 61;  // layout type 6: 32-byte swizzle
+  return d;
+}
+
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const volatile int* stop) {
   for (long i = 0; i < kWaitLimit; ++i) {
     uint32_t done;
@@ -193,6 +204,7 @@ __device__ __forceinline__ uint32_t make_idesc(int n) {
 struct HxLayout {
   uint32_t S;         // one Hankel buffer: G groups x 128 B
   uint32_t op;        // the column operator: COLS x K x (hi, lo) x 3 buffers
+  uint32_t ring;      // offset of the ring: op rounded up to 1 KB (swizzled tiles stay aligned)
   uint32_t ksub;      // one K-step of a stage: COLS x LPARTS x 4 KB
   uint32_t stage;     // one ring stage: ks K-steps
   uint32_t build;     // scratch of the operator build (inside the ring area)
@@ -202,6 +214,7 @@ __host__ __device__ inline HxLayout hx_layout(int n, int K, int cols, bool f16, 
   HxLayout L;
   L.S = (uint32_t)G * HX_CORE;
   L.op = (uint32_t)cols * K * 2 * 3 * L.S;
+  L.ring = (L.op + 1023u) & ~1023u;
   L.ksub = (uint32_t)cols * (f16 ? 1 : 2) * HX_TILE;
   L.stage = (uint32_t)ks * L.ksub;
   // P~ of the CTA's columns (float2) + their four split arrays (re hi, re lo, im hi, im lo),
@@ -232,14 +245,16 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
   const int K = a.K;
   const HxLayout L = hx_layout(N, K, COLS, F16, G, ks);
   unsigned char* op = base;              // resident operator
-  unsigned char* ring = base + L.op;     // ring stages (the operator build uses it first)
+  unsigned char* ring = base + L.ring;   // ring stages (the operator build uses it first)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int c0 = blockIdx.x * COLS;
   const int ntiles = (a.nrot + HX_R - 1) / HX_R;
 
   if (tid == 0) {
     for (int b = 0; b < nb; ++b) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_full[b])), "r"(HX_PRODUCERS));
+      // full: one cp.async arrival per producer thread, or (tiled rows) the one expect_tx arrival
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_full[b])),
+                   "r"(a.lop_tiled ? 1 : HX_PRODUCERS));
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_empty[b])));
     }
     for (int d = 0; d < 2; ++d) {
@@ -314,7 +329,63 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
   const uint32_t ring_s = smem_u32(ring);
   const uint32_t op_s = smem_u32(op);
 
-  if (warp < HX_PRODUCERS / 32) {
+  if (warp < HX_PRODUCERS / 32 && a.lop_tiled) {
+    // ---- producer, tiled rows: one thread issues every stage as bulk copies of whole 4 KB
+    // blocks (128 rotations x one K-step of one column and part, already in the swizzled
+    // K-major layout, untouched chunks already zero); the copies complete on the stage's full
+    // barrier by their byte count, in the async proxy the tensor cores read
+    if (tid == 0) {
+      const size_t bst = (size_t)a.lop_bstride;
+      const size_t tile_bytes = (size_t)K * 4 * NCOL * LPARTS * bst;
+      int s = 0, b = 0;
+      uint32_t round = 0;
+      bool ok = true;
+      for (int t = 0; t < ntiles && ok; ++t) {
+        const TilePlan p = load_plan(a.rec + t * HX_R);
+        if (p.steps == 0) continue;
+        const unsigned char* tb = a.lop + (size_t)t * tile_bytes;
+        for (int ai = 0; ai < p.nact && ok; ++ai) {
+          const int k = (int)((p.pk >> (4 * ai)) & 15);
+          const int jlo = (int)((p.pl >> (4 * ai)) & 15), jhi = (int)((p.ph >> (4 * ai)) & 15);
+          for (int j0 = jlo; j0 <= jhi; j0 += ks, ++s) {
+            if (s >= nb && !mbar_wait(smem_u32(&s_empty[b]), (round - 1) & 1u, &s_fail)) {
+              s_fail = 1;
+              ok = false;
+              break;
+            }
+            const uint32_t st = ring_s + (uint32_t)b * L.stage;
+            const uint32_t full = smem_u32(&s_full[b]);
+            const int jn = min(ks, jhi + 1 - j0);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(
+                             (uint32_t)(jn * COLS * LPARTS) * (uint32_t)kLopBlock),
+                         "r"(full)
+                         : "memory");
+            for (int jj = 0; jj < jn; ++jj)
+#pragma unroll
+              for (int cc = 0; cc < COLS; ++cc)
+#pragma unroll
+                for (int hl = 0; hl < LPARTS; ++hl) {
+                  const unsigned char* src =
+                      tb + ((((size_t)k * 4 + (j0 + jj)) * NCOL + c0 + cc) * LPARTS + hl) * bst;
+                  const uint32_t dst = st + (uint32_t)jj * L.ksub + (uint32_t)(cc * LPARTS + hl) * HX_TILE;
+                  asm volatile(
+                      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                      "l"(src), "r"((uint32_t)kLopBlock), "r"(full)
+                      : "memory");
+                }
+            if (++b == nb) {
+              b = 0;
+              ++round;
+            }
+          }
+        }
+      }
+      // every copy issued has landed before the CTA can leave (the last use of each ring slot;
+      // earlier uses were consumed before their slot was reissued)
+      for (int i = max(0, s - nb); i < s; ++i)
+        if (!mbar_wait(smem_u32(&s_full[i % nb]), (uint32_t)(i / nb) & 1u, nullptr)) s_fail = 1;
+    }
+  } else if (warp < HX_PRODUCERS / 32) {
     // ---- producers
     const int rr = tid;
     const uint32_t row_s = (uint32_t)(rr >> 3) * HX_CORE + (uint32_t)(rr & 7) * 16;
@@ -414,7 +485,10 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
     // start-address field (bits 0-13) holds the byte address >> 4, so moving a descriptor by a
     // 16-byte aligned byte offset adds offset >> 4 (shared addresses stay below 256 KB: no carry
     // out of the field).
-    const uint64_t dring = make_desc(ring_s, HX_TILE / 2, HX_CORE);  // ligand rows, slot 0
+    // ligand rows, slot 0: per-thread copies in the no-swizzle layout (re | im core matrices
+    // one half-tile apart), or tiled rows in the 32-byte swizzled layout (re | im in each row)
+    const bool tiled = a.lop_tiled != 0;
+    const uint64_t dring = tiled ? make_desc_sw32(ring_s, 256) : make_desc(ring_s, HX_TILE / 2, HX_CORE);
     const uint64_t dop = make_desc(op_s, L.S, HX_CORE);              // operator, group 0
     const uint64_t sS = L.S >> 4;
     int s = 0, u = 0, b = 0;
@@ -447,8 +521,9 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
             good = false;
             break;
           }
-          // the producers' cp.async writes (generic proxy) reach the tensor core (async proxy)
-          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          // the producers' cp.async writes (generic proxy) reach the tensor core (async proxy);
+          // bulk copies (tiled rows) write in the async proxy already
+          if (!tiled) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const int jn = min(ks, jhi + 1 - j0);
           const uint64_t aslot = dring + (uint64_t)((b * L.stage) >> 4);
@@ -651,8 +726,8 @@ bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out,
       for (int ks : {4, 3, 2, 1}) {
         if (ks_pref ? ks != ks_pref : (ks > 2 || (ks == 2 && jc < 2))) continue;
         const HxLayout L = hx_layout(n, K, cols, f16, G, ks);
-        if (cap <= L.op) continue;
-        int nb = (int)std::min<size_t>(HX_MAXSTAGES, (cap - L.op) / L.stage);
+        if (cap <= L.ring) continue;
+        int nb = (int)std::min<size_t>(HX_MAXSTAGES, (cap - L.ring) / L.stage);
         if (nb < 2 || nb * ks < (pass == 0 ? 8 : 4) || (size_t)nb * L.stage < L.build) continue;
         if (nb_cap > 0 && nb_cap < nb && (size_t)nb_cap * L.stage >= L.build && nb_cap >= 2) nb = nb_cap;
         out->cols = cols;
@@ -660,7 +735,7 @@ bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out,
         out->jc = jc;
         out->nb = nb;
         out->ks = ks;
-        out->smem = (size_t)L.op + (size_t)nb * L.stage + 1024;
+        out->smem = (size_t)L.ring + (size_t)nb * L.stage + 1024;
         // a CTA that takes all 512 tensor-memory columns must have its SM alone: its shared
         // memory then keeps a second CTA out (tcgen05.alloc would otherwise stall it)
         if (pass == 1) out->smem = std::max(out->smem, (size_t)120 * 1024);
@@ -693,11 +768,15 @@ cudaError_t launch_xpass_hankel(const WaveArgs& a, const float2* pt, const float
   if (!a.lop || !pt || a.K > KMAX) return cudaErrorInvalidValue;
   // the B layout must be the plan's (the inverse (y,z) pass reads what this pass writes)
   if ((a.bcol != 0) != (p.cols == 1) || (a.bcol && a.bgroup != 2 && a.bgroup != 4)) return cudaErrorInvalidValue;
+  if (a.lop_tiled && (a.lop_bstride < (int)kLopBlock || a.lop_bstride % 128)) return cudaErrorInvalidValue;
   HxScale sc{};
   for (int k = 0; k < a.K; ++k) sc.s[k] = (a.f16 && f16_scale) ? f16_scale[k] : 1.f;
-  // the stage plan of every 128-rotation tile (channels, K-steps, largest window)
-  cudaError_t e = launch_tile_plan(a, p.jc, s);
-  if (e != cudaSuccess) return e;
+  // the stage plan of every 128-rotation tile (channels, K-steps, largest window); with tiled
+  // rows the plane kernel's launch has computed it already (its zero fill follows the plan)
+  if (!a.lop_tiled) {
+    cudaError_t e = launch_tile_plan(a, p.jc, s);
+    if (e != cudaSuccess) return e;
+  }
 #define CDK_HX(NN)                                                                               \
   case NN:                                                                                       \
     if (a.f16) return p.cols == 2 ? launch_hx<NN, (NN <= 64 ? 2 : 1), true>(a, pt, sc, p.jc, p.G, p.nb, p.ks, p.smem, s) \

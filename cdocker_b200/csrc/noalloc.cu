@@ -19,8 +19,8 @@
 //    device, with that device current, looks the address up with cudaGetSymbolAddress and
 //    caches it for the life of the process. The cache does not survive cudaDeviceReset (or
 //    any teardown of the device's primary context): do not call this entry point after one.
-//  * The call synchronises its stream twice (to read back the ligand-box plan and, at the
-//    end, the overflow count), so it cannot be recorded into a CUDA graph.
+//  * The call synchronises its stream twice: to read back the ligand-box plan and, at the
+//    end, the overflow count.
 //  * All calls share the array and it keeps the previous call's contents. The counters the
 //    search relies on are cleared at the start of every call; everything else is written
 //    before it is read. Calls that overlap on the GPU (two streams, two host threads) race on

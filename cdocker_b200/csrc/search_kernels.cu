@@ -22,6 +22,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstdlib>
+
 #include "cdk_internal.h"
 #include "fft.cuh"
 
@@ -36,6 +38,26 @@ __device__ __forceinline__ void split_bf16x2(float a, float b, uint32_t& hi, uin
   const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
   hi = *reinterpret_cast<const uint32_t*>(&h);
   lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
+// one 32-byte store (p 32-byte aligned): words w0..w3 then w4..w7
+__device__ __forceinline__ void st_v8u(void* p, uint4 lo, uint4 hi) {
+  asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"(lo.x), "r"(lo.y),
+               "r"(lo.z), "r"(lo.w), "r"(hi.x), "r"(hi.y), "r"(hi.z), "r"(hi.w)
+               : "memory");
+}
+
+// Tiled ligand rows (WaveArgs.lop_tiled): the 32-byte row of rotation r in the 4 KB block of
+// (tile r / 128, channel k, chunk jc, column c, part hl); re and im planes exchanged where
+// r & 4 (the tensor cores' 32-byte swizzle XORs address bit 4 with bit 7)
+__device__ __forceinline__ void tiled_row_store(const WaveArgs& a, int r, int k, int jc, int hl, int c, uint4 re,
+                                                uint4 im) {
+  const int lp = a.f16 ? 1 : 2;
+  const int ncol = a.n * (a.n / 2 + 1);
+  const size_t blk = ((((size_t)(r / kTileRot) * a.K + k) * 4 + jc) * ncol + c) * lp + hl;
+  uint4* dst = reinterpret_cast<uint4*>(a.lop + blk * (size_t)a.lop_bstride) + (size_t)(r % kTileRot) * 2;
+  if (r & 4) st_v8u(dst, im, re);
+  else st_v8u(dst, re, im);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -328,6 +350,10 @@ __device__ __forceinline__ void plane_chunk_write(const WaveArgs& a, int r, int 
       hr[d / 2] = *reinterpret_cast<const uint32_t*>(&pr);
       hi[d / 2] = *reinterpret_cast<const uint32_t*>(&pi);
     }
+    if (a.lop_tiled) {
+      tiled_row_store(a, r, k, jc, 0, c, make_uint4(hr[0], hr[1], hr[2], hr[3]), make_uint4(hi[0], hi[1], hi[2], hi[3]));
+      return;
+    }
     uint4* dst = reinterpret_cast<uint4*>(a.lop) +
                  (((size_t)(r >> 3) * a.K + k) * 8 * (NCOL / 4) + (c >> 2)) * 32 + (r & 7) * 4 + (c & 3);
     constexpr size_t RS = (size_t)(NCOL / 4) * 32;  // one row
@@ -343,6 +369,11 @@ __device__ __forceinline__ void plane_chunk_write(const WaveArgs& a, int r, int 
       split_bf16x2(ax[d], ax[d + 1], rh[d / 2], rl[d / 2]);
       split_bf16x2(ay[d], ay[d + 1], ih[d / 2], il[d / 2]);
     }
+    if (a.lop_tiled) {
+      tiled_row_store(a, r, k, jc, 0, c, make_uint4(rh[0], rh[1], rh[2], rh[3]), make_uint4(ih[0], ih[1], ih[2], ih[3]));
+      tiled_row_store(a, r, k, jc, 1, c, make_uint4(rl[0], rl[1], rl[2], rl[3]), make_uint4(il[0], il[1], il[2], il[3]));
+      return;
+    }
     uint4* dst = reinterpret_cast<uint4*>(a.lop) +
                  (((size_t)(r >> 3) * a.K + k) * 16 * (NCOL / 4) + (c >> 2)) * 32 + (r & 7) * 4 + (c & 3);
     constexpr size_t RS = (size_t)(NCOL / 4) * 32;  // one row
@@ -351,6 +382,52 @@ __device__ __forceinline__ void plane_chunk_write(const WaveArgs& a, int r, int 
     dst[((1 * 4 + jc) * 2 + 0) * RS] = make_uint4(rl[0], rl[1], rl[2], rl[3]);
     dst[((1 * 4 + jc) * 2 + 1) * RS] = make_uint4(il[0], il[1], il[2], il[3]);
   }
+}
+
+// Tiled rows: zeros for a chunk of the tile's stage plan that this rotation's channel does not
+// touch (the bulk copies of the x pass load whole 128-rotation blocks)
+__device__ __forceinline__ void tiled_zero_chunk(const WaveArgs& a, int r, int k, int jc, int c) {
+  const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+  tiled_row_store(a, r, k, jc, 0, c, z, z);
+  if (!a.f16) tiled_row_store(a, r, k, jc, 1, c, z, z);
+}
+
+// The K-step range [lo, hi] of channel k in the stage plan of rotation r's tile (k_tile_plan);
+// lo > hi when no rotation of the tile touches the channel
+__device__ __forceinline__ void tile_plan_range(const WaveArgs& a, int r, int k, int& lo, int& hi) {
+  const unsigned long long* tp = a.rec[r - r % kTileRot].tplan;
+  const unsigned long long pk = tp[0], pl = tp[1], ph = tp[2];
+  const int nact = (int)(tp[3] & 0xFFFFu);
+  lo = 15;
+  hi = -1;
+  for (int ai = 0; ai < nact; ++ai)
+    if ((int)((pk >> (4 * ai)) & 15) == k) {
+      lo = (int)((pl >> (4 * ai)) & 15);
+      hi = (int)((ph >> (4 * ai)) & 15);
+    }
+}
+
+// plane kernel CTA order for tiled rows: rotation-major by default; the environment variable
+// CDK_PLANE_ORDER=1 keeps the channel-major order, for measurement
+}  // namespace
+
+int lop_block_stride() {
+  static const int v = [] {
+    const char* e = std::getenv("CDK_LOP_PAD");
+    const int pad = e ? std::atoi(e) : 0;
+    return (int)kLopBlock + ((pad >= 0 && pad <= 4096 && pad % 128 == 0) ? pad : 0);
+  }();
+  return v;
+}
+
+namespace {
+
+int plane_rot_major_host() {
+  static const int v = [] {
+    const char* e = std::getenv("CDK_PLANE_ORDER");
+    return (e && std::atoi(e) == 1) ? 0 : 1;
+  }();
+  return v;
 }
 
 constexpr int kPlaneColsPerThread = 2;  // columns per thread in the plane kernel
@@ -371,12 +448,22 @@ __global__ void __launch_bounds__(256, kPlaneColsPerThread == 1 ? 5 : 4) k_sprea
   int* s_atom = reinterpret_cast<int*>(s_rr + cap);               // [cap]
   __shared__ int s_cnt;
   __shared__ uint32_t s_cm[N / 8][3];  // per 8-plane chunk: the channel atoms touching it (bit j)
-  const int k = blockIdx.x, r = blockIdx.y;
+  // grid (K, nrot), or (nrot, K) for tiled rows: the CTAs in flight then write whole
+  // 128-rotation blocks of one channel together
+  const bool rot_major = LOP && a.plane_rot_major;
+  const int k = rot_major ? blockIdx.y : blockIdx.x, r = rot_major ? blockIdx.x : blockIdx.y;
   const RotRec* rec = a.rec + r;
   if (!rec->valid) return;
   const int xlo = rec->xlo[k], xhi = rec->xhi[k];
-  if (xlo > xhi) return;
   const int tid = threadIdx.x, nthr = blockDim.x;
+  // tiled rows: the chunks of the tile's plan outside this rotation's own range get zeros
+  int zlo = 15, zhi = -1;
+  if (LOP && a.lop_tiled) tile_plan_range(a, r, k, zlo, zhi);
+  if (xlo > xhi) {
+    for (int q = zlo; q <= zhi; ++q)
+      for (int c = tid; c < NCOL; c += nthr) tiled_zero_chunk(a, r, k, q, c);
+    return;
+  }
   for (int i = tid; i < N; i += nthr) tw[i] = a.tw[i];
   const RotDesc rd = a.rots[r];
   const ConfDesc cd = a.confs[rd.conf];
@@ -455,6 +542,11 @@ __global__ void __launch_bounds__(256, kPlaneColsPerThread == 1 ? 5 : 4) k_sprea
   // xi + 1, whose offsets in the chunk are the same for the whole CTA (a uniform switch).
   // CPT columns per thread (c, c + NCOL / CPT, ...): the atom visit (list walk, weights, the
   // offset switch) is shared by the columns, each column keeping its own accumulation order.
+  if (LOP && a.lop_tiled) {
+    for (int q = zlo; q <= zhi; ++q)
+      if (q < jc0 || q >= jc0 + njc)
+        for (int c = tid; c < NCOL; c += nthr) tiled_zero_chunk(a, r, k, q, c);
+  }
   constexpr int CPT = kPlaneColsPerThread;
   static_assert(NCOL % CPT == 0, "column split");
   static_assert(CPT != 2 || (NCOL / 2) % NZH == 0, "paired columns share kz");
@@ -1368,7 +1460,10 @@ cudaError_t launch_spread_yz_t(const WaveArgs& a, cudaStream_t s) {
     if (a.lop) {
       cudaError_t e = cudaFuncSetAttribute(k_spread_yz_direct<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       if (e != cudaSuccess) return e;
-      k_spread_yz_direct<N, true><<<dim3(a.K, a.nrot), 256, sm, s>>>(a, a.kyof, cap);
+      WaveArgs b = a;
+      b.plane_rot_major = (a.lop_tiled && plane_rot_major_host()) ? 1 : 0;
+      const dim3 grid = b.plane_rot_major ? dim3(a.nrot, a.K) : dim3(a.K, a.nrot);
+      k_spread_yz_direct<N, true><<<grid, 256, sm, s>>>(b, a.kyof, cap);
       return cudaGetLastError();
     }
     cudaError_t e = cudaFuncSetAttribute(k_spread_yz_direct<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -1628,6 +1723,12 @@ cudaError_t launch_prep(const WaveArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 cudaError_t launch_spread_yz(const WaveArgs& a, cudaStream_t s) {
+  if (a.lop_tiled) {
+    // the tiled rows zero-fill by the tiles' stage plans: k_tile_plan first
+    if (!a.lop || !direct_planes(a) || a.lop_bstride < (int)kLopBlock || a.lop_bstride % 128) return cudaErrorInvalidValue;
+    cudaError_t e = launch_tile_plan(a, (a.Lb + 7) / 8, s);
+    if (e != cudaSuccess) return e;
+  }
   CDK_DISPATCH_N(a.n, launch_spread_yz_t, a, s);
 }
 bool direct_planes(const WaveArgs& a) {

@@ -315,7 +315,8 @@ void worker_loop(cdk_server* s) {
   sc += up((size_t)W * sizeof(unsigned long long));
   a.A = reinterpret_cast<float2*>(sc);
   const bool f16 = s->streamed && s->v.form == CDK_FORM_FP16X2;
-  const size_t rows = s->streamed ? (size_t)((W + 7) & ~7) * stream_lop_bytes_per_rotation(n, K, f16) : 0;
+  // ligand rows of either layout (tiled rows round the wave up to whole 128-rotation tiles)
+  const size_t rows = s->streamed ? lop_wave_bytes(W, true, stream_lop_bytes_per_rotation(n, K, f16)) : 0;
   unsigned char* lop_base = reinterpret_cast<unsigned char*>(sc);
   sc += up(std::max((size_t)W * K * Lmax * ncol * sizeof(float2), rows));
   a.B = reinterpret_cast<float2*>(sc);
@@ -400,10 +401,14 @@ void worker_loop(cdk_server* s) {
     // the same x-pass choice as a plain search on the context (results alone and in the mix
     // stay identical): streamed tiles at 64^3 where they apply, the Hankel kernel elsewhere
     HankelPlan hp{};
-    const bool tile_wave = s->streamed && s->v.top != nullptr && stream_supported(n, lb) && direct_planes(a);
+    const bool tile_wave = s->streamed && s->v.top != nullptr && use_stream_tiles(s->v.tc_variant, f16) &&
+                           stream_supported(n, lb) && direct_planes(a);
     const bool tc_wave = tile_wave || (s->streamed && s->v.tc_variant != 3 && direct_planes(a) &&
                                        hankel_plan(n, K, lb, f16, 0, &hp));
     a.lop = tc_wave ? lop_base : nullptr;
+    // the Hankel x pass loads tiled rows (split-FP16) or untiled rows, as in a plain search
+    a.lop_tiled = (tc_wave && !tile_wave && hankel_tiled(s->v.hx_shape, f16)) ? 1 : 0;
+    a.lop_bstride = lop_block_stride();
     a.f16 = (tc_wave && f16) ? 1 : 0;
     a.bgroup = tc_wave ? stream_bgroup() : 1;
     a.bcol = 0;
@@ -491,7 +496,7 @@ int cdk_server_create(cdk_ctx* ctx, const cdk_server_opts* opts, cdk_server** ou
                 s->v.kyof != nullptr && s->v.ptilde != nullptr &&
                 (stream_supported(n, std::min(s->opts.max_box, 32)) ||
                  hankel_plan(n, K, std::min(s->opts.max_box, 32), s->v.form == CDK_FORM_FP16X2, 0, &probe));
-  if (s->streamed && s->v.tc_variant != 4 && stream_top_bytes(n, K) > 0) {
+  if (s->streamed && use_stream_tiles(s->v.tc_variant, s->v.form == CDK_FORM_FP16X2) && stream_top_bytes(n, K) > 0) {
     // 64^3: the streamed-tile kernel's operator image, built once per context
     const int rc = ctx_ensure_top(ctx);
     if (rc != CDK_OK) {
@@ -502,8 +507,8 @@ int cdk_server_create(cdk_ctx* ctx, const cdk_server_opts* opts, cdk_server** ou
   }
   for (int k = 0; k < KMAX; ++k) s->osc[k] = s->v.lscale[k] != 0.f ? 1.f / s->v.lscale[k] : 1.f;
   const size_t planes = (size_t)W * K * s->opts.max_box * ncol * sizeof(float2);
-  const size_t rows = s->streamed ? (size_t)((W + 7) & ~7) *
-                                        stream_lop_bytes_per_rotation(n, K, s->v.form == CDK_FORM_FP16X2)
+  const size_t rows = s->streamed ? lop_wave_bytes(W, true,
+                                                   stream_lop_bytes_per_rotation(n, K, s->v.form == CDK_FORM_FP16X2))
                                   : 0;
   const size_t scratch = up((size_t)W * s->opts.max_atoms * sizeof(float4)) +
                          up((size_t)W * sizeof(RotRec)) + up((size_t)W * 8) +

@@ -20,9 +20,9 @@ TILES = {CDK_FORM_BF16X3: "tcgen05_streamed", CDK_FORM_FP16X2: "tcgen05_streamed
 
 
 def auto_kind(n, form):
-    """The automatic tensor-core x pass: streamed operator tiles at 64^3, the Hankel kernel at
-    the other grid sizes."""
-    return TILES[form] if n == 64 else HANKEL[form]
+    """The automatic tensor-core x pass: in the split-BF16 form streamed operator tiles at 64^3,
+    otherwise the Hankel kernel (over tiled ligand rows in the split-FP16 form)."""
+    return TILES[form] if (n == 64 and form == CDK_FORM_BF16X3) else HANKEL[form]
 
 
 @pytest.mark.parametrize("form", [CDK_FORM_BF16X3, CDK_FORM_FP16X2])
@@ -103,6 +103,31 @@ def test_tensor_core_variants_agree(grids_cache, wave):
         eo, io = out[other]
         assert rel_err(es, eo).max() <= 1e-5
         assert np.mean(np.all(is_ == io, axis=1)) >= 0.99
+
+
+@pytest.mark.parametrize("form", [CDK_FORM_FP16X2, CDK_FORM_BF16X3])
+@pytest.mark.parametrize("name,n_conf,n_q,wave,cols", [("c1_64", 2, 150, 200, 1),
+                                                       ("c1_64", 3, 111, 0, 2),
+                                                       ("c4_128", 1, 70, 45, 1)])
+def test_tiled_rows_match_thread_copies(grids_cache, form, name, n_conf, n_q, wave, cols):
+    """The Hankel x pass loads its ligand rows either as 128-rotation tiles that the plane kernel
+    writes in the tensor cores' 32-byte swizzled layout (one bulk copy per K-step and column, the
+    default) or rotation by rotation with per-thread copies from the untiled rows. The MMAs see
+    the same operands either way, so results are bit-identical: ragged waves (partial tiles), one
+    and two columns per CTA, chunks of a tile's plan that a rotation does not touch (zeros written
+    by the plane kernel, zero-filled by the copies)."""
+    w = synth.make_workload(name, seed=17, n_conf=n_conf, n_q=n_q, grids_cache=grids_cache)
+    out = {}
+    for thread_copies in (False, True):
+        with Receptor(w.grids, w.spacing, form=form, wave_rotations=wave, tc_hankel=True,
+                      tc_cols=cols, tc_thread_copies=thread_copies) as rec:
+            out[thread_copies] = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
+            st = rec.stats()
+        assert st["xpass_kind"] == HANKEL[form] and st["col_tile"] == cols
+    (et, it), (ec, ic) = out[False], out[True]
+    assert np.isfinite(et).all()
+    assert np.array_equal(et.view(np.uint32), ec.view(np.uint32))
+    assert np.array_equal(it, ic)
 
 
 def test_streamed_falls_back_for_large_ligands(grids_cache):

@@ -1,7 +1,8 @@
 """cdk_search_device_noalloc: the search entry point for callers that cannot allocate.
 
-Callers that record the search into a CUDA graph, run it from a real-time loop, or own all
-device memory through a pool cannot let the library call cudaMalloc mid-search. This entry
+Callers that run the search from a real-time loop (cudaMalloc and cudaFree can synchronise
+the whole device), or that own all device memory through a pool, cannot let the library call
+cudaMalloc mid-search. This entry
 point takes the same device buffers as cdk_search_device and carves its scratch from a fixed
 64 MiB file-scope device array instead. The test calls it through the C-ABI twice in a row and
 checks both results against cdk_search_device (the existing entry point) on the same inputs.
