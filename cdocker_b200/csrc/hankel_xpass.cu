@@ -704,8 +704,8 @@ cudaError_t launch_hx(const WaveArgs& a, const float2* pt, const HxScale& sc, in
 }  // namespace
 
 // Shape of the x pass for (n, K, ligand box, form): columns per CTA, Hankel groups, ring stages
-// (each of ks K-steps) and dynamic shared memory. cols_pref: 0 = automatic, 1 or 2 = that many
-// columns (2 only where the operator of two columns fits); ks_pref: 0 = automatic (2 K-steps per
+// (each of ks K-steps) and dynamic shared memory. cols_pref: 0 = automatic (1), 1 or 2 = that
+// many columns (2 only where the operator of two columns fits); ks_pref: 0 = automatic (2 K-steps per
 // stage where the ligand box has several and the ring keeps as many K-steps in flight), 1 or 2.
 // Returns false when the operator and a minimal ring do not fit one CTA (large K at large n) or
 // the box exceeds 32 planes.
@@ -714,8 +714,9 @@ bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out,
     return false;
   const int jc = (Lb + 7) / 8;
   const int G = n / 8 + jc - 1;
-  for (int cols : {2, 1}) {
-    if (cols_pref && cols != cols_pref) continue;
+  // one column per CTA unless two are asked for (two measured 20-35 % slower at 64^3)
+  for (int cols : {1, 2}) {
+    if (cols_pref ? cols != cols_pref : cols != 1) continue;
     if (cols == 2 && n > 64) continue;  // the tensor memory of two double-buffered columns
     // two CTAs per SM when the tensor memory allows (<= 256 columns each) and the operator
     // leaves room for a ring of at least 8 K-steps; else one CTA with the largest ring
