@@ -225,7 +225,8 @@ __host__ __device__ inline HxLayout hx_layout(int n, int K, int cols, bool f16, 
 
 template <int N, int COLS, bool F16>
 __global__ void __launch_bounds__(HX_THREADS, 2)
-    k_xpass_hankel(WaveArgs a, const float2* __restrict__ pt, HxScale sc, int jc, int G, int nb, int ks) {
+    k_xpass_hankel(WaveArgs a, const float2* __restrict__ pt, HxScale sc, int jc, int G, int nb, int ks,
+                   int split) {
   constexpr int NCOL = N * (N / 2 + 1);
   constexpr int LPARTS = F16 ? 1 : 2;
   constexpr int NMAX = N;                          // TMEM columns of one output block (re or im)
@@ -247,8 +248,13 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
   unsigned char* op = base;              // resident operator
   unsigned char* ring = base + L.ring;   // ring stages (the operator build uses it first)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int c0 = blockIdx.x * COLS;
-  const int ntiles = (a.nrot + HX_R - 1) / HX_R;
+  // CTA = (column group, part): the wave's tiles split into `split` contiguous parts, so that
+  // the last round of CTAs is less ragged (each part builds its own operator)
+  const int c0 = (int)(blockIdx.x / split) * COLS;
+  const int part = (int)(blockIdx.x % split);
+  const int ntiles_all = (a.nrot + HX_R - 1) / HX_R;
+  const int tbeg = part * ntiles_all / split;
+  const int ntiles = (part + 1) * ntiles_all / split;  // one past the CTA's last tile
 
   if (tid == 0) {
     for (int b = 0; b < nb; ++b) {
@@ -340,7 +346,7 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
       int s = 0, b = 0;
       uint32_t round = 0;
       bool ok = true;
-      for (int t = 0; t < ntiles && ok; ++t) {
+      for (int t = tbeg; t < ntiles && ok; ++t) {
         const TilePlan p = load_plan(a.rec + t * HX_R);
         if (p.steps == 0) continue;
         const unsigned char* tb = a.lop + (size_t)t * tile_bytes;
@@ -411,8 +417,8 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
       for (int i = 0; i < 4; ++i) f.x[i] = xr[i];
     };
     Ahead nxt;
-    if (ntiles > 0) fetch(0, nxt);
-    for (int t = 0; t < ntiles; ++t) {
+    if (tbeg < ntiles) fetch(tbeg, nxt);
+    for (int t = tbeg; t < ntiles; ++t) {
       const Ahead cur = nxt;
       if (t + 1 < ntiles) fetch(t + 1, nxt);
       const int r0 = t * HX_R;
@@ -495,8 +501,8 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
     uint32_t round = 0;
     bool good = true;
     TilePlan pn{};  // the next tile's plan, loaded one tile ahead
-    if (ntiles > 0) pn = load_plan(a.rec);
-    for (int t = 0; t < ntiles && good; ++t) {
+    if (tbeg < ntiles) pn = load_plan(a.rec + tbeg * HX_R);
+    for (int t = tbeg; t < ntiles && good; ++t) {
       const TilePlan p = pn;
       if (t + 1 < ntiles) pn = load_plan(a.rec + (t + 1) * HX_R);
       if (p.steps == 0) continue;
@@ -587,7 +593,7 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
     const int gm = G2 - 1;
     const bool bcol = COLS == 1 && a.bcol != 0;
     int u = 0;
-    for (int t = 0; t < ntiles; ++t) {
+    for (int t = tbeg; t < ntiles; ++t) {
       const int r0 = t * HX_R;
       const int nr = min(HX_R, a.nrot - r0);
       const TilePlan p = load_plan(a.rec + r0);
@@ -688,16 +694,47 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
 constexpr size_t kSmemCap = 227 * 1024 - 1024;
 constexpr size_t kSmemHalf = 110 * 1024;  // per CTA when two share an SM
 
+// tile parts per column group: the smallest estimated time in rounds of CTAs over the device's
+// slots (S CTAs per column group, ceil(groups S / slots) rounds of 1/S of the work each), each
+// extra part charged 4 % for its operator build; never more parts than tiles
+static int hx_split(int groups, int ntiles, int ctas_per_sm) {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+      sms = 148;
+  }
+  if (const char* e = std::getenv("CDK_HX_SPLIT")) {
+    const int v = std::atoi(e);
+    if (v >= 1 && v <= 8) return std::max(1, std::min(v, ntiles));
+  }
+  const long slots = (long)sms * std::max(1, ctas_per_sm);
+  int best = 1;
+  double best_cost = 1e30;
+  for (int S = 1; S <= 4 && S <= std::max(1, ntiles); ++S) {
+    const double rounds = (double)((groups * (long)S + slots - 1) / slots);
+    const double cost = rounds / S * (1.0 + 0.04 * (S - 1));
+    if (cost < best_cost - 1e-9) {
+      best_cost = cost;
+      best = S;
+    }
+  }
+  return best;
+}
+
 template <int N, int COLS, bool F16>
 cudaError_t launch_hx(const WaveArgs& a, const float2* pt, const HxScale& sc, int jc, int G, int nb, int ks,
-                      size_t smem, cudaStream_t s) {
+                      size_t smem, int ctas_per_sm, cudaStream_t s) {
   constexpr int NCOL = N * (N / 2 + 1);
   auto kern = k_xpass_hankel<N, COLS, F16>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  kern<<<NCOL / COLS, HX_THREADS, smem, s>>>(a, pt, sc, jc, G, nb, ks);
+  const int groups = NCOL / COLS;
+  const int split = hx_split(groups, (a.nrot + HX_R - 1) / HX_R, ctas_per_sm);
+  kern<<<groups * split, HX_THREADS, smem, s>>>(a, pt, sc, jc, G, nb, ks, split);
   return cudaGetLastError();
 }
 
@@ -780,10 +817,10 @@ cudaError_t launch_xpass_hankel(const WaveArgs& a, const float2* pt, const float
   }
 #define CDK_HX(NN)                                                                               \
   case NN:                                                                                       \
-    if (a.f16) return p.cols == 2 ? launch_hx<NN, (NN <= 64 ? 2 : 1), true>(a, pt, sc, p.jc, p.G, p.nb, p.ks, p.smem, s) \
-                                  : launch_hx<NN, 1, true>(a, pt, sc, p.jc, p.G, p.nb, p.ks, p.smem, s);             \
-    return p.cols == 2 ? launch_hx<NN, (NN <= 64 ? 2 : 1), false>(a, pt, sc, p.jc, p.G, p.nb, p.ks, p.smem, s)       \
-                       : launch_hx<NN, 1, false>(a, pt, sc, p.jc, p.G, p.nb, p.ks, p.smem, s);
+    if (a.f16) return p.cols == 2 ? launch_hx<NN, (NN <= 64 ? 2 : 1), true>(a, pt, sc, p.jc, p.G, p.nb, p.ks, p.smem, p.ctas_per_sm, s) \
+                                  : launch_hx<NN, 1, true>(a, pt, sc, p.jc, p.G, p.nb, p.ks, p.smem, p.ctas_per_sm, s);             \
+    return p.cols == 2 ? launch_hx<NN, (NN <= 64 ? 2 : 1), false>(a, pt, sc, p.jc, p.G, p.nb, p.ks, p.smem, p.ctas_per_sm, s)       \
+                       : launch_hx<NN, 1, false>(a, pt, sc, p.jc, p.G, p.nb, p.ks, p.smem, p.ctas_per_sm, s);
   switch (a.n) {
     CDK_HX(32)
     CDK_HX(64)

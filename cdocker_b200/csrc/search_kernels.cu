@@ -776,22 +776,37 @@ __global__ void __launch_bounds__(256, 2) k_xpass2(WaveArgs a, int rot_per_cta) 
 }
 
 // ---------------------------------------------------------------------------------------
-// keep the two smallest keys (b1 < b2) of a stream of distinct keys
 // Plane x of rotation r read from B in any of its layouts; at(f) is column f of the plane.
 // Column-pair groups (cs = 1): float2 (f >> 1) 2G + (f & 1) past the plane's first pair; single-
 // column groups (cs = 0): float2 f G past the plane's first column. The plain layout is G = 1.
+// BL fixes the layout at compile time (the loads of a butterfly then share one base address):
+// kBPlain, kBPairs2 (column pairs, G = 2), kBSingle4 (single columns, G = 4); kBAny reads the
+// layout from WaveArgs.
+constexpr int kBAny = 0, kBPlain = 1, kBPairs2 = 2, kBSingle4 = 3;
+template <int BL>
 struct BPlane {
   const float2* p;
   int cs, gs;
   __device__ __forceinline__ BPlane(const WaveArgs& a, int r, int x, int n, int ncol) {
-    const int G = a.bgroup > 1 ? a.bgroup : 1;
-    cs = a.bcol ? 0 : 1;
+    const int G = BL == kBPlain ? 1 : BL == kBPairs2 ? 2 : BL == kBSingle4 ? 4 : (a.bgroup > 1 ? a.bgroup : 1);
+    cs = BL == kBSingle4 ? 0 : BL == kBAny ? (a.bcol ? 0 : 1) : 1;
     gs = G << cs;
     p = a.B + ((size_t)r * n + (x - x % G)) * ncol + ((x % G) << cs);
   }
-  __device__ __forceinline__ float2 at(int f) const { return p[(size_t)(f >> cs) * gs + (f & cs)]; }
+  __device__ __forceinline__ float2 at(int f) const {
+    if constexpr (BL == kBPlain) return p[f];
+    else if constexpr (BL == kBPairs2) return p[(f >> 1) * 4 + (f & 1)];
+    else if constexpr (BL == kBSingle4) return p[f * 4];
+    else return p[(size_t)(f >> cs) * gs + (f & cs)];
+  }
 };
+// the compile-time layout of a wave's B (kBAny for the others)
+inline int b_layout(const WaveArgs& a) {
+  if (a.bcol) return a.bgroup == 4 ? kBSingle4 : kBAny;
+  return a.bgroup <= 1 ? kBPlain : a.bgroup == 2 ? kBPairs2 : kBAny;
+}
 
+// keep the two smallest keys (b1 < b2) of a stream of distinct keys
 __device__ __forceinline__ void top2_insert(unsigned long long k, unsigned long long& b1, unsigned long long& b2) {
   // most candidates lose to the current second-smallest on the energy bits alone (one 32-bit
   // compare); the 64-bit order decides the rest
@@ -813,9 +828,45 @@ __device__ __forceinline__ void top2_merge(unsigned long long o1, unsigned long 
   b1 = n1;
 }
 
+// Candidate energies e at linear index lin, into a thread's smallest key (b1) or two smallest
+// keys (b1, b2). thr is the float of the largest key kept (+inf while a slot is empty): a value
+// strictly above it (as floats, the same order as the keys) cannot enter and is rejected before
+// its key is built; equal values, NaN and signed zeros take the exact 64-bit key path.
+template <bool TOP2>
+__device__ __forceinline__ void keep_min(float e, unsigned int lin, unsigned long long& b1, unsigned long long& b2,
+                                         float& thr) {
+  if (e > thr) return;
+  const unsigned long long k = ((unsigned long long)order_key(e) << 32) | lin;
+  if constexpr (TOP2) {
+    top2_insert(k, b1, b2);
+    thr = b2 == ~0ull ? INFINITY : key_to_float((unsigned int)(b2 >> 32));
+  } else {
+    if (k < b1) {
+      b1 = k;
+      thr = key_to_float((unsigned int)(k >> 32));
+    }
+  }
+}
+
+// smallest 64-bit key of the warp: redux on the high words, then on the low words of the lanes
+// holding the smallest high word
+__device__ __forceinline__ unsigned long long warp_min_key(unsigned long long k) {
+  const unsigned int hi = __reduce_min_sync(0xffffffffu, (unsigned int)(k >> 32));
+  const unsigned int lo = __reduce_min_sync(0xffffffffu, (unsigned int)(k >> 32) == hi ? (unsigned int)k : 0xffffffffu);
+  return ((unsigned long long)hi << 32) | lo;
+}
+// the warp's two smallest keys from every lane's (b1 < b2) of distinct keys: the smallest b1,
+// then the smallest of (b2 on the lane holding it, b1 elsewhere)
+template <bool TOP2>
+__device__ __forceinline__ void warp_keep_min(unsigned long long& b1, unsigned long long& b2) {
+  const unsigned long long k1 = warp_min_key(b1);
+  if constexpr (TOP2) b2 = warp_min_key(b1 == k1 ? b2 : b1);
+  b1 = k1;
+}
+
 // inverse (y,z) of one (rotation, x in window) plane + min / first argmin; TOP2: also the
 // plane's second-smallest key, for the FP64 near-tie break (WaveArgs.keys2)
-template <int N, bool TOP2>
+template <int N, bool TOP2, int BL>
 __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveArgs a) {
   constexpr int NZH = N / 2 + 1;
   constexpr int NCOL = N * NZH;
@@ -839,7 +890,7 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
   // plane x: NCOL / 2 column pairs, 16 B each, contiguous (plain layout) or every G-th of the
   // plane group (grouped layout, G planes per 16 B x column-pair block); or, single-column
   // groups, one float2 of every G
-  const BPlane bp(a, r, x, N, NCOL);
+  const BPlane<BL> bp(a, r, x, N, NCOL);
   if constexpr (ALIAS) {
     // y: positions -> natural rows, the first (R1-point, twiddle-free) stage reading its rows
     // straight from B: item (column l, block b) takes positions b R1 + j of column l, plane
@@ -868,6 +919,7 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
   const int npairs = (Wy + 1) / 2;
   const float inv = 1.0f / (float)((double)N * N * N);
   unsigned long long best = ~0ull, best2 = ~0ull;
+  float thr = INFINITY;
   if constexpr (ALIAS) {
     // Rows (2p, 2p+1) as one complex line Z_p(k) = Y(2p, k) + i Y(2p+1, k) with the Hermitian
     // extension over z, inverse-transformed in two radix stages (N = R0 R1), one work item per
@@ -932,17 +984,8 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
 #pragma unroll
       for (int j = 0; j < R0; ++j) {
         if (np + R1 * j < Wz) {
-          const unsigned long long k0 =
-              ((unsigned long long)order_key(v[j].x * inv) << 32) | (lin0 + (unsigned int)(R1 * j));
-          const unsigned long long k1 =
-              ((unsigned long long)order_key(v[j].y * inv) << 32) | (lin0 + (unsigned int)(N + R1 * j));
-          if constexpr (TOP2) {
-            if (row0) top2_insert(k0, best, best2);
-            if (row1) top2_insert(k1, best, best2);
-          } else {
-            if (row0) best = k0 < best ? k0 : best;
-            if (row1) best = k1 < best ? k1 : best;
-          }
+          if (row0) keep_min<TOP2>(v[j].x * inv, lin0 + (unsigned int)(R1 * j), best, best2, thr);
+          if (row1) keep_min<TOP2>(v[j].y * inv, lin0 + (unsigned int)(N + R1 * j), best, best2, thr);
         }
       }
     }
@@ -976,36 +1019,27 @@ __global__ void __launch_bounds__(256, (N <= 64 ? 8 : 2)) k_yz_inv_argmin(WaveAr
       for (int z = tid & 31; z < Wz; z += 32) {
         const float2 v = row[z];
         const float e = ((y & 1) ? v.y : v.x) * inv;
-        const unsigned int lin = (unsigned int)((x * N + y) * N + z);
-        const unsigned long long key = ((unsigned long long)order_key(e) << 32) | lin;
-        if constexpr (TOP2) top2_insert(key, best, best2);
-        else best = key < best ? key : best;
+        keep_min<TOP2>(e, (unsigned int)((x * N + y) * N + z), best, best2, thr);
       }
     }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
-    if constexpr (TOP2) {
-      const unsigned long long other2 = __shfl_xor_sync(0xffffffffu, best2, o);
-      top2_merge(other, other2, best, best2);
-    } else {
-      best = other < best ? other : best;
-    }
-  }
+  warp_keep_min<TOP2>(best, best2);
   if ((tid & 31) == 0) {
     s_best[tid >> 5] = best;
     if constexpr (TOP2) s_best2[tid >> 5] = best2;
   }
   __syncthreads();
-  if (tid == 0) {
-    for (int w = 1; w < (nthr >> 5); ++w) {
-      if constexpr (TOP2) top2_merge(s_best[w], s_best2[w], best, best2);
-      else best = s_best[w] < best ? s_best[w] : best;
-    }
-    atomicMin(a.keys + r, best);
-    if constexpr (TOP2) {
-      a.keys2[((size_t)r * N + x) * 2] = best;
-      a.keys2[((size_t)r * N + x) * 2 + 1] = best2;
+  if (tid < 32) {
+    const int nw = nthr >> 5;
+    best = tid < nw ? s_best[tid] : ~0ull;
+    if constexpr (TOP2) best2 = tid < nw ? s_best2[tid] : ~0ull;
+    warp_keep_min<TOP2>(best, best2);
+    if (tid == 0) {
+      atomicMin(a.keys + r, best);
+      if constexpr (TOP2) {
+        a.keys2[((size_t)r * N + x) * 2] = best;
+        a.keys2[((size_t)r * N + x) * 2 + 1] = best2;
+      }
     }
   }
 }
@@ -1036,7 +1070,7 @@ constexpr size_t octet_smem() {
   return sizeof(float2) * (N + (size_t)N * (N / 2 + 1));
 }
 
-template <int N, bool TOP2>
+template <int N, bool TOP2, int BL>
 __global__ void __launch_bounds__(32 * kOctWarps, 3) k_yz_octet(WaveArgs a) {
   constexpr int NZH = N / 2 + 1, NCOL = N * NZH;
   constexpr int R1 = N / 8;           // stage-1 radix; stage 2 is radix 8
@@ -1055,7 +1089,7 @@ __global__ void __launch_bounds__(32 * kOctWarps, 3) k_yz_octet(WaveArgs a) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int o = lane >> 3, t = lane & 7, g = warp * 4 + o;
   for (int i = tid; i < N; i += 32 * kOctWarps) s_tw[i] = a.tw[i];
-  const BPlane bp(a, r, x, N, NCOL);
+  const BPlane<BL> bp(a, r, x, N, NCOL);
   __syncthreads();
   // line position of stage-1 output m of block blk
   auto xpos = [](int blk, int m) { return blk * R1 + (m + blk) % R1; };
@@ -1101,6 +1135,7 @@ __global__ void __launch_bounds__(32 * kOctWarps, 3) k_yz_octet(WaveArgs a) {
   const int npairs = (Wy + 1) / 2;
   const float inv = 1.0f / (float)((double)N * N * N);
   unsigned long long best = ~0ull, best2 = ~0ull;
+  float thr = INFINITY;
   constexpr int ZR = (N / 2 + kOctets - 1) / kOctets;
 #pragma unroll 1
   for (int it = 0; it < ZR; ++it) {
@@ -1151,43 +1186,29 @@ __global__ void __launch_bounds__(32 * kOctWarps, 3) k_yz_octet(WaveArgs a) {
           const int z = np + R1 * j;
           if (z < Wz) {
             const unsigned int lin0 = (unsigned int)((x * N + y0) * N + z);
-            const unsigned long long k0 = ((unsigned long long)order_key(u[j].x * inv) << 32) | lin0;
-            const unsigned long long k1 = ((unsigned long long)order_key(u[j].y * inv) << 32) | (lin0 + N);
-            if constexpr (TOP2) {
-              if (row0) top2_insert(k0, best, best2);
-              if (row1) top2_insert(k1, best, best2);
-            } else {
-              if (row0) best = k0 < best ? k0 : best;
-              if (row1) best = k1 < best ? k1 : best;
-            }
+            if (row0) keep_min<TOP2>(u[j].x * inv, lin0, best, best2, thr);
+            if (row1) keep_min<TOP2>(u[j].y * inv, lin0 + N, best, best2, thr);
           }
         }
       }
     }
   }
-  for (int off = 16; off > 0; off >>= 1) {
-    const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, off);
-    if constexpr (TOP2) {
-      const unsigned long long other2 = __shfl_xor_sync(0xffffffffu, best2, off);
-      top2_merge(other, other2, best, best2);
-    } else {
-      best = other < best ? other : best;
-    }
-  }
+  warp_keep_min<TOP2>(best, best2);
   if (lane == 0) {
     s_best[warp] = best;
     if constexpr (TOP2) s_best2[warp] = best2;
   }
   __syncthreads();
-  if (tid == 0) {
-    for (int w = 1; w < kOctWarps; ++w) {
-      if constexpr (TOP2) top2_merge(s_best[w], s_best2[w], best, best2);
-      else best = s_best[w] < best ? s_best[w] : best;
-    }
-    atomicMin(a.keys + r, best);
-    if constexpr (TOP2) {
-      a.keys2[((size_t)r * N + x) * 2] = best;
-      a.keys2[((size_t)r * N + x) * 2 + 1] = best2;
+  if (warp == 0) {
+    best = lane < kOctWarps ? s_best[lane] : ~0ull;
+    if constexpr (TOP2) best2 = lane < kOctWarps ? s_best2[lane] : ~0ull;
+    warp_keep_min<TOP2>(best, best2);
+    if (lane == 0) {
+      atomicMin(a.keys + r, best);
+      if constexpr (TOP2) {
+        a.keys2[((size_t)r * N + x) * 2] = best;
+        a.keys2[((size_t)r * N + x) * 2 + 1] = best2;
+      }
     }
   }
 }
@@ -1486,9 +1507,16 @@ cudaError_t launch_yz_inv_t(const WaveArgs& a, cudaStream_t s) {
   // block stages at n <= 64 (the packed rows alias the plane there, 8 CTAs per SM: 1.6x faster
   // than the octets at 64^3); yz_block_stages: 1 forces block stages, 2 forces octets
   const bool octet = a.yz_block_stages == 2 || (a.yz_block_stages == 0 && N >= 96);
+  // the B layout as a template argument (kBAny reads it at run time)
+  const int bl = b_layout(a);
+#define CDK_YZ_PICK(KERN)                                                                     \
+  (bl == kBPlain    ? (a.keys2 ? KERN<N, true, kBPlain> : KERN<N, false, kBPlain>)           \
+   : bl == kBPairs2 ? (a.keys2 ? KERN<N, true, kBPairs2> : KERN<N, false, kBPairs2>)         \
+   : bl == kBSingle4 ? (a.keys2 ? KERN<N, true, kBSingle4> : KERN<N, false, kBSingle4>)      \
+                     : (a.keys2 ? KERN<N, true, kBAny> : KERN<N, false, kBAny>))
   if (octet) {
     constexpr size_t sm = octet_smem<N>();
-    auto kern = a.keys2 ? k_yz_octet<N, true> : k_yz_octet<N, false>;
+    auto kern = CDK_YZ_PICK(k_yz_octet);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     dim3 grid(N, a.nrot);
@@ -1497,7 +1525,8 @@ cudaError_t launch_yz_inv_t(const WaveArgs& a, cudaStream_t s) {
   }
   // twiddles + one plane (n <= 64: the packed rows alias it) [+ the packed rows]
   const size_t sm = sizeof(float2) * (N + N * (N / 2 + 1) + (N <= 64 ? 0 : (N / 2) * (N + 1)));
-  auto kern = a.keys2 ? k_yz_inv_argmin<N, true> : k_yz_inv_argmin<N, false>;
+  auto kern = CDK_YZ_PICK(k_yz_inv_argmin);
+#undef CDK_YZ_PICK
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   dim3 grid(N, a.nrot);
