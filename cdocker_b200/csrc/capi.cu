@@ -328,7 +328,7 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   }
   const bool f16 = f16form && rows;
   // the Hankel x pass loads tiled ligand rows by bulk copies, or untiled rows by per-thread copies
-  const bool tiled = hankel && hankel_tiled(c->opts.reserved[5], f16form);
+  const bool tiled = hankel && hankel_tiled(c->opts.reserved[5], f16form, n);
   const size_t lop_per = rows ? stream_lop_bytes_per_rotation(n, K, f16) : 0;
   int wave = c->opts.wave_rotations;
   if (wave <= 0) {

@@ -128,10 +128,14 @@ inline size_t lop_rotations(long nrot, bool tiled) {
 // The automatic tensor-core x pass at n = 64 (variant: opts.reserved[3]): streamed operator tiles
 // in the split-BF16 form, the Hankel kernel (over tiled rows) in the split-FP16 form
 inline bool use_stream_tiles(int variant, bool f16form) { return variant == 3 || (variant == 0 && !f16form); }
-// The Hankel x pass loads tiled rows by bulk copies in the split-FP16 form (opts.reserved[5] bit 6:
-// in the split-BF16 form too, whose plane kernel then writes its two parts as 32-byte pieces more
-// slowly than the untiled rows; bit 5: never)
-inline bool hankel_tiled(int reserved5, bool f16form) { return !(reserved5 & 32) && (f16form || (reserved5 & 64)); }
+// The Hankel x pass loads tiled rows by bulk copies in the split-FP16 form at n <= 64
+// (opts.reserved[5] bit 6: at every n and in the split-BF16 form too; bit 5: never). The plane
+// kernel writes tiled rows as one 32-byte piece per 128-byte line, more slowly than untiled rows;
+// the x pass gains more than that only at 64^3 split-FP16 (measured: 64^3 -8 % per search,
+// 96^3 and 128^3 +1-2 %, split-BF16 +20-30 %)
+inline bool hankel_tiled(int reserved5, bool f16form, int n) {
+  return !(reserved5 & 32) && ((f16form && n <= 64) || (reserved5 & 64));
+}
 // tiled rows: the stride of their 4 KB blocks (a pad after each block spreads the plane
 // kernel's 32-byte stores of neighbouring columns over more DRAM banks)
 int lop_block_stride();

@@ -407,7 +407,7 @@ void worker_loop(cdk_server* s) {
                                        hankel_plan(n, K, lb, f16, 0, &hp));
     a.lop = tc_wave ? lop_base : nullptr;
     // the Hankel x pass loads tiled rows (split-FP16) or untiled rows, as in a plain search
-    a.lop_tiled = (tc_wave && !tile_wave && hankel_tiled(s->v.hx_shape, f16)) ? 1 : 0;
+    a.lop_tiled = (tc_wave && !tile_wave && hankel_tiled(s->v.hx_shape, f16, n)) ? 1 : 0;
     a.lop_bstride = lop_block_stride();
     a.f16 = (tc_wave && f16) ? 1 : 0;
     a.bgroup = tc_wave ? stream_bgroup() : 1;

@@ -73,8 +73,8 @@ typedef struct cdk_opts {
                           1 to 4), bit 5: ligand rows copied per rotation by the producer
                           threads, bit 6: ligand rows written by the plane kernel in
                           128-rotation tiles that the x pass loads by bulk copies (default:
-                          tiles in the split-FP16 form, per-rotation copies in the split-BF16
-                          form; the same results either way);
+                          tiles in the split-FP16 form at n <= 64, per-rotation copies
+                          otherwise; the same results either way);
                           [6] precision forms: poses per wave re-scored in FP64
                           (cdk_ctx_top_poses): 0 = 8 (none in the FP32 form), -1 = none,
                           1..32; [7] = 1: no FP64 near-tie break of the argmin in the

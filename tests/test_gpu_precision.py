@@ -111,16 +111,18 @@ def test_tensor_core_variants_agree(grids_cache, wave):
                                                        ("c4_128", 1, 70, 45, 1)])
 def test_tiled_rows_match_thread_copies(grids_cache, form, name, n_conf, n_q, wave, cols):
     """The Hankel x pass loads its ligand rows either as 128-rotation tiles that the plane kernel
-    writes in the tensor cores' 32-byte swizzled layout (one bulk copy per K-step and column, the
-    default) or rotation by rotation with per-thread copies from the untiled rows. The MMAs see
-    the same operands either way, so results are bit-identical: ragged waves (partial tiles), one
-    and two columns per CTA, chunks of a tile's plan that a rotation does not touch (zeros written
-    by the plane kernel, zero-filled by the copies)."""
+    writes in the tensor cores' 32-byte swizzled layout (one bulk copy per K-step and column; the
+    default for split-FP16 at 64^3, forced here in both forms and at 128^3) or rotation by
+    rotation with per-thread copies from the untiled rows. The MMAs see the same operands either
+    way, so results are bit-identical: ragged waves (partial tiles), one and two columns per CTA,
+    chunks of a tile's plan that a rotation does not touch (zeros written by the plane kernel,
+    zero-filled by the copies)."""
     w = synth.make_workload(name, seed=17, n_conf=n_conf, n_q=n_q, grids_cache=grids_cache)
     out = {}
     for thread_copies in (False, True):
         with Receptor(w.grids, w.spacing, form=form, wave_rotations=wave, tc_hankel=True,
-                      tc_cols=cols, tc_thread_copies=thread_copies) as rec:
+                      tc_cols=cols, tc_thread_copies=thread_copies,
+                      tc_tiled_rows=not thread_copies) as rec:
             out[thread_copies] = rec.search(w.coor, w.charge, w.eps, w.slot, w.quats)
             st = rec.stats()
         assert st["xpass_kind"] == HANKEL[form] and st["col_tile"] == cols
