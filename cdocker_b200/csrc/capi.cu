@@ -225,8 +225,8 @@ int autotune_xpass(cdk_ctx* c, WaveArgs a, const RotDesc* d_rots, long nRot, int
 }
 
 // Times the Hankel tensor-core x pass on the search's first wave (rotations in the order the
-// waves use) under each candidate shape -- one or two columns per CTA (n <= 64), ring caps of
-// 8, 16 and 32 stages -- and keeps the fastest for this ligand box. The candidates run the same
+// waves use) under each candidate shape -- one or two columns per CTA (n <= 64), 1 to 3 K-steps
+// per ring stage, ring caps of 4, 8, 16 and 32 stages -- and keeps the fastest for this ligand box. The candidates run the same
 // MMAs per column in the same order, so the results are identical whichever wins.
 int autotune_hankel(cdk_ctx* c, WaveArgs a, const RotDesc* order, long nRot, int wave, bool f16,
                     const float* osc, cudaStream_t s) {
@@ -237,7 +237,7 @@ int autotune_hankel(cdk_ctx* c, WaveArgs a, const RotDesc* order, long nRot, int
   struct Cand { int cols, nb, ks; };
   std::vector<Cand> cands;
   for (int cols : {1, 2})
-    for (int ks : {1, 2})
+    for (int ks : {1, 2, 3})
       for (int nb : {4, 8, 16, 32}) {
         HankelPlan p{};
         if (!hankel_plan(c->n, c->K, a.Lb, f16, cols, &p, nb, ks) || p.cols != cols || p.ks != ks) continue;
