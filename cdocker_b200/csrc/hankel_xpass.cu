@@ -760,9 +760,10 @@ bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out,
     const bool two = 2 * 2 * cols * n <= 256;
     for (int pass = two ? 0 : 1; pass < 2; ++pass) {
       const size_t cap = (pass == 0 ? kSmemHalf : kSmemCap) - 1024;
-      // automatic: 3 K-steps per stage at n >= 96 where the box has at least 3 (measured 5 %
-      // faster at 96^3, 0-2 % at 128^3), else 2 where it has several, else 1
-      const int ks_auto = (n >= 96 && jc >= 3) ? 3 : jc >= 2 ? 2 : 1;
+      // automatic: 3 K-steps per stage at n >= 96 where the box has at least 3 (measured: x pass
+      // 5 % faster at 96^3 in both forms and 2 % at 128^3 split-BF16; 128^3 split-FP16 keeps 2,
+      // 3 measured 2.6 % slower there), else 2 where it has several, else 1
+      const int ks_auto = (n >= 96 && jc >= 3 && !(f16 && n >= 128)) ? 3 : jc >= 2 ? 2 : 1;
       for (int ks : {4, 3, 2, 1}) {
         if (ks_pref ? ks != ks_pref : ks > ks_auto) continue;
         const HxLayout L = hx_layout(n, K, cols, f16, G, ks);
