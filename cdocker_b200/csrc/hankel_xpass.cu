@@ -81,6 +81,17 @@ __device__ __forceinline__ uint64_t make_desc_sw32(uint32_t saddr, uint32_t sbo)
   return d;
 }
 
+// shared-memory matrix descriptor: K-major with 64-byte swizzle (rows of 64 bytes = two K-steps
+// of 16 values, 8-row atoms of 512 bytes; SBO: M/N stride of the atoms; LBO unused: 1)
+__device__ __forceinline__ uint64_t make_desc_sw64(uint32_t saddr, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)4 << 61;  // layout type 4: 64-byte swizzle
+  return d;
+}
+
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const volatile int* stop) {
   for (long i = 0; i < kWaitLimit; ++i) {
     uint32_t done;
@@ -494,7 +505,12 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
     // ligand rows, slot 0: per-thread copies in the no-swizzle layout (re | im core matrices
     // one half-tile apart), or tiled rows in the 32-byte swizzled layout (re | im in each row)
     const bool tiled = a.lop_tiled != 0;
-    const uint64_t dring = tiled ? make_desc_sw32(ring_s, 256) : make_desc(ring_s, HX_TILE / 2, HX_CORE);
+    // (split-BF16 tiled rows: one 8 KB tile of 64-byte rows, 64-byte swizzle, hi part in the
+    // first 32 bytes of each row and lo part in the next)
+    const uint64_t dring = !tiled ? make_desc(ring_s, HX_TILE / 2, HX_CORE)
+                           : F16  ? make_desc_sw32(ring_s, 256)
+                                  : make_desc_sw64(ring_s, 512);
+    const uint64_t lo_step = tiled ? 2u : (uint64_t)(HX_TILE >> 4);  // to the lo part
     const uint64_t dop = make_desc(op_s, L.S, HX_CORE);              // operator, group 0
     const uint64_t sS = L.S >> 4;
     int s = 0, u = 0, b = 0;
@@ -544,7 +560,7 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
                 umma(dre, ahi, bre_hi, idesc, acc0);
                 umma(dim, ahi, bre_hi + sS, idesc, acc0);
                 if constexpr (!F16) {
-                  const uint64_t alo = ahi + (HX_TILE >> 4);
+                  const uint64_t alo = ahi + lo_step;
                   umma(dre, alo, bre_hi, idesc, 1u);
                   umma(dim, alo, bre_hi + sS, idesc, 1u);
                 }

@@ -60,6 +60,27 @@ __device__ __forceinline__ void tiled_row_store(const WaveArgs& a, int r, int k,
   else st_v8u(dst, re, im);
 }
 
+// Tiled split-BF16 rows: the two 4 KB blocks of (tile, channel, chunk jc, column c) hold one
+// 8 KB tile of 128 rows of 64 B -- [hi re | hi im | lo re | lo im] of rotation m -- in the tensor
+// cores' K-major layout with 64-byte swizzle (16-byte chunk q of row m at q ^ ((m >> 1) & 3)), so
+// one lane writes its rotation's chunk as one 64-byte run; the x pass reads the lo part 32 bytes
+// into the same rows. rows[0..3]: hi re, hi im, lo re, lo im.
+__device__ __forceinline__ void tiled_row_store64(const WaveArgs& a, int r, int k, int jc, int c, const uint4* rows) {
+  const int ncol = a.n * (a.n / 2 + 1);
+  const size_t blk0 = ((((size_t)(r / kTileRot) * a.K + k) * 4 + jc) * ncol + c) * 2;
+  const int m = r % kTileRot;
+  // rows 0-63 in the part-0 block, rows 64-127 in the part-1 block (lop_bstride apart)
+  unsigned char* row = a.lop + (blk0 + (size_t)(m >> 6)) * (size_t)a.lop_bstride + (size_t)(m & 63) * 64;
+  const int sw = (m >> 1) & 3;
+  const bool s1 = (sw & 2) != 0, s0 = (sw & 1) != 0;
+  const uint4 e0 = s1 ? rows[2] : rows[0], e1 = s1 ? rows[3] : rows[1];
+  const uint4 e2 = s1 ? rows[0] : rows[2], e3 = s1 ? rows[1] : rows[3];
+  uint4* dst = reinterpret_cast<uint4*>(row);
+  st_v8u(dst, s0 ? e1 : e0, s0 ? e0 : e1);
+  st_v8u(dst + 2, s0 ? e3 : e2, s0 ? e2 : e3);
+}
+
+
 // ---------------------------------------------------------------------------------------
 // exact-order float rotation (src/QuaternionMultiply.cpp:3-11, src/Rotate.cpp:4-27)
 __device__ __forceinline__ void qmul_rn(const float* l, const float* r, float* o) {
@@ -370,8 +391,9 @@ __device__ __forceinline__ void plane_chunk_write(const WaveArgs& a, int r, int 
       split_bf16x2(ay[d], ay[d + 1], ih[d / 2], il[d / 2]);
     }
     if (a.lop_tiled) {
-      tiled_row_store(a, r, k, jc, 0, c, make_uint4(rh[0], rh[1], rh[2], rh[3]), make_uint4(ih[0], ih[1], ih[2], ih[3]));
-      tiled_row_store(a, r, k, jc, 1, c, make_uint4(rl[0], rl[1], rl[2], rl[3]), make_uint4(il[0], il[1], il[2], il[3]));
+      const uint4 rows[4] = {make_uint4(rh[0], rh[1], rh[2], rh[3]), make_uint4(ih[0], ih[1], ih[2], ih[3]),
+                             make_uint4(rl[0], rl[1], rl[2], rl[3]), make_uint4(il[0], il[1], il[2], il[3])};
+      tiled_row_store64(a, r, k, jc, c, rows);
       return;
     }
     uint4* dst = reinterpret_cast<uint4*>(a.lop) +
@@ -388,8 +410,12 @@ __device__ __forceinline__ void plane_chunk_write(const WaveArgs& a, int r, int 
 // touch (the bulk copies of the x pass load whole 128-rotation blocks)
 __device__ __forceinline__ void tiled_zero_chunk(const WaveArgs& a, int r, int k, int jc, int c) {
   const uint4 z = make_uint4(0u, 0u, 0u, 0u);
-  tiled_row_store(a, r, k, jc, 0, c, z, z);
-  if (!a.f16) tiled_row_store(a, r, k, jc, 1, c, z, z);
+  if (a.f16) {
+    tiled_row_store(a, r, k, jc, 0, c, z, z);
+  } else {
+    const uint4 zz[4] = {z, z, z, z};
+    tiled_row_store64(a, r, k, jc, c, zz);
+  }
 }
 
 // The K-step range [lo, hi] of channel k in the stage plan of rotation r's tile (k_tile_plan);
