@@ -136,8 +136,8 @@ inline bool use_stream_tiles(int variant, bool f16form) { return variant == 3 ||
 inline bool hankel_tiled(int reserved5, bool f16form, int n) {
   return !(reserved5 & 32) && ((f16form && n <= 64) || (reserved5 & 64));
 }
-// tiled rows: the stride of their 4 KB blocks (a pad after each block spreads the plane
-// kernel's 32-byte stores of neighbouring columns over more DRAM banks)
+// tiled rows: the stride of their 4 KB blocks (the blocks are packed; the kernels take the stride
+// from WaveArgs.lop_bstride)
 int lop_block_stride();
 // bytes of a wave's ligand rows: per-rotation bytes scaled by the block stride when tiled
 inline size_t lop_wave_bytes(long nrot, bool tiled, size_t per_rotation) {

@@ -437,14 +437,7 @@ __device__ __forceinline__ void tile_plan_range(const WaveArgs& a, int r, int k,
 // CDK_PLANE_ORDER=1 keeps the channel-major order, for measurement
 }  // namespace
 
-int lop_block_stride() {
-  static const int v = [] {
-    const char* e = std::getenv("CDK_LOP_PAD");
-    const int pad = e ? std::atoi(e) : 0;
-    return (int)kLopBlock + ((pad >= 0 && pad <= 4096 && pad % 128 == 0) ? pad : 0);
-  }();
-  return v;
-}
+int lop_block_stride() { return (int)kLopBlock; }
 
 namespace {
 
