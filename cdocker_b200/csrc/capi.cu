@@ -296,12 +296,12 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   probe.kyof = (c->opts.reserved[1] & 1) ? nullptr : c->d_kyof;
   probe.max_atoms = maxAtoms;
   probe.atom_cap = maxAtoms;
-  // automatic choice (reserved[3] = 0): at 64^3 the streamed-tile kernel where it applies (box
-  // <= 32 planes; measured 1.4x faster there than the Hankel kernel), the Hankel kernel at the
-  // other sizes; 3 forces streamed tiles, 4 the Hankel kernel
+  // automatic choice (reserved[3] = 0): the Hankel kernel over tiled rows (64^3: 5 % faster per
+  // search than the streamed-tile kernel in the split-BF16 form); 3 forces streamed tiles (64^3,
+  // box <= 32 planes), 4 the Hankel kernel
   const int variant = c->opts.reserved[3];
   const bool can_stream = tc && stream_supported(n, Lb) && direct_planes(probe);
-  const bool streamed = can_stream && use_stream_tiles(variant, f16form);
+  const bool streamed = can_stream && use_stream_tiles(variant);
   HankelPlan hp{};
   const bool hankel = tc && !streamed && (variant == 0 || variant == 4) && direct_planes(probe) &&
                       hankel_plan(n, K, Lb, f16form, c->opts.reserved[5] & 3, &hp, 0, (c->opts.reserved[5] >> 2) & 7);
@@ -327,8 +327,8 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
     return CDK_ERR_UNSUPPORTED;
   }
   const bool f16 = f16form && rows;
-  // the Hankel x pass loads tiled ligand rows by bulk copies, or untiled rows by per-thread copies
-  const bool tiled = hankel && hankel_tiled(c->opts.reserved[5], f16form, n);
+  // the Hankel x pass loads tiled ligand rows by tensor copies, or untiled rows by per-thread copies
+  const bool tiled = hankel && hankel_tiled(c->opts.reserved[5]);
   const size_t lop_per = rows ? stream_lop_bytes_per_rotation(n, K, f16) : 0;
   int wave = c->opts.wave_rotations;
   if (wave <= 0) {
@@ -377,7 +377,6 @@ int run_waves(cdk_ctx* c, const float* d_coor, const AtomParam* d_params, const 
   a.A = rows ? nullptr : reinterpret_cast<float2*>(base + b_rotxyz + b_rec + b_keys);
   a.lop = rows ? reinterpret_cast<unsigned char*>(base + b_rotxyz + b_rec + b_keys) : nullptr;
   a.lop_tiled = tiled ? 1 : 0;
-  a.lop_bstride = lop_block_stride();
   a.B = reinterpret_cast<float2*>(base + b_rotxyz + b_rec + b_keys + b_A);
   a.keys2 = tiebreak ? reinterpret_cast<unsigned long long*>(base + b_rotxyz + b_rec + b_keys + b_A + b_B) : nullptr;
   a.phat = c->d_phat;

@@ -105,44 +105,37 @@ struct WaveArgs {
   int lop_tiled;             // 0: [nrot/8][K][hi/lo][chunk j < 4][re/im][ncol/4][nrot%8][ncol%4]
                              //    x 16 B of 8 planes (nrot rounded up to a multiple of 8), the
                              //    streamed-tile x pass's rows;
-                             // 1: 128-rotation tiles [nrot/128][K][chunk j < 4][ncol][hi/lo]
-                             //    of 4 KB blocks (lop_bstride bytes apart) in the tensor cores'
-                             //    K-major layout with 32-byte
-                             //    swizzle (rotation m of the tile at 32 m: its re and im planes,
-                             //    16 B each, the halves exchanged where m & 4), one bulk copy
-                             //    per K-step for the Hankel x pass; chunks of the tile's stage
-                             //    plan that a valid rotation does not touch hold zeros (the
-                             //    plane kernel runs after k_tile_plan)
+                             // 1: 128-rotation row sets [nrot/128][K][chunk j < 4][rotation
+                             //    m < 128][ncol] of one row per (rotation, column): 32 B
+                             //    [re | im] (split-FP16) or 64 B [hi re | hi im | lo re | lo im]
+                             //    (split-BF16) of 8 planes, natural order; the Hankel x pass
+                             //    loads column c of a row set (128 rows) with one tensor copy
+                             //    per K-step, which applies the tensor cores' 32- or 64-byte
+                             //    swizzle; chunks of the tile's stage plan that a valid rotation
+                             //    does not touch hold zeros (the plane kernel runs after
+                             //    k_tile_plan)
   int plane_rot_major;       // set by the plane kernel's launcher: grid (nrot, K) instead of
                              // (K, nrot)
-  int lop_bstride;           // tiled rows: bytes from one 4 KB block to the next (>= 4096)
 };
-// rotations per tensor-core tile (the MMA's M), and the 4 KB block of one (tile, channel, chunk,
-// part, column) in the tiled ligand-row layout
+// rotations per tensor-core tile (the MMA's M), and the bytes of one K-step (128 rows of 32 B)
+// of one column and part in the tiled ligand-row layout
 constexpr int kTileRot = 128;
 constexpr size_t kLopBlock = 4096;
 // rotations a wave's ligand rows are allocated for
 inline size_t lop_rotations(long nrot, bool tiled) {
   return tiled ? (size_t)((nrot + kTileRot - 1) / kTileRot) * kTileRot : (size_t)((nrot + 7) & ~7L);
 }
-// The automatic tensor-core x pass at n = 64 (variant: opts.reserved[3]): streamed operator tiles
-// in the split-BF16 form, the Hankel kernel (over tiled rows) in the split-FP16 form
-inline bool use_stream_tiles(int variant, bool f16form) { return variant == 3 || (variant == 0 && !f16form); }
-// The Hankel x pass loads tiled rows by bulk copies in the split-FP16 form at n <= 64
-// (opts.reserved[5] bit 6: at every n and in the split-BF16 form too; bit 5: never). The plane
-// kernel writes tiled rows as one 32-byte piece per 128-byte line, more slowly than untiled rows;
-// the x pass gains more than that only at 64^3 split-FP16 (measured: 64^3 -8 % per search,
-// 96^3 and 128^3 +1-2 %, split-BF16 +20-30 %)
-inline bool hankel_tiled(int reserved5, bool f16form, int n) {
-  return !(reserved5 & 32) && ((f16form && n <= 64) || (reserved5 & 64));
-}
-// tiled rows: the stride of their 4 KB blocks (the blocks are packed; the kernels take the stride
-// from WaveArgs.lop_bstride)
-int lop_block_stride();
-// bytes of a wave's ligand rows: per-rotation bytes scaled by the block stride when tiled
+// The automatic tensor-core x pass (variant: opts.reserved[3] = 0) is the Hankel kernel at every
+// n; the 64^3 kernel with streamed operator tiles runs on request (3)
+inline bool use_stream_tiles(int variant) { return variant == 3; }
+// The Hankel x pass loads tiled rows (one tensor copy per K-step and column) unless
+// opts.reserved[5] bit 5 asks for per-rotation copies by its producer threads (bit 6, tiled
+// rows, is the default). Measured per search against per-rotation copies: 64^3 -13 % (split-FP16)
+// and -19 % (split-BF16), 96^3 -6 % and -13 %, 128^3 -3 % and -6 %
+inline bool hankel_tiled(int reserved5) { return !(reserved5 & 32); }
+// bytes of a wave's ligand rows (per-rotation bytes times the rotations allocated)
 inline size_t lop_wave_bytes(long nrot, bool tiled, size_t per_rotation) {
-  return tiled ? lop_rotations(nrot, true) * (per_rotation / kLopBlock) * (size_t)lop_block_stride()
-               : lop_rotations(nrot, false) * per_rotation;
+  return lop_rotations(nrot, tiled) * per_rotation;
 }
 
 // Launchers (stream-ordered, no synchronisation). Return cudaError_t of the launch.

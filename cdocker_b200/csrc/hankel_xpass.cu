@@ -22,10 +22,12 @@
 // P~ and stays resident: no operator bytes are streamed per tile.
 //
 // CTA = COLS columns, persistent over the wave's 128-rotation tiles; 288 threads:
-//   warps 0-3  producers: thread = rotation of the tile; per stage (one or two K-steps of one
-//              channel, all COLS columns) 16-byte cp.async copies of its ligand rows (rows of chunks the
-//              rotation does not touch are zero-filled by the copy itself), then one
-//              cp.async-completion arrival on the stage's "full" mbarrier;
+//   warps 0-3  producers. Tiled rows (the default): thread 0 issues per stage (one to three
+//              K-steps of one channel, all COLS columns) one tensor copy per K-step and column of
+//              the 128 rotations' rows, already in the K-major swizzled layout, completing on the
+//              stage's "full" mbarrier by byte count. Untiled rows: thread = rotation of the tile;
+//              16-byte cp.async copies of its ligand rows (rows of chunks the rotation does not
+//              touch are zero-filled by the copy itself), then one cp.async-completion arrival;
 //   warp 4     MMA issuer (one elected lane issues): per K-step and column 2 (real, imaginary) x 2
 //              (split-FP16: operator hi, lo) or x 3 (split-BF16: hi*hi, lo*hi, hi*lo) MMAs;
 //              commits each stage (1 or 2 K-steps) to its "empty" mbarrier and each tile to a
@@ -34,6 +36,8 @@
 //              other of two TMEM accumulator sets (TMEM "empty" mbarrier per set).
 // Every wait is bounded; a wait that gives up sets the fault flag, the other roles stop at their
 // next wait, issued copies land and TMEM is freed.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -236,8 +240,8 @@ __host__ __device__ inline HxLayout hx_layout(int n, int K, int cols, bool f16, 
 
 template <int N, int COLS, bool F16>
 __global__ void __launch_bounds__(HX_THREADS, 2)
-    k_xpass_hankel(WaveArgs a, const float2* __restrict__ pt, HxScale sc, int jc, int G, int nb, int ks,
-                   int split) {
+    k_xpass_hankel(const __grid_constant__ CUtensorMap rows_map, WaveArgs a, const float2* __restrict__ pt,
+                   HxScale sc, int jc, int G, int nb, int ks, int split) {
   constexpr int NCOL = N * (N / 2 + 1);
   constexpr int LPARTS = F16 ? 1 : 2;
   constexpr int NMAX = N;                          // TMEM columns of one output block (re or im)
@@ -347,20 +351,18 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
   const uint32_t op_s = smem_u32(op);
 
   if (warp < HX_PRODUCERS / 32 && a.lop_tiled) {
-    // ---- producer, tiled rows: one thread issues every stage as bulk copies of whole 4 KB
-    // blocks (128 rotations x one K-step of one column and part, already in the swizzled
-    // K-major layout, untouched chunks already zero); the copies complete on the stage's full
-    // barrier by their byte count, in the async proxy the tensor cores read
+    // ---- producer, tiled rows: one thread issues every stage as tensor copies of column c of
+    // a row set (128 rotations x one K-step, both parts in split-BF16; rows_map applies the
+    // tensor cores' swizzle; untouched chunks already zero); the copies complete on the stage's
+    // full barrier by their byte count, in the async proxy the tensor cores read
     if (tid == 0) {
-      const size_t bst = (size_t)a.lop_bstride;
-      const size_t tile_bytes = (size_t)K * 4 * NCOL * LPARTS * bst;
+      const uint64_t map = reinterpret_cast<uint64_t>(&rows_map);
       int s = 0, b = 0;
       uint32_t round = 0;
       bool ok = true;
       for (int t = tbeg; t < ntiles && ok; ++t) {
         const TilePlan p = load_plan(a.rec + t * HX_R);
         if (p.steps == 0) continue;
-        const unsigned char* tb = a.lop + (size_t)t * tile_bytes;
         for (int ai = 0; ai < p.nact && ok; ++ai) {
           const int k = (int)((p.pk >> (4 * ai)) & 15);
           const int jlo = (int)((p.pl >> (4 * ai)) & 15), jhi = (int)((p.ph >> (4 * ai)) & 15);
@@ -377,19 +379,18 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
                              (uint32_t)(jn * COLS * LPARTS) * (uint32_t)kLopBlock),
                          "r"(full)
                          : "memory");
-            for (int jj = 0; jj < jn; ++jj)
+            for (int jj = 0; jj < jn; ++jj) {
+              const int row0 = ((t * K + k) * 4 + (j0 + jj)) * HX_R;  // the row set's first row
 #pragma unroll
-              for (int cc = 0; cc < COLS; ++cc)
-#pragma unroll
-                for (int hl = 0; hl < LPARTS; ++hl) {
-                  const unsigned char* src =
-                      tb + ((((size_t)k * 4 + (j0 + jj)) * NCOL + c0 + cc) * LPARTS + hl) * bst;
-                  const uint32_t dst = st + (uint32_t)jj * L.ksub + (uint32_t)(cc * LPARTS + hl) * HX_TILE;
-                  asm volatile(
-                      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                      "l"(src), "r"((uint32_t)kLopBlock), "r"(full)
-                      : "memory");
-                }
+              for (int cc = 0; cc < COLS; ++cc) {
+                const uint32_t dst = st + (uint32_t)jj * L.ksub + (uint32_t)(cc * LPARTS) * HX_TILE;
+                asm volatile(
+                    "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                    " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+                    "l"(map), "r"(0), "r"(c0 + cc), "r"(row0), "r"(full)
+                    : "memory");
+              }
+            }
             if (++b == nb) {
               b = 0;
               ++round;
@@ -544,7 +545,7 @@ __global__ void __launch_bounds__(HX_THREADS, 2)
             break;
           }
           // the producers' cp.async writes (generic proxy) reach the tensor core (async proxy);
-          // bulk copies (tiled rows) write in the async proxy already
+          // tensor copies (tiled rows) write in the async proxy already
           if (!tiled) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const int jn = min(ks, jhi + 1 - j0);
@@ -739,6 +740,41 @@ static int hx_split(int groups, int ntiles, int ctas_per_sm) {
   return best;
 }
 
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// The tensor map of a wave's tiled ligand rows: rows of 16 (split-FP16) or 32 (split-BF16) 16-bit
+// values, ncol of them per rotation, 128 rotations per row set and K x 4 row sets per tile; a
+// box is column c of 128 consecutive rows (one row set), swizzled as the tensor cores read it.
+// L2 promotion to 256-byte requests (a row is 32 or 64 bytes; the neighbouring columns' CTAs read
+// the rest of each line): measured 50.2 ms per 1e5 rotations at 64^3 split-FP16 with none or
+// 128 bytes, 49.9 with 256 and 91 with 64
+cudaError_t rows_tensor_map(CUtensorMap* map, const void* rows, int n, int K, int ntiles, bool f16) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return cudaErrorNotSupported;
+  if ((reinterpret_cast<uintptr_t>(rows) & 127) || ntiles < 1) return cudaErrorInvalidValue;
+  const cuuint64_t ncol = (cuuint64_t)n * (n / 2 + 1);
+  const cuuint64_t rb = f16 ? 32 : 64;  // bytes per row
+  const cuuint64_t dims[3] = {rb / 2, ncol, (cuuint64_t)ntiles * K * 4 * HX_R};
+  const cuuint64_t strides[2] = {rb, ncol * rb};
+  const cuuint32_t box[3] = {(cuuint32_t)(rb / 2), 1, (cuuint32_t)HX_R};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, const_cast<void*>(rows), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, f16 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_64B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 template <int N, int COLS, bool F16>
 cudaError_t launch_hx(const WaveArgs& a, const float2* pt, const HxScale& sc, int jc, int G, int nb, int ks,
                       size_t smem, int ctas_per_sm, cudaStream_t s) {
@@ -749,8 +785,14 @@ cudaError_t launch_hx(const WaveArgs& a, const float2* pt, const HxScale& sc, in
   e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
   const int groups = NCOL / COLS;
-  const int split = hx_split(groups, (a.nrot + HX_R - 1) / HX_R, ctas_per_sm);
-  kern<<<groups * split, HX_THREADS, smem, s>>>(a, pt, sc, jc, G, nb, ks, split);
+  const int ntiles = (a.nrot + HX_R - 1) / HX_R;
+  const int split = hx_split(groups, ntiles, ctas_per_sm);
+  CUtensorMap map{};
+  if (a.lop_tiled) {
+    e = rows_tensor_map(&map, a.lop, N, a.K, ntiles, F16);
+    if (e != cudaSuccess) return e;
+  }
+  kern<<<groups * split, HX_THREADS, smem, s>>>(map, a, pt, sc, jc, G, nb, ks, split);
   return cudaGetLastError();
 }
 
@@ -776,10 +818,11 @@ bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out,
     const bool two = 2 * 2 * cols * n <= 256;
     for (int pass = two ? 0 : 1; pass < 2; ++pass) {
       const size_t cap = (pass == 0 ? kSmemHalf : kSmemCap) - 1024;
-      // automatic: 3 K-steps per stage at n >= 96 where the box has at least 3 (measured: x pass
-      // 5 % faster at 96^3 in both forms and 2 % at 128^3 split-BF16; 128^3 split-FP16 keeps 2,
-      // 3 measured 2.6 % slower there), else 2 where it has several, else 1
-      const int ks_auto = (n >= 96 && jc >= 3 && !(f16 && n >= 128)) ? 3 : jc >= 2 ? 2 : 1;
+      // automatic: 3 K-steps per stage where the box has at least 3 (measured over tiled rows,
+      // x pass: split-BF16 12 % faster at 64^3, 4.5 % at 128^3; split-FP16 4.5 % at 128^3, and
+      // 5 % at 96^3 in both forms), except at n <= 64 in the split-FP16 form (2: 3 measured
+      // 1.5 % slower), else 2 where it has several, else 1
+      const int ks_auto = (jc >= 3 && !(f16 && n <= 64)) ? 3 : jc >= 2 ? 2 : 1;
       for (int ks : {4, 3, 2, 1}) {
         if (ks_pref ? ks != ks_pref : ks > ks_auto) continue;
         const HxLayout L = hx_layout(n, K, cols, f16, G, ks);
@@ -825,7 +868,6 @@ cudaError_t launch_xpass_hankel(const WaveArgs& a, const float2* pt, const float
   if (!a.lop || !pt || a.K > KMAX) return cudaErrorInvalidValue;
   // the B layout must be the plan's (the inverse (y,z) pass reads what this pass writes)
   if ((a.bcol != 0) != (p.cols == 1) || (a.bcol && a.bgroup != 2 && a.bgroup != 4)) return cudaErrorInvalidValue;
-  if (a.lop_tiled && (a.lop_bstride < (int)kLopBlock || a.lop_bstride % 128)) return cudaErrorInvalidValue;
   HxScale sc{};
   for (int k = 0; k < a.K; ++k) sc.s[k] = (a.f16 && f16_scale) ? f16_scale[k] : 1.f;
   // the stage plan of every 128-rotation tile (channels, K-steps, largest window); with tiled

@@ -47,37 +47,27 @@ __device__ __forceinline__ void st_v8u(void* p, uint4 lo, uint4 hi) {
                : "memory");
 }
 
-// Tiled ligand rows (WaveArgs.lop_tiled): the 32-byte row of rotation r in the 4 KB block of
-// (tile r / 128, channel k, chunk jc, column c, part hl); re and im planes exchanged where
-// r & 4 (the tensor cores' 32-byte swizzle XORs address bit 4 with bit 7)
-__device__ __forceinline__ void tiled_row_store(const WaveArgs& a, int r, int k, int jc, int hl, int c, uint4 re,
-                                                uint4 im) {
-  const int lp = a.f16 ? 1 : 2;
+// Tiled ligand rows (WaveArgs.lop_tiled): (tile r / 128, channel k, chunk jc) is a row set of
+// 128 rotations x ncol columns; rotation m = r % 128 keeps its columns side by side, so the lanes
+// of a warp (consecutive columns) write one contiguous run. Rows are in natural order: the x
+// pass's tensor copies gather column c of the 128 rotations and apply the tensor cores' swizzle.
+__device__ __forceinline__ unsigned char* tiled_row(const WaveArgs& a, int r, int k, int jc, int c, int row_bytes) {
   const int ncol = a.n * (a.n / 2 + 1);
-  const size_t blk = ((((size_t)(r / kTileRot) * a.K + k) * 4 + jc) * ncol + c) * lp + hl;
-  uint4* dst = reinterpret_cast<uint4*>(a.lop + blk * (size_t)a.lop_bstride) + (size_t)(r % kTileRot) * 2;
-  if (r & 4) st_v8u(dst, im, re);
-  else st_v8u(dst, re, im);
+  const size_t set = ((size_t)(r / kTileRot) * a.K + k) * 4 + jc;
+  return a.lop + ((set * kTileRot + (size_t)(r % kTileRot)) * ncol + c) * (size_t)row_bytes;
 }
 
-// Tiled split-BF16 rows: the two 4 KB blocks of (tile, channel, chunk jc, column c) hold one
-// 8 KB tile of 128 rows of 64 B -- [hi re | hi im | lo re | lo im] of rotation m -- in the tensor
-// cores' K-major layout with 64-byte swizzle (16-byte chunk q of row m at q ^ ((m >> 1) & 3)), so
-// one lane writes its rotation's chunk as one 64-byte run; the x pass reads the lo part 32 bytes
-// into the same rows. rows[0..3]: hi re, hi im, lo re, lo im.
+// split-FP16: one 32-byte row [re | im] of the 8 planes
+__device__ __forceinline__ void tiled_row_store(const WaveArgs& a, int r, int k, int jc, int c, uint4 re, uint4 im) {
+  st_v8u(tiled_row(a, r, k, jc, c, 32), re, im);
+}
+
+// split-BF16: one 64-byte row [hi re | hi im | lo re | lo im]; the x pass reads the lo part 32
+// bytes into the same rows. rows[0..3]: hi re, hi im, lo re, lo im.
 __device__ __forceinline__ void tiled_row_store64(const WaveArgs& a, int r, int k, int jc, int c, const uint4* rows) {
-  const int ncol = a.n * (a.n / 2 + 1);
-  const size_t blk0 = ((((size_t)(r / kTileRot) * a.K + k) * 4 + jc) * ncol + c) * 2;
-  const int m = r % kTileRot;
-  // rows 0-63 in the part-0 block, rows 64-127 in the part-1 block (lop_bstride apart)
-  unsigned char* row = a.lop + (blk0 + (size_t)(m >> 6)) * (size_t)a.lop_bstride + (size_t)(m & 63) * 64;
-  const int sw = (m >> 1) & 3;
-  const bool s1 = (sw & 2) != 0, s0 = (sw & 1) != 0;
-  const uint4 e0 = s1 ? rows[2] : rows[0], e1 = s1 ? rows[3] : rows[1];
-  const uint4 e2 = s1 ? rows[0] : rows[2], e3 = s1 ? rows[1] : rows[3];
-  uint4* dst = reinterpret_cast<uint4*>(row);
-  st_v8u(dst, s0 ? e1 : e0, s0 ? e0 : e1);
-  st_v8u(dst + 2, s0 ? e3 : e2, s0 ? e2 : e3);
+  uint4* dst = reinterpret_cast<uint4*>(tiled_row(a, r, k, jc, c, 64));
+  st_v8u(dst, rows[0], rows[1]);
+  st_v8u(dst + 2, rows[2], rows[3]);
 }
 
 
@@ -372,7 +362,7 @@ __device__ __forceinline__ void plane_chunk_write(const WaveArgs& a, int r, int 
       hi[d / 2] = *reinterpret_cast<const uint32_t*>(&pi);
     }
     if (a.lop_tiled) {
-      tiled_row_store(a, r, k, jc, 0, c, make_uint4(hr[0], hr[1], hr[2], hr[3]), make_uint4(hi[0], hi[1], hi[2], hi[3]));
+      tiled_row_store(a, r, k, jc, c, make_uint4(hr[0], hr[1], hr[2], hr[3]), make_uint4(hi[0], hi[1], hi[2], hi[3]));
       return;
     }
     uint4* dst = reinterpret_cast<uint4*>(a.lop) +
@@ -407,11 +397,11 @@ __device__ __forceinline__ void plane_chunk_write(const WaveArgs& a, int r, int 
 }
 
 // Tiled rows: zeros for a chunk of the tile's stage plan that this rotation's channel does not
-// touch (the bulk copies of the x pass load whole 128-rotation blocks)
+// touch (the x pass's tensor copies load the rows of all 128 rotations of a row set)
 __device__ __forceinline__ void tiled_zero_chunk(const WaveArgs& a, int r, int k, int jc, int c) {
   const uint4 z = make_uint4(0u, 0u, 0u, 0u);
   if (a.f16) {
-    tiled_row_store(a, r, k, jc, 0, c, z, z);
+    tiled_row_store(a, r, k, jc, c, z, z);
   } else {
     const uint4 zz[4] = {z, z, z, z};
     tiled_row_store64(a, r, k, jc, c, zz);
@@ -435,12 +425,6 @@ __device__ __forceinline__ void tile_plan_range(const WaveArgs& a, int r, int k,
 
 // plane kernel CTA order for tiled rows: rotation-major by default; the environment variable
 // CDK_PLANE_ORDER=1 keeps the channel-major order, for measurement
-}  // namespace
-
-int lop_block_stride() { return (int)kLopBlock; }
-
-namespace {
-
 int plane_rot_major_host() {
   static const int v = [] {
     const char* e = std::getenv("CDK_PLANE_ORDER");
@@ -1773,7 +1757,7 @@ cudaError_t launch_prep(const WaveArgs& a, cudaStream_t s) {
 cudaError_t launch_spread_yz(const WaveArgs& a, cudaStream_t s) {
   if (a.lop_tiled) {
     // the tiled rows zero-fill by the tiles' stage plans: k_tile_plan first
-    if (!a.lop || !direct_planes(a) || a.lop_bstride < (int)kLopBlock || a.lop_bstride % 128) return cudaErrorInvalidValue;
+    if (!a.lop || !direct_planes(a) || (reinterpret_cast<uintptr_t>(a.lop) & 127)) return cudaErrorInvalidValue;
     cudaError_t e = launch_tile_plan(a, (a.Lb + 7) / 8, s);
     if (e != cudaSuccess) return e;
   }

@@ -401,14 +401,13 @@ void worker_loop(cdk_server* s) {
     // the same x-pass choice as a plain search on the context (results alone and in the mix
     // stay identical): streamed tiles at 64^3 where they apply, the Hankel kernel elsewhere
     HankelPlan hp{};
-    const bool tile_wave = s->streamed && s->v.top != nullptr && use_stream_tiles(s->v.tc_variant, f16) &&
+    const bool tile_wave = s->streamed && s->v.top != nullptr && use_stream_tiles(s->v.tc_variant) &&
                            stream_supported(n, lb) && direct_planes(a);
     const bool tc_wave = tile_wave || (s->streamed && s->v.tc_variant != 3 && direct_planes(a) &&
                                        hankel_plan(n, K, lb, f16, 0, &hp));
     a.lop = tc_wave ? lop_base : nullptr;
     // the Hankel x pass loads tiled rows (split-FP16) or untiled rows, as in a plain search
-    a.lop_tiled = (tc_wave && !tile_wave && hankel_tiled(s->v.hx_shape, f16, n)) ? 1 : 0;
-    a.lop_bstride = lop_block_stride();
+    a.lop_tiled = (tc_wave && !tile_wave && hankel_tiled(s->v.hx_shape)) ? 1 : 0;
     a.f16 = (tc_wave && f16) ? 1 : 0;
     a.bgroup = tc_wave ? stream_bgroup() : 1;
     a.bcol = 0;
@@ -496,7 +495,7 @@ int cdk_server_create(cdk_ctx* ctx, const cdk_server_opts* opts, cdk_server** ou
                 s->v.kyof != nullptr && s->v.ptilde != nullptr &&
                 (stream_supported(n, std::min(s->opts.max_box, 32)) ||
                  hankel_plan(n, K, std::min(s->opts.max_box, 32), s->v.form == CDK_FORM_FP16X2, 0, &probe));
-  if (s->streamed && use_stream_tiles(s->v.tc_variant, s->v.form == CDK_FORM_FP16X2) && stream_top_bytes(n, K) > 0) {
+  if (s->streamed && use_stream_tiles(s->v.tc_variant) && stream_top_bytes(n, K) > 0) {
     // 64^3: the streamed-tile kernel's operator image, built once per context
     const int rc = ctx_ensure_top(ctx);
     if (rc != CDK_OK) {

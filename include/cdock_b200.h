@@ -60,8 +60,7 @@ typedef struct cdk_opts {
                           line transforms at every n (default: block stages at n <= 64,
                           warp-local lines at n >= 96); [2] = 1: autotune the x pass on the first wave
                           of each new ligand box; [3] precision-form x pass: 0 = automatic
-                          (ligands <= 96 atoms, box <= 32 planes: in the split-BF16 form tcgen05
-                          with streamed operator tiles at n = 64, else tcgen05 with the Hankel
+                          (ligands <= 96 atoms, box <= 32 planes: tcgen05 with the Hankel
                           operator resident in shared memory; else the next one); 1 = mma.sync;
                           2 = tcgen05 with operands built inside the kernel (n = 64);
                           3 = streamed operator tiles (n = 64); 4 = the Hankel kernel;
@@ -71,10 +70,9 @@ typedef struct cdk_opts {
                           [5] Hankel x pass shape: bits 0-1 columns per CTA (0 = automatic,
                           1, or 2 at n <= 64), bits 2-4 K-steps per ring stage (0 = automatic,
                           1 to 4), bit 5: ligand rows copied per rotation by the producer
-                          threads, bit 6: ligand rows written by the plane kernel in
-                          128-rotation tiles that the x pass loads by bulk copies (default:
-                          tiles in the split-FP16 form at n <= 64, per-rotation copies
-                          otherwise; the same results either way);
+                          threads, bit 6 (the default): ligand rows written by the plane
+                          kernel in 128-rotation row sets that the x pass loads by tensor
+                          copies (the same results either way);
                           [6] precision forms: poses per wave re-scored in FP64
                           (cdk_ctx_top_poses): 0 = 8 (none in the FP32 form), -1 = none,
                           1..32; [7] = 1: no FP64 near-tie break of the argmin in the

@@ -16,13 +16,12 @@ TOL_TC = 1e-3
 
 
 HANKEL = {CDK_FORM_BF16X3: "tcgen05_hankel", CDK_FORM_FP16X2: "tcgen05_hankel_fp16"}
-TILES = {CDK_FORM_BF16X3: "tcgen05_streamed", CDK_FORM_FP16X2: "tcgen05_streamed_fp16"}
 
 
 def auto_kind(n, form):
-    """The automatic tensor-core x pass: in the split-BF16 form streamed operator tiles at 64^3,
-    otherwise the Hankel kernel (over tiled ligand rows in the split-FP16 form)."""
-    return TILES[form] if (n == 64 and form == CDK_FORM_BF16X3) else HANKEL[form]
+    """The automatic tensor-core x pass: the Hankel kernel over tiled ligand rows at every n and
+    in both forms (streamed operator tiles only on request)."""
+    return HANKEL[form]
 
 
 @pytest.mark.parametrize("form", [CDK_FORM_BF16X3, CDK_FORM_FP16X2])
@@ -87,7 +86,7 @@ def test_tensor_core_variants_agree(grids_cache, wave):
              "build": "tcgen05_build", "mma_sync": "mma_sync"}
     for name, kw in [("hankel", {"tc_hankel": True}), ("hankel_1col", {"tc_hankel": True, "tc_cols": 1}),
                      ("hankel_2col", {"tc_hankel": True, "tc_cols": 2}),
-                     ("stream_tiles", {}), ("build", {"tc_build": True}),
+                     ("stream_tiles", {"tc_stream_tiles": True}), ("build", {"tc_build": True}),
                      ("mma_sync", {"tc_mma_sync": True})]:
         with Receptor(w.grids, w.spacing, form=CDK_FORM_BF16X3, wave_rotations=wave, **kw) as r:
             out[name] = r.search(w.coor, w.charge, w.eps, w.slot, w.quats)
@@ -110,13 +109,13 @@ def test_tensor_core_variants_agree(grids_cache, wave):
                                                        ("c1_64", 3, 111, 0, 2),
                                                        ("c4_128", 1, 70, 45, 1)])
 def test_tiled_rows_match_thread_copies(grids_cache, form, name, n_conf, n_q, wave, cols):
-    """The Hankel x pass loads its ligand rows either as 128-rotation tiles that the plane kernel
-    writes in the tensor cores' 32-byte swizzled layout (one bulk copy per K-step and column; the
-    default for split-FP16 at 64^3, forced here in both forms and at 128^3) or rotation by
-    rotation with per-thread copies from the untiled rows. The MMAs see the same operands either
-    way, so results are bit-identical: ragged waves (partial tiles), one and two columns per CTA,
-    chunks of a tile's plan that a rotation does not touch (zeros written by the plane kernel,
-    zero-filled by the copies)."""
+    """The Hankel x pass loads its ligand rows either as 128-rotation row sets that the plane
+    kernel writes column by column (one tensor copy per K-step and column gathers the 128 rows
+    and applies the tensor cores' 32- or 64-byte swizzle; the default) or rotation by rotation
+    with per-thread copies from the untiled rows. The MMAs see the same operands either way, so
+    results are bit-identical: ragged waves (partial tiles), one and two columns per CTA, chunks
+    of a tile's plan that a rotation does not touch (zeros written by the plane kernel,
+    zero-filled by the copies), 64^3 and 128^3."""
     w = synth.make_workload(name, seed=17, n_conf=n_conf, n_q=n_q, grids_cache=grids_cache)
     out = {}
     for thread_copies in (False, True):
