@@ -107,6 +107,7 @@ def test_tensor_core_variants_agree(grids_cache, wave):
 @pytest.mark.parametrize("form", [CDK_FORM_FP16X2, CDK_FORM_BF16X3])
 @pytest.mark.parametrize("name,n_conf,n_q,wave,cols", [("c1_64", 2, 150, 200, 1),
                                                        ("c1_64", 3, 111, 0, 2),
+                                                       ("c3_96", 1, 130, 0, 1),
                                                        ("c4_128", 1, 70, 45, 1)])
 def test_tiled_rows_match_thread_copies(grids_cache, form, name, n_conf, n_q, wave, cols):
     """The Hankel x pass loads its ligand rows either as 128-rotation row sets that the plane
@@ -115,7 +116,7 @@ def test_tiled_rows_match_thread_copies(grids_cache, form, name, n_conf, n_q, wa
     with per-thread copies from the untiled rows. The MMAs see the same operands either way, so
     results are bit-identical: ragged waves (partial tiles), one and two columns per CTA, chunks
     of a tile's plan that a rotation does not touch (zeros written by the plane kernel,
-    zero-filled by the copies), 64^3 and 128^3."""
+    zero-filled by the copies), 64^3, 96^3 and 128^3."""
     w = synth.make_workload(name, seed=17, n_conf=n_conf, n_q=n_q, grids_cache=grids_cache)
     out = {}
     for thread_copies in (False, True):
