@@ -819,16 +819,21 @@ bool hankel_plan(int n, int K, int Lb, bool f16, int cols_pref, HankelPlan* out,
     for (int pass = two ? 0 : 1; pass < 2; ++pass) {
       const size_t cap = (pass == 0 ? kSmemHalf : kSmemCap) - 1024;
       // automatic: 3 K-steps per stage where the box has at least 3 (measured over tiled rows,
-      // x pass: split-BF16 12 % faster at 64^3, 4.5 % at 128^3; split-FP16 4.5 % at 128^3, and
-      // 5 % at 96^3 in both forms), except at n <= 64 in the split-FP16 form (2: 3 measured
-      // 1.5 % slower), else 2 where it has several, else 1
+      // x pass: split-BF16 4.5 % faster at 128^3; split-FP16 4.5 % at 128^3, and 5 % at 96^3 in
+      // both forms), except at n <= 64 in the split-FP16 form (2: 3 measured 1.5 % slower), else
+      // 2 where it has several, else 1; fewer where the ring would not keep two CTAs per SM
+      // busy otherwise (split-BF16 at 64^3: 1, below)
       const int ks_auto = (jc >= 3 && !(f16 && n <= 64)) ? 3 : jc >= 2 ? 2 : 1;
       for (int ks : {4, 3, 2, 1}) {
         if (ks_pref ? ks != ks_pref : ks > ks_auto) continue;
         const HxLayout L = hx_layout(n, K, cols, f16, G, ks);
         if (cap <= L.ring) continue;
         int nb = (int)std::min<size_t>(HX_MAXSTAGES, (cap - L.ring) / L.stage);
-        if (nb < 2 || nb * ks < (pass == 0 ? 8 : 4) || (size_t)nb * L.stage < L.build) continue;
+        // two CTAs per SM want 8 K-steps in flight, or at least 4 stages (split-BF16 at 64^3: 5
+        // stages of one K-step, x pass 72.0 ms per 1e5 rotations against 88.5 with one CTA per
+        // SM and 6 stages of 3 K-steps, 82.7 with two CTAs of 2 stages of 2 K-steps)
+        const bool enough = pass == 0 ? (nb * ks >= 8 || (nb >= 4 && nb * ks >= 4)) : nb * ks >= 4;
+        if (nb < 2 || !enough || (size_t)nb * L.stage < L.build) continue;
         if (nb_cap > 0 && nb_cap < nb && (size_t)nb_cap * L.stage >= L.build && nb_cap >= 2) nb = nb_cap;
         out->cols = cols;
         out->G = G;
