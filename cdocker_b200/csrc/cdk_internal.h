@@ -132,7 +132,9 @@ inline bool use_stream_tiles(int variant) { return variant == 3; }
 // opts.reserved[5] bit 5 asks for per-rotation copies by its producer threads (bit 6, tiled
 // rows, is the default). Measured per search against per-rotation copies: 64^3 -13 % (split-FP16)
 // and -19 % (split-BF16), 96^3 -6 % and -13 %, 128^3 -3 % and -6 %
-inline bool hankel_tiled(int reserved5) { return !(reserved5 & 32); }
+// (and the driver provides the tensor-map encoder; without it the per-rotation copies run)
+bool tensor_maps_available();
+inline bool hankel_tiled(int reserved5) { return !(reserved5 & 32) && tensor_maps_available(); }
 // bytes of a wave's ligand rows (per-rotation bytes times the rotations allocated)
 inline size_t lop_wave_bytes(long nrot, bool tiled, size_t per_rotation) {
   return lop_rotations(nrot, tiled) * per_rotation;

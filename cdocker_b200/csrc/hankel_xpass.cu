@@ -798,6 +798,8 @@ cudaError_t launch_hx(const WaveArgs& a, const float2* pt, const HxScale& sc, in
 
 }  // namespace
 
+bool tensor_maps_available() { return tensor_map_encoder() != nullptr; }
+
 // Shape of the x pass for (n, K, ligand box, form): columns per CTA, Hankel groups, ring stages
 // (each of ks K-steps) and dynamic shared memory. cols_pref: 0 = automatic (1), 1 or 2 = that
 // many columns (2 only where the operator of two columns fits); ks_pref: 0 = automatic (2 K-steps per

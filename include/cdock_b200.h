@@ -70,9 +70,10 @@ typedef struct cdk_opts {
                           [5] Hankel x pass shape: bits 0-1 columns per CTA (0 = automatic,
                           1, or 2 at n <= 64), bits 2-4 K-steps per ring stage (0 = automatic,
                           1 to 4), bit 5: ligand rows copied per rotation by the producer
-                          threads, bit 6 (the default): ligand rows written by the plane
-                          kernel in 128-rotation row sets that the x pass loads by tensor
-                          copies (the same results either way);
+                          threads, bit 6 (the default where the driver provides the
+                          tensor-map encoder): ligand rows written by the plane kernel in
+                          128-rotation row sets that the x pass loads by tensor copies (the
+                          same results either way);
                           [6] precision forms: poses per wave re-scored in FP64
                           (cdk_ctx_top_poses): 0 = 8 (none in the FP32 form), -1 = none,
                           1..32; [7] = 1: no FP64 near-tie break of the argmin in the
